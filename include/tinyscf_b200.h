@@ -1,0 +1,85 @@
+/*
+ * Extensions of the B200 engine beyond the reference's TinySCF API. None of
+ * these exist in the reference; they give FFI callers status codes instead of
+ * abort(), let tests feed a density in, and expose device timings.
+ */
+#ifndef TINYSCF_B200_EXT_H
+#define TINYSCF_B200_EXT_H
+
+#include <stddef.h>
+#include "TinySCF.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (0 = success). */
+#define TINYSCF_OK              0
+#define TINYSCF_ERR_CUDA        1
+#define TINYSCF_ERR_FILEIO      2
+#define TINYSCF_ERR_INPUT       3
+#define TINYSCF_ERR_UNSUPPORTED 4
+#define TINYSCF_ERR_ALLOC       5
+#define TINYSCF_ERR_NUMERIC     6
+#define TINYSCF_ERR_STATE       7
+
+/* Device-event timers (milliseconds of the last call of each phase). */
+enum {
+    TINYSCF_T_HCORE = 0,     /* S, Hcore, X                          */
+    TINYSCF_T_SCHWARZ,       /* Schwarz quartets + DF screening      */
+    TINYSCF_T_GUESS,         /* SAD upload + pivoted Cholesky        */
+    TINYSCF_T_3C,            /* 3-centre integrals                   */
+    TINYSCF_T_2C,            /* (P|Q)                                */
+    TINYSCF_T_INVSQRT,       /* (P|Q)^-1/2                           */
+    TINYSCF_T_DFGEMM,        /* B = (mn|P) (P|Q)^-1/2                */
+    TINYSCF_T_J,             /* J build                              */
+    TINYSCF_T_K_HT,          /* K occupied half-transform            */
+    TINYSCF_T_K_SYRK,        /* K = T T^T                            */
+    TINYSCF_T_FOCK,          /* F = H + 2J - K and energy            */
+    TINYSCF_T_DIIS,          /* DIIS                                 */
+    TINYSCF_T_DENSITY,       /* eigensolve + density                 */
+    TINYSCF_T_ITER,          /* one SCF iteration                    */
+    TINYSCF_T_SCF,           /* the whole TinySCF_do_SCF             */
+    TINYSCF_T_COUNT
+};
+
+/* malloc a zeroed struct for callers that cannot use sizeof (FFI);
+ * free_TinySCF releases it, as it does a caller-malloc'd struct. */
+TINYSCF_API TinySCF_t TinySCF_alloc(void);
+/* sizeof(struct TinySCF_struct) as compiled into the library, for FFI mirrors. */
+TINYSCF_API size_t TinySCF_struct_size(void);
+TINYSCF_API const char *TinySCF_status_string(int status);
+
+/* Status-returning twins of the TinySCF API (same semantics, no abort). */
+TINYSCF_API int TinySCF_init_status(TinySCF_t t, const char *bas_fname, const char *df_bas_fname,
+                        const char *xyz_fname, int niters);
+TINYSCF_API int TinySCF_compute_Hcore_Ovlp_mat_status(TinySCF_t t);
+TINYSCF_API int TinySCF_compute_sq_Schwarz_scrvals_status(TinySCF_t t);
+TINYSCF_API int TinySCF_prepare_sparsity_status(TinySCF_t t);
+TINYSCF_API int TinySCF_get_initial_guess_status(TinySCF_t t);
+TINYSCF_API int TinySCF_build_DF_tensor_status(TinySCF_t t);
+TINYSCF_API int TinySCF_build_FockMat_status(TinySCF_t t);
+TINYSCF_API int TinySCF_DIIS_status(TinySCF_t t);
+TINYSCF_API int TinySCF_build_DenMat_status(TinySCF_t t);
+TINYSCF_API int TinySCF_do_SCF_status(TinySCF_t t);
+TINYSCF_API int TinySCF_free_status(TinySCF_t t);
+
+/* Upload a density (nbf x nbf) and its factor (nbf x n_occ; NULL keeps the
+ * current one) from host memory; used before TinySCF_build_FockMat. */
+TINYSCF_API int TinySCF_set_density(TinySCF_t t, const double *D, const double *Cocc);
+/* Upload a Fock matrix (nbf x nbf): the input of TinySCF_DIIS, or, with
+ * orthogonal != 0, the X^T F X input of TinySCF_build_DenMat. */
+TINYSCF_API int TinySCF_set_fock(TinySCF_t t, const double *F, int orthogonal);
+/* Copy S, Hcore, X, F, D, J, K, Cocc, eigval and DIIS state to the host mirrors. */
+TINYSCF_API int TinySCF_sync_host(TinySCF_t t);
+/* Copy the DF tensor in the reference's layout: rows in bf_pair CSR order
+ * (nnz rows), df_nbf columns. out must hold num_bf_pair_scr * df_nbf doubles. */
+TINYSCF_API int TinySCF_get_df_tensor(TinySCF_t t, double *out);
+/* Timers: writes min(n, TINYSCF_T_COUNT) values in milliseconds. */
+TINYSCF_API int TinySCF_get_timings(TinySCF_t t, double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

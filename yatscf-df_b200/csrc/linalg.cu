@@ -1,0 +1,318 @@
+// Dense FP64 building blocks for the SCF: a tiled DGEMM, the symmetric
+// eigensolver wrapper (cuSOLVER syevd), inverse square roots from
+// eigenpairs (TinySCF.c:58-76, build_DF_tensor.c:205-237), and the pivoted
+// Cholesky of the initial guess (TinySCF.c:282-322, LAPACK dpstf2 semantics).
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cusolverDn.h>
+
+#include "tscf_internal.h"
+
+namespace tscf {
+
+// ------------------------------------------------------------------ DGEMM
+// 64x64 output tile per 256-thread block, 4x4 outputs per thread, K step 16.
+// op(A) is m x k, op(B) is k x n, everything row-major.
+constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256) k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
+                                               const double *__restrict__ B, int ldb, double beta, double *C, int ldc)
+{
+    __shared__ double As[GB_K][GB_M + 1];
+    __shared__ double Bs[GB_K][GB_N + 1];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int m0 = blockIdx.y * GB_M, n0 = blockIdx.x * GB_N;
+    double acc[4][4] = {};
+    for (int k0 = 0; k0 < k; k0 += GB_K) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            int l = tid + 256 * r;
+            int row, kk;
+            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / GB_M; row = l % GB_M; }
+            int gi = m0 + row, gk = k0 + kk;
+            double v = 0.0;
+            if (gi < m && gk < k) v = TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk];
+            As[kk][row] = v;
+            int col;
+            if (!TB) { kk = l / GB_N; col = l % GB_N; } else { col = l / GB_K; kk = l % GB_K; }
+            int gj = n0 + col;
+            gk = k0 + kk;
+            double w = 0.0;
+            if (gj < n && gk < k) w = TB ? B[(size_t) gj * ldb + gk] : B[(size_t) gk * ldb + gj];
+            Bs[kk][col] = w;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GB_K; kk++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int gi = m0 + ty + 16 * i;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            int gj = n0 + tx + 16 * j;
+            if (gj >= n) continue;
+            double *c = C + (size_t) gi * ldc + gj;
+            *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * *c;
+        }
+    }
+}
+
+void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda, const double *B, int ldb,
+           double beta, double *C, int ldc, cudaStream_t s)
+{
+    if (m <= 0 || n <= 0) return;
+    dim3 grid((n + GB_N - 1) / GB_N, (m + GB_M - 1) / GB_M);
+    if (!ta && !tb) k_dgemm<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (!ta && tb) k_dgemm<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (ta && !tb) k_dgemm<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else k_dgemm<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+// ------------------------------------------------------------------ eigensolver
+struct Eig {
+    int n;
+    cusolverDnHandle_t h;
+    double *work;
+    int lwork;
+    int *info;
+};
+
+Eig *eig_create(int n, cudaStream_t s)
+{
+    Eig *e = new Eig();
+    e->n = n;
+    if (cusolverDnCreate(&e->h) != CUSOLVER_STATUS_SUCCESS) { delete e; return nullptr; }
+    cusolverDnSetStream(e->h, s);
+    int lw = 0;
+    if (cusolverDnDsyevd_bufferSize(e->h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, nullptr, n, nullptr,
+                                    &lw) != CUSOLVER_STATUS_SUCCESS) {
+        cusolverDnDestroy(e->h);
+        delete e;
+        return nullptr;
+    }
+    e->lwork = lw;
+    if (cudaMalloc(&e->work, sizeof(double) * (size_t) (lw > 0 ? lw : 1)) != cudaSuccess ||
+        cudaMalloc(&e->info, sizeof(int)) != cudaSuccess) {
+        cusolverDnDestroy(e->h);
+        delete e;
+        return nullptr;
+    }
+    return e;
+}
+
+void eig_destroy(Eig *e)
+{
+    if (!e) return;
+    cudaFree(e->work);
+    cudaFree(e->info);
+    cusolverDnDestroy(e->h);
+    delete e;
+}
+
+// A symmetric, so row- and column-major agree; cuSOLVER leaves the eigenvectors
+// in the columns of its column-major output, i.e. in the rows of our row-major view.
+int eig_run(Eig *e, const double *d_A, double *d_w, double *d_V, cudaStream_t s)
+{
+    if (d_V != d_A) cudaMemcpyAsync(d_V, d_A, sizeof(double) * (size_t) e->n * e->n, cudaMemcpyDeviceToDevice, s);
+    cusolverDnSetStream(e->h, s);
+    cusolverStatus_t st = cusolverDnDsyevd(e->h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, e->n, d_V, e->n,
+                                           d_w, e->work, e->lwork, e->info);
+    return st == CUSOLVER_STATUS_SUCCESS ? OK : ERR_NUMERIC;
+}
+
+__global__ void k_scale_rows_invsqrt(const double *w, const double *V, double *out, int n)
+{
+    size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t) n * n) return;
+    int k = (int) (idx / n);
+    out[idx] = V[idx] / sqrt(w[k]);
+}
+
+void inv_sqrt_from_eig(const double *d_w, const double *d_V, double *d_X, double *d_tmp, int n, cudaStream_t s)
+{
+    size_t nn = (size_t) n * n;
+    k_scale_rows_invsqrt<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(d_w, d_V, d_tmp, n);
+    // X = V^T diag(w^-1/2) V
+    dgemm(true, false, n, n, n, 1.0, d_V, n, d_tmp, n, 0.0, d_X, n, s);
+}
+
+// ------------------------------------------------------------------ pivoted Cholesky
+// One 1024-thread block runs LAPACK dpstf2 (UPLO = 'L') step for step on the
+// logical matrix A(i,j) = A[i*n + j]: left-looking column updates, diagonal
+// candidates A(i,i) - sum_k A(i,k)^2 accumulated in work[], first-maximum
+// pivot, the same row/column swaps, stop when the pivot <= tol.
+struct ValIdx {
+    double v;
+    int i;
+};
+__device__ __forceinline__ ValIdx better(ValIdx a, ValIdx b)
+{
+    if (b.v > a.v || (b.v == a.v && b.i < a.i)) return b;
+    return a;
+}
+
+__device__ ValIdx block_argmax(ValIdx x, ValIdx *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        ValIdx y;
+        y.v = __shfl_down_sync(0xffffffff, x.v, o);
+        y.i = __shfl_down_sync(0xffffffff, x.i, o);
+        x = better(x, y);
+    }
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        x = (lane < (int) (blockDim.x >> 5)) ? sh[lane] : ValIdx{-DBL_MAX, 0x7fffffff};
+        for (int o = 16; o > 0; o >>= 1) {
+            ValIdx y;
+            y.v = __shfl_down_sync(0xffffffff, x.v, o);
+            y.i = __shfl_down_sync(0xffffffff, x.i, o);
+            x = better(x, y);
+        }
+        if (lane == 0) sh[0] = x;
+    }
+    __syncthreads();
+    ValIdx r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, int *piv, int *rank_out, double *work)
+{
+    __shared__ ValIdx sh[32];
+    __shared__ int s_stop;
+    double *dot = work, *cand = work + n;
+#define AA(i, j) A[(size_t) (i) * n + (j)]
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        dot[i] = 0.0;
+        piv[i] = i;
+    }
+    __syncthreads();
+    // j = 0: pivot on the largest diagonal element
+    ValIdx best{-DBL_MAX, 0x7fffffff};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) best = better(best, ValIdx{AA(i, i), i});
+    best = block_argmax(best, sh);
+    double ajj = best.v;
+    int pvt = best.i;
+    if (threadIdx.x == 0) s_stop = (ajj <= 0.0 || isnan(ajj)) ? 1 : 0;
+    __syncthreads();
+    if (s_stop) {
+        if (threadIdx.x == 0) *rank_out = 0;
+        return;
+    }
+    int rank = n;
+    for (int j = 0; j < n; j++) {
+        if (j > 0) {
+            ValIdx b{-DBL_MAX, 0x7fffffff};
+            for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+                double a = AA(i, j - 1);
+                dot[i] += a * a;
+                double c = AA(i, i) - dot[i];
+                cand[i] = c;
+                b = better(b, ValIdx{c, i});
+            }
+            b = block_argmax(b, sh);
+            pvt = b.i;
+            ajj = b.v;
+            if (ajj <= tol || isnan(ajj)) {
+                if (threadIdx.x == 0) AA(j, j) = ajj;
+                rank = j;
+                break;
+            }
+        }
+        if (j != pvt) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                AA(pvt, pvt) = AA(j, j);
+                double t = dot[j]; dot[j] = dot[pvt]; dot[pvt] = t;
+                int p = piv[pvt]; piv[pvt] = piv[j]; piv[j] = p;
+            }
+            for (int c = threadIdx.x; c < j; c += blockDim.x) {          // rows j and pvt, columns 0..j-1
+                double t = AA(j, c); AA(j, c) = AA(pvt, c); AA(pvt, c) = t;
+            }
+            for (int r = pvt + 1 + threadIdx.x; r < n; r += blockDim.x) { // columns j and pvt below pvt
+                double t = AA(r, j); AA(r, j) = AA(r, pvt); AA(r, pvt) = t;
+            }
+            for (int r = j + 1 + threadIdx.x; r < pvt; r += blockDim.x) { // column j (rows j+1..pvt-1) vs row pvt
+                double t = AA(r, j); AA(r, j) = AA(pvt, r); AA(pvt, r) = t;
+            }
+            __syncthreads();
+        }
+        ajj = sqrt(ajj);
+        if (threadIdx.x == 0) AA(j, j) = ajj;
+        __syncthreads();
+        // A(j+1:n, j) = (A(j+1:n, j) - A(j+1:n, 0:j) A(j, 0:j)^T) / ajj : one warp per row
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        const double rinv = 1.0 / ajj;
+        for (int r = j + 1 + wid; r < n; r += nw) {
+            double s = 0.0;
+            for (int c = lane; c < j; c += 32) s += AA(r, c) * AA(j, c);
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffff, s, o);
+            if (lane == 0) AA(r, j) = (AA(r, j) - s) * rinv;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *rank_out = rank;
+#undef AA
+}
+
+void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s)
+{
+    k_pstf2<<<1, 1024, 0, s>>>(d_A, n, tol, d_piv, d_rank, d_work);
+}
+
+__global__ void k_d2cocc(const double *chol, const int *rank_p, double *C, int nbf, int nocc)
+{
+    size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t) nbf * nocc) return;
+    int i = (int) (idx / nocc), j = (int) (idx % nocc);
+    int rank = *rank_p;
+    double v = (j < nbf) ? chol[(size_t) i * nbf + j] : 0.0;
+    if (rank < nocc && j >= rank) v = 0.0;
+    if (i < nocc && j >= i) v = 0.0;
+    C[idx] = v;
+}
+
+void d2cocc_copy(const double *d_chol, const int *d_rank, double *d_Cocc, int nbf, int nocc, cudaStream_t s)
+{
+    size_t n = (size_t) nbf * nocc;
+    k_d2cocc<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(d_chol, d_rank, d_Cocc, nbf, nocc);
+}
+
+// ------------------------------------------------------------------ elementwise
+__global__ void k_fill(double *d, double v, size_t n)
+{
+    size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = v;
+}
+void fill(double *d, double v, size_t n, cudaStream_t s)
+{
+    if (n) k_fill<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(d, v, n);
+}
+__global__ void k_scale_copy(const double *a, double *b, double f, size_t n)
+{
+    size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = f * a[i];
+}
+void scale_copy(const double *src, double *dst, double a, size_t n, cudaStream_t s)
+{
+    if (n) k_scale_copy<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(src, dst, a, n);
+}
+
+}  // namespace tscf

@@ -1,0 +1,1245 @@
+// Host side of the B200 DF-RHF engine: the TinySCF C API (include/TinySCF.h
+// and friends) over the sm_100a kernels of ints.cu, linalg.cu, fock.cu and
+// scf.cu. Input parsing follows libCMS (CMS_BasisSet.c) so the same .gbs/.xyz
+// and SAD files give the same shells, charges and guesses; the screening and
+// sparsity bookkeeping follows TinySCF.c:112-280 on the host (small, O(nbf^2)),
+// everything O(nbf^2 * naux) and up runs on the device.
+#include <algorithm>
+#include <cctype>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "TinySCF.h"
+#include "DIIS.h"
+#include "build_DF_tensor.h"
+#include "build_Fock.h"
+#include "build_density.h"
+#include "tinyscf_b200.h"
+#include "tscf_internal.h"
+
+using namespace tscf;
+
+namespace {
+
+const double A2BOHR = 1.0 / 0.52917720859;   // CMS_BasisSet.c:39
+const int ELEN = 50;
+const char *ETABLE[ELEN] = {"H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg", "Al",
+                            "Si", "P",  "S",  "Cl", "Ar", "K",  "Ca", "Sc", "Ti", "V",  "Cr", "Mn", "Fe",
+                            "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",
+                            "Zr", "Nb", "Mo", "Tc", "Ru", "Rh", "Pd", "Ag", "Cd", "In", "Sn"};
+const char MTABLE[] = "SPDFG";
+
+struct ShellDef {
+    int am;
+    std::vector<double> ex, cc;
+};
+
+struct BasisDef {
+    std::map<int, std::vector<ShellDef>> elem;   // 0-based element index -> shells
+    std::string dir;
+};
+
+struct Molecule {
+    int natoms = 0, Q = 0, nelec = 0;
+    std::vector<int> eid;        // 0-based element index
+    std::vector<double> xyz;     // Bohr
+    double enuc = 0.0;
+};
+
+struct HostShells {
+    int nsh = 0, nbf = 0, maxam = 0;
+    std::vector<int> am, nprim, poff, bfoff, atom_of;
+    std::vector<double> cen, alpha, coef;
+    std::vector<int> atom_bf0, atom_bf1;
+};
+
+int elem_index(const char *s)
+{
+    for (int i = 0; i < ELEN; i++)
+        if (strcmp(s, ETABLE[i]) == 0) return i;
+    return -1;
+}
+
+// CMS_import_molecule (CMS_BasisSet.c:310-426)
+int parse_xyz(const char *fn, Molecule &m)
+{
+    FILE *f = fopen(fn, "r");
+    if (!f) return ERR_FILEIO;
+    char line[1024], str[1024];
+    int rc = OK;
+    if (!fgets(line, sizeof(line), f) || sscanf(line, "%d", &m.natoms) != 1 || m.natoms <= 0) rc = ERR_INPUT;
+    if (rc == OK && !fgets(line, sizeof(line), f)) rc = ERR_INPUT;
+    if (rc == OK) m.Q = (int) atof(line);
+    while (rc == OK && fgets(line, sizeof(line), f)) {
+        double x, y, z;
+        int nsc = sscanf(line, "%1023s %lf %lf %lf", str, &x, &y, &z);
+        if (nsc < 1 || !isalpha((unsigned char) str[0])) continue;
+        int e = (strlen(str) <= 2) ? elem_index(str) : -1;
+        if (e < 0 || nsc < 4) { rc = ERR_INPUT; break; }
+        m.eid.push_back(e);
+        m.xyz.push_back(x * A2BOHR);
+        m.xyz.push_back(y * A2BOHR);
+        m.xyz.push_back(z * A2BOHR);
+        m.nelec += e + 1;
+    }
+    fclose(f);
+    if (rc != OK) return rc;
+    if ((int) m.eid.size() != m.natoms) return ERR_INPUT;
+    m.enuc = 0.0;
+    for (int a = 0; a < m.natoms; a++)
+        for (int b = a + 1; b < m.natoms; b++) {
+            double dx = m.xyz[3 * a] - m.xyz[3 * b], dy = m.xyz[3 * a + 1] - m.xyz[3 * b + 1],
+                   dz = m.xyz[3 * a + 2] - m.xyz[3 * b + 2];
+            m.enuc += (m.eid[a] + 1.0) * (m.eid[b] + 1.0) / sqrt(dx * dx + dy * dy + dz * dz);
+        }
+    return OK;
+}
+
+// CMS_import_basis (CMS_BasisSet.c:439-642): SP-type shells split into S, P, ...
+int parse_gbs(const char *fn, BasisDef &b)
+{
+    FILE *f = fopen(fn, "r");
+    if (!f) return ERR_FILEIO;
+    std::vector<std::string> lines;
+    char buf[1024];
+    while (fgets(buf, sizeof(buf), f)) lines.push_back(buf);
+    fclose(f);
+    if (lines.empty()) return ERR_INPUT;
+    char str[1024] = {0};
+    if (sscanf(lines[0].c_str(), "%1023s", str) == 1 && strcmp(str, "spherical") == 0)
+        return ERR_UNSUPPORTED;   // the engine is Cartesian-only, like Simint's path in the reference
+    size_t i = 1;
+    while (i < lines.size()) {
+        const std::string &L = lines[i++];
+        if (L.empty() || !isalpha((unsigned char) L[0])) continue;
+        sscanf(L.c_str(), "%1023s", str);
+        int e = elem_index(str);
+        if (e < 0) return ERR_INPUT;
+        std::vector<ShellDef> shells;
+        while (i < lines.size()) {
+            const std::string &S = lines[i++];
+            if (!S.empty() && isalpha((unsigned char) S[0])) {
+                int nexp = 0;
+                double beta = 0;
+                char kind[64] = {0};
+                if (sscanf(S.c_str(), "%63s %d %lf", kind, &nexp, &beta) < 2) return ERR_INPUT;
+                int ns = (int) strlen(kind);
+                if (nexp <= 0 || ns <= 0 || ns > 3) return ERR_INPUT;
+                if (i + nexp > lines.size()) return ERR_INPUT;
+                std::vector<double> ex(nexp), cc[3];
+                for (int k = 0; k < 3; k++) cc[k].assign(nexp, 0.0);
+                for (int p = 0; p < nexp; p++) {
+                    const std::string &R = lines[i + p];
+                    if (R.empty() || R[0] == '*' || isalpha((unsigned char) R[0])) return ERR_INPUT;
+                    double v[4] = {0, 0, 0, 0};
+                    sscanf(R.c_str(), "%lf %lf %lf %lf", &v[0], &v[1], &v[2], &v[3]);
+                    ex[p] = v[0];
+                    for (int k = 0; k < 3; k++) cc[k][p] = v[1 + k];
+                }
+                i += nexp;
+                for (int k = 0; k < ns; k++) {
+                    const char *pos = strchr(MTABLE, kind[k]);
+                    if (!pos || kind[k] == 0) return ERR_INPUT;
+                    ShellDef d;
+                    d.am = (int) (pos - MTABLE);
+                    d.ex = ex;
+                    d.cc = cc[k];
+                    shells.push_back(d);
+                }
+            }
+            if (!S.empty() && S[0] == '*') break;
+        }
+        b.elem[e] = shells;
+    }
+    std::string p(fn);
+    size_t sl = p.find_last_of('/');
+    b.dir = (sl == std::string::npos) ? std::string(".") : p.substr(0, sl);
+    return OK;
+}
+
+// CMS_import_guess (CMS_BasisSet.c:657-746): one value per line; a missing,
+// short or (one-sidedly) asymmetric file gives a zero block.
+std::vector<double> load_sad(const BasisDef &b, int e, int nf)
+{
+    std::vector<double> g((size_t) nf * nf, 0.0);
+    std::string fn = b.dir + "/" + ETABLE[e] + ".dat";
+    FILE *f = fopen(fn.c_str(), "r");
+    if (!f) return g;
+    char line[1024];
+    bool bad = false;
+    for (int k = 0; k < nf * nf; k++) {
+        if (!fgets(line, sizeof(line), f)) { bad = true; break; }
+        sscanf(line, "%le", &g[k]);
+    }
+    fclose(f);
+    if (!bad)
+        for (int j = 0; j < nf && !bad; j++)
+            for (int k = 0; k < nf; k++)
+                if (g[(size_t) j * nf + k] - g[(size_t) k * nf + j] > 1e-12) { bad = true; break; }
+    if (bad) std::fill(g.begin(), g.end(), 0.0);
+    return g;
+}
+
+double dfact(int n)
+{
+    double r = 1.0;
+    for (int k = n; k > 1; k -= 2) r *= k;
+    return r;
+}
+
+// Contracted-shell normalisation with unit-norm x^l component.
+void normalize(int am, const std::vector<double> &al, const std::vector<double> &cc, std::vector<double> &out)
+{
+    const int n = (int) al.size();
+    const double df = dfact(2 * am - 1);
+    out.resize(n);
+    for (int k = 0; k < n; k++)
+        out[k] = cc[k] * pow(2.0 * al[k] / M_PI, 0.75) * pow(4.0 * al[k], 0.5 * am) / sqrt(df);
+    double s = 0.0;
+    for (int k = 0; k < n; k++)
+        for (int l = 0; l < n; l++) {
+            double p = al[k] + al[l];
+            s += out[k] * out[l] * pow(M_PI / p, 1.5) * df / pow(2.0 * p, am);
+        }
+    double fct = 1.0 / sqrt(s);
+    for (auto &v : out) v *= fct;
+}
+
+int build_shells(const Molecule &m, const BasisDef &b, HostShells &h)
+{
+    h = HostShells();
+    for (int a = 0; a < m.natoms; a++) {
+        auto it = b.elem.find(m.eid[a]);
+        if (it == b.elem.end()) return ERR_INPUT;
+        h.atom_bf0.push_back(h.nbf);
+        for (const ShellDef &d : it->second) {
+            std::vector<double> cn;
+            normalize(d.am, d.ex, d.cc, cn);
+            h.am.push_back(d.am);
+            h.nprim.push_back((int) d.ex.size());
+            h.poff.push_back((int) h.alpha.size());
+            h.bfoff.push_back(h.nbf);
+            h.atom_of.push_back(a);
+            for (int k = 0; k < 3; k++) h.cen.push_back(m.xyz[3 * a + k]);
+            h.alpha.insert(h.alpha.end(), d.ex.begin(), d.ex.end());
+            h.coef.insert(h.coef.end(), cn.begin(), cn.end());
+            h.nbf += ncart(d.am);
+            h.maxam = std::max(h.maxam, d.am);
+            h.nsh++;
+        }
+        h.atom_bf1.push_back(h.nbf);
+    }
+    h.bfoff.push_back(h.nbf);
+    return OK;
+}
+
+// ------------------------------------------------------------------ device state
+struct DevArrays {
+    int *am = nullptr, *np = nullptr, *poff = nullptr, *bfoff = nullptr, *ids = nullptr;
+    double *cen = nullptr, *al = nullptr, *co = nullptr;
+    std::vector<int> am_start;
+    DevShells view() const
+    {
+        return DevShells{0, am, np, poff, bfoff, cen, al, co};
+    }
+};
+
+struct Engine {
+    Molecule mol;
+    BasisDef bas, dfbas;
+    HostShells sh, ash;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev0[TINYSCF_T_COUNT], ev1[TINYSCF_T_COUNT];
+    bool ev_used[TINYSCF_T_COUNT];
+    double timers[TINYSCF_T_COUNT];
+    DevArrays dsh, dash;
+    double *Z = nullptr, *xyz = nullptr;
+    size_t nn = 0;
+    double *S = nullptr, *H = nullptr, *X = nullptr, *F = nullptr, *Fp = nullptr, *D = nullptr, *J = nullptr,
+           *K = nullptr, *Cocc = nullptr, *tmp = nullptr, *tmp2 = nullptr, *w = nullptr, *V = nullptr;
+    double *F0 = nullptr, *R = nullptr;
+    DiisState *diis = nullptr;
+    double *sp_scr = nullptr, *bf_scr = nullptr, *df_scr = nullptr;
+    int *piv = nullptr, *rank = nullptr;
+    double *pwork = nullptr;
+    // sparsity
+    int nnz = 0, nu = 0, nup = 0;
+    int *csr_j = nullptr, *csr_displs = nullptr, *csr_u = nullptr, *up_i = nullptr, *up_j = nullptr,
+        *up_u = nullptr, *upair = nullptr;
+    int2 *pairs3c = nullptr;
+    std::vector<int> cls_start, cls_la, cls_lb;
+    double *B = nullptr;
+    double *T = nullptr, *Kpart = nullptr;
+    int2 *tiles = nullptr;
+    int ksplit = 1;
+    double *Jt = nullptr, *Jpart = nullptr, *Jw = nullptr;
+    int jblk = 1;
+    double *epart = nullptr, *E = nullptr;
+    Eig *eig = nullptr;
+    int stage = 0;            // 1 hcore, 2 schwarz, 3 sparsity, 4 guess, 5 df
+    bool F_is_orth = false;   // which buffer currently plays the reference's F_mat
+    std::vector<void *> allocs;
+
+    FockPlan plan() const
+    {
+        FockPlan p;
+        p.nbf = sh.nbf;
+        p.naux = ash.nbf;
+        p.nocc = 0;
+        p.nnz = nnz;
+        p.nup = nup;
+        p.csr_j = csr_j;
+        p.csr_displs = csr_displs;
+        p.csr_u = csr_u;
+        p.up_i = up_i;
+        p.up_j = up_j;
+        p.up_u = up_u;
+        p.B = B;
+        return p;
+    }
+};
+
+Engine *E_(TinySCF_t t) { return (Engine *) t->dev; }
+
+template <typename T>
+int dalloc(Engine *e, T **p, size_t count)
+{
+    void *q = nullptr;
+    if (cudaMalloc(&q, sizeof(T) * (count ? count : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        fprintf(stderr, "[tinyscf] device allocation of %zu bytes failed\n", sizeof(T) * count);
+        return ERR_ALLOC;
+    }
+    e->allocs.push_back(q);
+    *p = (T *) q;
+    return OK;
+}
+
+void dfree(Engine *e, void *p)
+{
+    if (!p) return;
+    cudaFree(p);
+    auto it = std::find(e->allocs.begin(), e->allocs.end(), p);
+    if (it != e->allocs.end()) e->allocs.erase(it);
+}
+
+template <typename T>
+int upload(Engine *e, T **p, const std::vector<T> &v)
+{
+    int rc = dalloc(e, p, v.size());
+    if (rc) return rc;
+    if (!v.empty() && cudaMemcpyAsync(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, e->s) != cudaSuccess)
+        return ERR_CUDA;
+    return OK;
+}
+
+void tstart(Engine *e, int k)
+{
+    cudaEventRecord(e->ev0[k], e->s);
+}
+void tstop(Engine *e, int k)
+{
+    cudaEventRecord(e->ev1[k], e->s);
+    e->ev_used[k] = true;
+}
+void tcollect(Engine *e)
+{
+    for (int k = 0; k < TINYSCF_T_COUNT; k++)
+        if (e->ev_used[k]) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e->ev0[k], e->ev1[k]) == cudaSuccess) e->timers[k] = ms;
+            e->ev_used[k] = false;
+        }
+}
+
+int cuda_rc(const char *what)
+{
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {
+        fprintf(stderr, "[tinyscf] CUDA error after %s: %s\n", what, cudaGetErrorString(err));
+        return ERR_CUDA;
+    }
+    return OK;
+}
+
+int sync_rc(Engine *e, const char *what)
+{
+    cudaError_t err = cudaStreamSynchronize(e->s);
+    if (err == cudaSuccess) err = cudaGetLastError();
+    if (err != cudaSuccess) {
+        fprintf(stderr, "[tinyscf] CUDA error in %s: %s\n", what, cudaGetErrorString(err));
+        return ERR_CUDA;
+    }
+    return OK;
+}
+
+int upload_shells(Engine *e, const HostShells &h, int maxl, DevArrays &d)
+{
+    int rc;
+    if ((rc = upload(e, &d.am, h.am)) || (rc = upload(e, &d.np, h.nprim)) || (rc = upload(e, &d.poff, h.poff)) ||
+        (rc = upload(e, &d.bfoff, h.bfoff)) || (rc = upload(e, &d.cen, h.cen)) || (rc = upload(e, &d.al, h.alpha)) ||
+        (rc = upload(e, &d.co, h.coef)))
+        return rc;
+    std::vector<int> ids;
+    d.am_start.assign(maxl + 2, 0);
+    for (int l = 0; l <= maxl; l++) {
+        d.am_start[l] = (int) ids.size();
+        for (int i = 0; i < h.nsh; i++)
+            if (h.am[i] == l) ids.push_back(i);
+    }
+    d.am_start[maxl + 1] = (int) ids.size();
+    return upload(e, &d.ids, ids);
+}
+
+DevShells shells_view(const DevArrays &d, int nsh)
+{
+    DevShells v = d.view();
+    v.nsh = nsh;
+    return v;
+}
+
+void *amalloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (posix_memalign(&p, 64, bytes ? bytes : 64)) return nullptr;
+    memset(p, 0, bytes ? bytes : 64);
+    return p;
+}
+
+#define RC(x)                    \
+    do {                         \
+        int rc__ = (x);          \
+        if (rc__) return rc__;   \
+    } while (0)
+
+// ------------------------------------------------------------------ init
+int init_impl(TinySCF_t t, const char *bas_fname, const char *df_bas_fname, const char *xyz_fname, int niters)
+{
+    double st = 0;
+    {
+        struct timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        st = ts.tv_sec + 1e-9 * ts.tv_nsec;
+    }
+    memset(t, 0, sizeof(*t));
+    const char *vb = getenv("TINYSCF_VERBOSE");
+    t->verbose = vb ? atoi(vb) : 1;
+    const char *dv = getenv("TINYSCF_DEVICE");
+    t->device = dv ? atoi(dv) : 0;
+    Engine *e = new Engine();
+    t->dev = e;
+    RC(parse_xyz(xyz_fname, e->mol));
+    RC(parse_gbs(bas_fname, e->bas));
+    RC(parse_gbs(df_bas_fname, e->dfbas));
+    RC(build_shells(e->mol, e->bas, e->sh));
+    RC(build_shells(e->mol, e->dfbas, e->ash));
+    if (e->sh.maxam > MAX_L_ORB || e->ash.maxam > MAX_L_AUX) {
+        fprintf(stderr, "[tinyscf] shells beyond d (orbital) / f (auxiliary) are not supported\n");
+        return ERR_UNSUPPORTED;
+    }
+    const int nbf = e->sh.nbf, naux = e->ash.nbf;
+    t->natoms = e->mol.natoms;
+    t->nshells = e->sh.nsh;
+    t->nbasfuncs = nbf;
+    t->n_occ = (e->mol.nelec - e->mol.Q) / 2;   // CMS_BasisSet.c:788-791
+    t->charge = e->mol.Q;
+    t->electron = e->mol.nelec;
+    t->df_nbf = naux;
+    t->df_nshells = e->ash.nsh;
+    t->nshellpairs = t->nshells * t->nshells;
+    t->mat_size = nbf * nbf;
+    t->num_uniq_sp = (t->nshells + 1) * t->nshells / 2;
+    t->max_dim = ncart(e->sh.maxam);
+    t->niters = niters;
+    t->iter = 0;
+    t->ene_tol = 1e-11;
+    t->shell_scrtol2 = 1e-11 * 1e-11;
+    t->max_diis = MAX_DIIS;
+    t->nuc_energy = e->mol.enuc;
+    if (t->n_occ <= 0 || t->n_occ > nbf) return ERR_INPUT;
+    if (t->verbose) {
+        printf("Job information:\n");
+        printf("    basis set            = %s\n", bas_fname);
+        printf("    DF basis set         = %s\n", df_bas_fname);
+        printf("    molecule             = %s\n", xyz_fname);
+        printf("    # atoms              = %d\n", t->natoms);
+        printf("    # shells             = %d\n", t->nshells);
+        printf("    # basis functions    = %d\n", t->nbasfuncs);
+        printf("    # DF shells          = %d\n", t->df_nshells);
+        printf("    # DF basis functions = %d\n", t->df_nbf);
+        printf("    # occupied orbits    = %d\n", t->n_occ);
+        printf("    # charge             = %d\n", t->charge);
+        printf("    # electrons          = %d\n", t->electron);
+    }
+
+    // host mirrors
+    size_t nn = (size_t) nbf * nbf;
+    t->sp_scrval = (double *) amalloc(sizeof(double) * t->nshellpairs);
+    t->bf_pair_scrval = (double *) amalloc(sizeof(double) * nn);
+    t->df_sp_scrval = (double *) amalloc(sizeof(double) * t->df_nshells);
+    t->uniq_sp_lid = (int *) amalloc(sizeof(int) * t->num_uniq_sp);
+    t->uniq_sp_rid = (int *) amalloc(sizeof(int) * t->num_uniq_sp);
+    t->bf_pair_mask = (int *) amalloc(sizeof(int) * nn);
+    t->bf_pair_j = (int *) amalloc(sizeof(int) * nn);
+    t->bf_pair_diag = (int *) amalloc(sizeof(int) * nbf);
+    t->bf_mask_displs = (int *) amalloc(sizeof(int) * (nbf + 1));
+    t->shell_bf_sind = (int *) amalloc(sizeof(int) * (t->nshells + 1));
+    t->shell_bf_num = (int *) amalloc(sizeof(int) * t->nshells);
+    t->df_shell_bf_sind = (int *) amalloc(sizeof(int) * (t->df_nshells + 1));
+    t->df_shell_bf_num = (int *) amalloc(sizeof(int) * t->df_nshells);
+    for (int i = 0; i <= t->nshells; i++) t->shell_bf_sind[i] = e->sh.bfoff[i];
+    for (int i = 0; i < t->nshells; i++) t->shell_bf_num[i] = ncart(e->sh.am[i]);
+    for (int i = 0; i <= t->df_nshells; i++) t->df_shell_bf_sind[i] = e->ash.bfoff[i];
+    for (int i = 0; i < t->df_nshells; i++) t->df_shell_bf_num[i] = ncart(e->ash.am[i]);
+    double **mats[] = {&t->Hcore_mat, &t->S_mat, &t->F_mat, &t->D_mat, &t->J_mat, &t->K_mat, &t->X_mat, &t->tmp_mat};
+    for (double **m : mats) *m = (double *) amalloc(sizeof(double) * nn);
+    t->Cocc_mat = (double *) amalloc(sizeof(double) * nbf * t->n_occ);
+    t->eigval = (double *) amalloc(sizeof(double) * nbf);
+    t->ev_idx = (int *) amalloc(sizeof(int) * nbf);
+    for (int i = 0; i < nbf; i++) t->ev_idx[i] = i;
+    t->DIIS_bmax = -DBL_MAX;
+
+    // device
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        fprintf(stderr, "[tinyscf] no CUDA device available: the engine has no CPU path\n");
+        return ERR_CUDA;
+    }
+    if (t->device < 0 || t->device >= ndev) t->device = 0;
+    TSCF_CUDA_CHECK(cudaSetDevice(t->device));
+    TSCF_CUDA_CHECK(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
+    for (int k = 0; k < TINYSCF_T_COUNT; k++) {
+        TSCF_CUDA_CHECK(cudaEventCreate(&e->ev0[k]));
+        TSCF_CUDA_CHECK(cudaEventCreate(&e->ev1[k]));
+        e->ev_used[k] = false;
+        e->timers[k] = 0.0;
+    }
+    boys_table_init(e->s);
+    RC(upload_shells(e, e->sh, MAX_L_ORB, e->dsh));
+    RC(upload_shells(e, e->ash, MAX_L_AUX, e->dash));
+    std::vector<double> Z(e->mol.natoms);
+    for (int a = 0; a < e->mol.natoms; a++) Z[a] = e->mol.eid[a] + 1.0;
+    RC(upload(e, &e->Z, Z));
+    RC(upload(e, &e->xyz, e->mol.xyz));
+    e->nn = nn;
+    double **dm[] = {&e->S, &e->H, &e->X, &e->F, &e->Fp, &e->D, &e->J, &e->K, &e->tmp, &e->tmp2, &e->V};
+    for (double **m : dm) {
+        RC(dalloc(e, m, nn));
+        cudaMemsetAsync(*m, 0, sizeof(double) * nn, e->s);
+    }
+    RC(dalloc(e, &e->Cocc, (size_t) nbf * t->n_occ));
+    RC(dalloc(e, &e->w, nbf));
+    RC(dalloc(e, &e->F0, nn * MAX_DIIS));
+    RC(dalloc(e, &e->R, nn * MAX_DIIS));
+    cudaMemsetAsync(e->F0, 0, sizeof(double) * nn * MAX_DIIS, e->s);
+    cudaMemsetAsync(e->R, 0, sizeof(double) * nn * MAX_DIIS, e->s);
+    RC(dalloc(e, &e->diis, 1));
+    diis_init(e->diis, e->s);
+    RC(dalloc(e, &e->sp_scr, (size_t) t->nshellpairs));
+    RC(dalloc(e, &e->bf_scr, nn));
+    RC(dalloc(e, &e->df_scr, (size_t) t->df_nshells));
+    RC(dalloc(e, &e->piv, nbf));
+    RC(dalloc(e, &e->rank, 1));
+    RC(dalloc(e, &e->pwork, 2 * (size_t) nbf));
+    RC(dalloc(e, &e->epart, ENERGY_BLOCKS));
+    RC(dalloc(e, &e->E, 1));
+    e->eig = eig_create(nbf, e->s);
+    if (!e->eig) return ERR_CUDA;
+    RC(sync_rc(e, "init"));
+    t->mem_size = (double) nn * 8 * (13 + 2 * MAX_DIIS);
+    {
+        struct timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        t->init_time = ts.tv_sec + 1e-9 * ts.tv_nsec - st;
+    }
+    return OK;
+}
+
+// ------------------------------------------------------------------ Hcore, S, X (TinySCF.c:20-83)
+int hcore_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e) return ERR_STATE;
+    const int nbf = t->nbasfuncs;
+    tstart(e, TINYSCF_T_HCORE);
+    DevShells v = shells_view(e->dsh, e->sh.nsh);
+    launch_one_electron_grouped(v, e->dsh.ids, e->dsh.am_start.data(), e->mol.natoms, e->Z, e->xyz, e->S, e->H, nbf,
+                                e->s);
+    RC(cuda_rc("one-electron integrals"));
+    RC(eig_run(e->eig, e->S, e->w, e->V, e->s));
+    inv_sqrt_from_eig(e->w, e->V, e->X, e->tmp, nbf, e->s);
+    tstop(e, TINYSCF_T_HCORE);
+    RC(sync_rc(e, "Hcore/S/X"));
+    tcollect(e);
+    t->S_Hcore_time = e->timers[TINYSCF_T_HCORE] * 1e-3;
+    cudaMemcpy(t->S_mat, e->S, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->Hcore_mat, e->H, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->X_mat, e->X, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    if (t->verbose)
+        printf("TinySCF precompute Hcore, S, and X matrices over,  elapsed time = %.3lf (s)\n", t->S_Hcore_time);
+    e->stage = std::max(e->stage, 1);
+    return OK;
+}
+
+// ------------------------------------------------------------------ Schwarz (TinySCF.c:112-226)
+int schwarz_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e) return ERR_STATE;
+    const int nbf = t->nbasfuncs, nsh = t->nshells;
+    tstart(e, TINYSCF_T_SCHWARZ);
+    DevShells v = shells_view(e->dsh, nsh), av = shells_view(e->dash, t->df_nshells);
+    launch_schwarz_grouped(v, e->dsh.ids, e->dsh.am_start.data(), e->sp_scr, e->bf_scr, nbf, e->s);
+    launch_df_scrval(av, e->df_scr, e->s);
+    tstop(e, TINYSCF_T_SCHWARZ);
+    RC(cuda_rc("Schwarz quartets"));
+    RC(sync_rc(e, "Schwarz"));
+    tcollect(e);
+    cudaMemcpy(t->sp_scrval, e->sp_scr, sizeof(double) * nsh * nsh, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->bf_pair_scrval, e->bf_scr, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->df_sp_scrval, e->df_scr, sizeof(double) * t->df_nshells, cudaMemcpyDeviceToHost);
+    double mx = 0.0, dmx = 0.0;
+    for (int i = 0; i < nsh * nsh; i++) mx = std::max(mx, t->sp_scrval[i]);
+    for (int i = 0; i < t->df_nshells; i++) dmx = std::max(dmx, t->df_sp_scrval[i]);
+    t->max_scrval = mx;
+    t->max_df_scrval = dmx;
+    const double eta = t->shell_scrtol2 / t->max_df_scrval;
+    std::vector<std::pair<int, int>> pairs;
+    for (int M = 0; M < nsh; M++)
+        for (int N = M; N < nsh; N++)
+            if (t->sp_scrval[M * nsh + N] > eta) {
+                int mn = e->sh.am[M] * 5 + e->sh.am[N], nm = e->sh.am[N] * 5 + e->sh.am[M];   // CMS_Simint.c:308-312
+                pairs.push_back(mn > nm ? std::make_pair(M, N) : std::make_pair(N, M));
+            }
+    std::sort(pairs.begin(), pairs.end());
+    t->num_uniq_sp = (int) pairs.size();
+    for (size_t k = 0; k < pairs.size(); k++) {
+        t->uniq_sp_lid[k] = pairs[k].first;
+        t->uniq_sp_rid[k] = pairs[k].second;
+    }
+    t->shell_scr_time = e->timers[TINYSCF_T_SCHWARZ] * 1e-3;
+    if (t->verbose)
+        printf("TinySCF precompute shell screening info over,      elapsed time = %.3lf (s)\n", t->shell_scr_time);
+    e->stage = std::max(e->stage, 2);
+    return OK;
+}
+
+// ------------------------------------------------------------------ sparsity (TinySCF.c:228-280)
+int sparsity_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e || e->stage < 2) return ERR_STATE;
+    const int nbf = t->nbasfuncs, naux = t->df_nbf, nocc = t->n_occ;
+    const double eta = t->shell_scrtol2 / t->max_df_scrval;
+    int nnz = 0;
+    t->bf_mask_displs[0] = 0;
+    for (int i = 0; i < nbf; i++) {
+        for (int j = 0; j < nbf; j++) {
+            if (t->bf_pair_scrval[(size_t) i * nbf + j] > eta) {
+                t->bf_pair_mask[(size_t) i * nbf + j] = nnz;
+                t->bf_pair_j[nnz] = j;
+                nnz++;
+            } else {
+                t->bf_pair_mask[(size_t) i * nbf + j] = -1;
+            }
+        }
+        t->bf_pair_diag[i] = t->bf_pair_mask[(size_t) i * nbf + i];
+        t->bf_mask_displs[i + 1] = nnz;
+    }
+    t->num_bf_pair_scr = nnz;
+    e->nnz = nnz;
+    // one DF-tensor row per unordered pair that survives in either order
+    std::vector<int> upair((size_t) nbf * nbf, -1);
+    int nu = 0;
+    for (int i = 0; i < nbf; i++)
+        for (int j = i; j < nbf; j++)
+            if (t->bf_pair_mask[(size_t) i * nbf + j] >= 0 || t->bf_pair_mask[(size_t) j * nbf + i] >= 0) {
+                upair[(size_t) i * nbf + j] = nu;
+                upair[(size_t) j * nbf + i] = nu;
+                nu++;
+            }
+    e->nu = nu;
+    std::vector<int> csr_j(t->bf_pair_j, t->bf_pair_j + nnz), csr_u(nnz), displs(t->bf_mask_displs,
+                                                                               t->bf_mask_displs + nbf + 1);
+    std::vector<int> up_i, up_j, up_u;
+    for (int i = 0; i < nbf; i++)
+        for (int r = displs[i]; r < displs[i + 1]; r++) {
+            int j = csr_j[r];
+            csr_u[r] = upair[(size_t) i * nbf + j];
+            if (j >= i) {
+                up_i.push_back(i);
+                up_j.push_back(j);
+                up_u.push_back(csr_u[r]);
+            }
+        }
+    e->nup = (int) up_i.size();
+    RC(upload(e, &e->csr_j, csr_j));
+    RC(upload(e, &e->csr_u, csr_u));
+    RC(upload(e, &e->csr_displs, displs));
+    RC(upload(e, &e->up_i, up_i));
+    RC(upload(e, &e->up_j, up_j));
+    RC(upload(e, &e->up_u, up_u));
+    RC(upload(e, &e->upair, upair));
+    // 3-centre work list: unique shell pairs grouped by (am(M), am(N)) class
+    std::vector<int2> pl;
+    e->cls_start.clear();
+    e->cls_la.clear();
+    e->cls_lb.clear();
+    for (int la = 0; la <= MAX_L_ORB; la++)
+        for (int lb = 0; lb <= la; lb++) {
+            e->cls_start.push_back((int) pl.size());
+            e->cls_la.push_back(la);
+            e->cls_lb.push_back(lb);
+            for (int k = 0; k < t->num_uniq_sp; k++) {
+                int M = t->uniq_sp_lid[k], N = t->uniq_sp_rid[k];
+                if (e->sh.am[M] == la && e->sh.am[N] == lb) pl.push_back(make_int2(M, N));
+            }
+        }
+    e->cls_start.push_back((int) pl.size());
+    RC(upload(e, &e->pairs3c, pl));
+    // DF tensor, K and J buffers
+    RC(dalloc(e, &e->B, (size_t) nu * naux));
+    RC(dalloc(e, &e->T, (size_t) nbf * nocc * naux));
+    const int nt = (nbf + 63) / 64, ntiles = nt * (nt + 1) / 2;
+    e->ksplit = std::max(1, std::min(64, (4 * 148 + ntiles - 1) / ntiles));
+    RC(dalloc(e, &e->Kpart, (size_t) e->ksplit * nbf * nbf));
+    {
+        std::vector<int2> tl;
+        for (int a = 0; a < nt; a++)
+            for (int b = a; b < nt; b++) tl.push_back(make_int2(a, b));
+        RC(upload(e, &e->tiles, tl));
+    }
+    FockPlan p = e->plan();
+    e->jblk = build_J_part_blocks(p);
+    RC(dalloc(e, &e->Jt, naux));
+    RC(dalloc(e, &e->Jpart, (size_t) e->jblk * naux));
+    RC(dalloc(e, &e->Jw, std::max(1, e->nup)));
+    RC(sync_rc(e, "sparsity"));
+    t->mem_size = (double) nu * naux * 8 + (double) nbf * nocc * naux * 8 + 24.0 * e->nn * 8;
+    if (t->verbose) {
+        printf("TinySCF handling shell pair sparsity over,         elapsed time = %.3lf (s)\n", 0.0);
+        printf("TinySCF memory allocation and initialization over, elapsed time = %.3lf (s)\n", 0.0);
+        printf("TinySCF regular + density fitting memory usage = %.2lf MB \n", t->mem_size / 1048576.0);
+        printf("#### Sparsity of basis function pairs = %lf, %lf\n", (double) t->num_uniq_sp / t->nshellpairs,
+               (double) nnz / t->mat_size);
+    }
+    e->stage = std::max(e->stage, 3);
+    return OK;
+}
+
+// ------------------------------------------------------------------ guess (TinySCF.c:282-364)
+int guess_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e) return ERR_STATE;
+    const int nbf = t->nbasfuncs, nocc = t->n_occ;
+    std::vector<double> D((size_t) nbf * nbf, 0.0);
+    for (int a = 0; a < t->natoms; a++) {
+        int el = e->mol.eid[a];
+        int b0 = e->sh.atom_bf0[a], b1 = e->sh.atom_bf1[a], nf = b1 - b0;
+        std::vector<double> g = load_sad(e->bas, el, nf);
+        for (int i = 0; i < nf; i++)
+            for (int j = 0; j < nf; j++) D[(size_t) (b0 + i) * nbf + b0 + j] = g[(size_t) i * nf + j];
+    }
+    double R = 1.0;
+    if (t->charge != 0 && t->electron != 0) R = (double) (t->electron - t->charge) / (double) t->electron;
+    R *= 0.5;
+    for (auto &v : D) v *= R;
+    tstart(e, TINYSCF_T_GUESS);
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(e->D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, e->s));
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(e->tmp, e->D, sizeof(double) * D.size(), cudaMemcpyDeviceToDevice, e->s));
+    pivoted_cholesky(e->tmp, nbf, 1e-12, e->piv, e->rank, e->pwork, e->s);
+    d2cocc_copy(e->tmp, e->rank, e->Cocc, nbf, nocc, e->s);
+    tstop(e, TINYSCF_T_GUESS);
+    RC(cuda_rc("initial guess"));
+    RC(sync_rc(e, "initial guess"));
+    tcollect(e);
+    memcpy(t->D_mat, D.data(), sizeof(double) * D.size());
+    cudaMemcpy(t->Cocc_mat, e->Cocc, sizeof(double) * nbf * nocc, cudaMemcpyDeviceToHost);
+    if (t->verbose)
+        printf("TinySCF SAD initial guess: D mat / Cocc mat used %lf, %lf (s)\n", 0.0,
+               e->timers[TINYSCF_T_GUESS] * 1e-3);
+    e->stage = std::max(e->stage, 4);
+    return OK;
+}
+
+// ------------------------------------------------------------------ DF tensor (build_DF_tensor.c:256-287)
+int df_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e || e->stage < 3) return ERR_STATE;
+    const int nbf = t->nbasfuncs, naux = t->df_nbf;
+    if (t->verbose) printf("---------- DF tensor construction ----------\n");
+    double *pqA = nullptr, *Jpq = nullptr, *Jw = nullptr, *JV = nullptr, *Jinv = nullptr;
+    RC(dalloc(e, &pqA, (size_t) e->nu * naux));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(pqA, 0, sizeof(double) * (size_t) e->nu * naux, e->s));
+    ThreeCenterPlan pl;
+    pl.pairs = e->pairs3c;
+    pl.npairs = e->cls_start.back();
+    pl.class_start = e->cls_start.data();
+    pl.class_la = e->cls_la.data();
+    pl.class_lb = e->cls_lb.data();
+    pl.nclass = (int) e->cls_la.size();
+    pl.aux_by_am = e->dash.ids;
+    pl.aux_am_start = e->dash.am_start.data();
+    pl.sp_scr = e->sp_scr;
+    pl.df_scr = e->df_scr;
+    pl.scrtol2 = t->shell_scrtol2;
+    pl.upair_index = e->upair;
+    pl.nbf = nbf;
+    pl.naux = naux;
+    DevShells v = shells_view(e->dsh, t->nshells), av = shells_view(e->dash, t->df_nshells);
+    tstart(e, TINYSCF_T_3C);
+    launch_three_center(v, av, pl, pqA, e->s);
+    tstop(e, TINYSCF_T_3C);
+    RC(cuda_rc("3-centre integrals"));
+    RC(dalloc(e, &Jpq, (size_t) naux * naux));
+    RC(dalloc(e, &JV, (size_t) naux * naux));
+    RC(dalloc(e, &Jinv, (size_t) naux * naux));
+    RC(dalloc(e, &Jw, naux));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(Jpq, 0, sizeof(double) * (size_t) naux * naux, e->s));
+    tstart(e, TINYSCF_T_2C);
+    launch_two_center_grouped(av, e->dash.ids, e->dash.am_start.data(), e->df_scr, t->shell_scrtol2, Jpq, naux, e->s);
+    tstop(e, TINYSCF_T_2C);
+    RC(cuda_rc("2-centre integrals"));
+    tstart(e, TINYSCF_T_INVSQRT);
+    Eig *eg = eig_create(naux, e->s);
+    if (!eg) return ERR_CUDA;
+    int erc = eig_run(eg, Jpq, Jw, JV, e->s);
+    inv_sqrt_from_eig(Jw, JV, Jinv, Jpq, naux, e->s);
+    tstop(e, TINYSCF_T_INVSQRT);
+    if (erc) { eig_destroy(eg); return erc; }
+    tstart(e, TINYSCF_T_DFGEMM);
+    dgemm(false, false, e->nu, naux, naux, 1.0, pqA, naux, Jinv, naux, 0.0, e->B, naux, e->s);
+    tstop(e, TINYSCF_T_DFGEMM);
+    RC(cuda_rc("DF tensor GEMM"));
+    int rc = sync_rc(e, "DF tensor");
+    eig_destroy(eg);
+    dfree(e, pqA);
+    dfree(e, Jpq);
+    dfree(e, JV);
+    dfree(e, Jinv);
+    dfree(e, Jw);
+    if (rc) return rc;
+    tcollect(e);
+    if (t->verbose) {
+        printf("* 3-center integral : %.3lf (s)\n", e->timers[TINYSCF_T_3C] * 1e-3);
+        printf("* 2-center integral : %.3lf (s)\n", e->timers[TINYSCF_T_2C] * 1e-3);
+        printf("* matrix inv-sqrt   : %.3lf (s)\n", e->timers[TINYSCF_T_INVSQRT] * 1e-3);
+        printf("* build DF tensor   : %.3lf (s)\n", e->timers[TINYSCF_T_DFGEMM] * 1e-3);
+        printf("---------- DF tensor construction finished ----------\n");
+    }
+    e->stage = std::max(e->stage, 5);
+    return OK;
+}
+
+// ------------------------------------------------------------------ Fock (build_Fock.c:349-396)
+int fock_device(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    FockPlan p = e->plan();
+    p.nocc = t->n_occ;
+    tstart(e, TINYSCF_T_J);
+    build_J(p, e->D, e->J, e->Jt, e->Jpart, e->jblk, e->Jw, e->s);
+    tstop(e, TINYSCF_T_J);
+    tstart(e, TINYSCF_T_K_HT);
+    build_K_halftransform(p, e->Cocc, e->T, e->s);
+    tstop(e, TINYSCF_T_K_HT);
+    tstart(e, TINYSCF_T_K_SYRK);
+    build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->tiles, e->s);
+    tstop(e, TINYSCF_T_K_SYRK);
+    tstart(e, TINYSCF_T_FOCK);
+    build_F_energy(e->H, e->J, e->K, e->D, e->F, e->epart, t->nbasfuncs, e->s);
+    energy_reduce(e->epart, e->E, e->s);
+    tstop(e, TINYSCF_T_FOCK);
+    e->F_is_orth = false;
+    return cuda_rc("Fock build");
+}
+
+int fock_impl(TinySCF_t t, bool to_host)
+{
+    Engine *e = E_(t);
+    if (!e || e->stage < 5) return ERR_STATE;
+    RC(fock_device(t));
+    RC(sync_rc(e, "Fock build"));
+    tcollect(e);
+    if (to_host) {
+        cudaMemcpy(t->J_mat, e->J, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+        cudaMemcpy(t->K_mat, e->K, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+        cudaMemcpy(t->F_mat, e->F, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+        cudaMemcpy(&t->HF_energy, e->E, sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    return OK;
+}
+
+// ------------------------------------------------------------------ DIIS (DIIS.c:12-123)
+int diis_device(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    const int n = t->nbasfuncs;
+    tstart(e, TINYSCF_T_DIIS);
+    if (t->iter <= 1) {
+        xtfx(e->X, e->F, e->Fp, e->tmp, n, e->s);
+    } else {
+        int md = t->max_diis;
+        if (md < 1 || md > MAX_DIIS) md = MAX_DIIS;
+        diis_step(e->diis, md, e->F, e->D, e->S, e->X, e->Fp, e->F0, e->R, e->tmp, e->tmp2, n, e->s);
+    }
+    tstop(e, TINYSCF_T_DIIS);
+    e->F_is_orth = true;
+    return cuda_rc("DIIS");
+}
+
+int diis_impl(TinySCF_t t, bool to_host)
+{
+    Engine *e = E_(t);
+    if (!e || e->stage < 1) return ERR_STATE;
+    RC(diis_device(t));
+    RC(sync_rc(e, "DIIS"));
+    tcollect(e);
+    if (to_host) cudaMemcpy(t->F_mat, e->Fp, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    return OK;
+}
+
+// ------------------------------------------------------------------ density (build_density.c:37-69)
+int density_device(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    const int n = t->nbasfuncs;
+    tstart(e, TINYSCF_T_DENSITY);
+    const double *Fo = e->F_is_orth ? e->Fp : e->F;
+    RC(eig_run(e->eig, Fo, e->w, e->V, e->s));
+    density_from_eig(e->X, e->V, e->Cocc, e->D, n, t->n_occ, e->s);
+    tstop(e, TINYSCF_T_DENSITY);
+    return cuda_rc("density");
+}
+
+int density_impl(TinySCF_t t, bool to_host)
+{
+    Engine *e = E_(t);
+    if (!e || e->stage < 1) return ERR_STATE;
+    RC(density_device(t));
+    RC(sync_rc(e, "density"));
+    tcollect(e);
+    if (to_host) {
+        cudaMemcpy(t->D_mat, e->D, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+        cudaMemcpy(t->Cocc_mat, e->Cocc, sizeof(double) * t->nbasfuncs * t->n_occ, cudaMemcpyDeviceToHost);
+        cudaMemcpy(t->eigval, e->w, sizeof(double) * t->nbasfuncs, cudaMemcpyDeviceToHost);
+    }
+    return OK;
+}
+
+int sync_host_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e) return ERR_STATE;
+    RC(sync_rc(e, "sync"));
+    const int nbf = t->nbasfuncs;
+    cudaMemcpy(t->S_mat, e->S, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->Hcore_mat, e->H, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->X_mat, e->X, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->F_mat, e->F_is_orth ? e->Fp : e->F, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->D_mat, e->D, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->J_mat, e->J, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->K_mat, e->K, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->Cocc_mat, e->Cocc, sizeof(double) * nbf * t->n_occ, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t->eigval, e->w, sizeof(double) * nbf, cudaMemcpyDeviceToHost);
+    DiisState st;
+    cudaMemcpy(&st, e->diis, sizeof(st), cudaMemcpyDeviceToHost);
+    t->DIIS_len = st.len;
+    t->DIIS_bmax_id = st.bmax_id;
+    t->DIIS_bmax = st.bmax;
+    return cuda_rc("sync to host");
+}
+
+// ------------------------------------------------------------------ SCF loop (TinySCF.c:378-435)
+int scf_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e || e->stage < 5) return ERR_STATE;
+    if (t->verbose) {
+        printf("TinySCF SCF iteration started...\n");
+        printf("Nuclear energy = %.10lf\n", t->nuc_energy);
+    }
+    cudaEvent_t scf0, scf1;
+    cudaEventCreate(&scf0);
+    cudaEventCreate(&scf1);
+    cudaEventRecord(scf0, e->s);
+    t->iter = 0;
+    double prev_energy = 0, energy_delta = 223;
+    while ((t->iter < t->niters) && (energy_delta >= t->ene_tol)) {
+        if (t->verbose) printf("--------------- Iteration %d ---------------\n", t->iter);
+        tstart(e, TINYSCF_T_ITER);
+        RC(fock_device(t));
+        RC(diis_device(t));
+        RC(density_device(t));
+        tstop(e, TINYSCF_T_ITER);
+        double E = 0.0;
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(&E, e->E, sizeof(double), cudaMemcpyDeviceToHost, e->s));
+        RC(sync_rc(e, "SCF iteration"));
+        tcollect(e);
+        t->HF_energy = E;
+        energy_delta = fabs(t->HF_energy - prev_energy);
+        prev_energy = t->HF_energy;
+        if (!std::isfinite(E)) {
+            fprintf(stderr, "[tinyscf] SCF energy is not finite at iteration %d\n", t->iter);
+            return ERR_NUMERIC;
+        }
+        if (t->verbose) {
+            const double *tm = e->timers;
+            printf("* Build Fock matrix     : %.3lf (s)\n", (tm[TINYSCF_T_J] + tm[TINYSCF_T_K_HT] + tm[TINYSCF_T_K_SYRK] + tm[TINYSCF_T_FOCK]) * 1e-3);
+            printf("|---- J matrix          |---- %.3lf (s)\n", tm[TINYSCF_T_J] * 1e-3);
+            printf("|---- aux. K tensor     |---- %.3lf (s)\n", tm[TINYSCF_T_K_HT] * 1e-3);
+            printf("|---- K matrix          |---- %.3lf (s)\n", tm[TINYSCF_T_K_SYRK] * 1e-3);
+            printf("* DIIS procedure        : %.3lf (s)\n", tm[TINYSCF_T_DIIS] * 1e-3);
+            printf("* Build density matrix  : %.3lf (s)\n", tm[TINYSCF_T_DENSITY] * 1e-3);
+            printf("* Iteration runtime     = %.3lf (s)\n", tm[TINYSCF_T_ITER] * 1e-3);
+            printf("* Energy = %.10lf (%.10lf)", t->HF_energy + t->nuc_energy, t->HF_energy);
+            if (t->iter > 0) printf(", delta = %e\n", energy_delta);
+            else printf("\n");
+        }
+        if (t->iter == 0) energy_delta = 223;
+        t->iter++;
+    }
+    cudaEventRecord(scf1, e->s);
+    cudaEventSynchronize(scf1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, scf0, scf1);
+    e->timers[TINYSCF_T_SCF] = ms;
+    cudaEventDestroy(scf0);
+    cudaEventDestroy(scf1);
+    if (t->verbose) printf("--------------- SCF iterations finished ---------------\n");
+    return sync_host_impl(t);
+}
+
+void free_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (e) {
+        if (e->s) cudaStreamSynchronize(e->s);
+        eig_destroy(e->eig);
+        for (void *p : e->allocs) cudaFree(p);
+        e->allocs.clear();
+        if (e->s) {
+            for (int k = 0; k < TINYSCF_T_COUNT; k++) {
+                cudaEventDestroy(e->ev0[k]);
+                cudaEventDestroy(e->ev1[k]);
+            }
+            cudaStreamDestroy(e->s);
+        }
+        delete e;
+        t->dev = nullptr;
+    }
+    void *hp[] = {t->sp_scrval, t->bf_pair_scrval, t->df_sp_scrval, t->uniq_sp_lid, t->uniq_sp_rid, t->bf_pair_mask,
+                  t->bf_pair_j, t->bf_pair_diag, t->bf_mask_displs, t->shell_bf_sind, t->shell_bf_num,
+                  t->df_shell_bf_sind, t->df_shell_bf_num, t->Hcore_mat, t->S_mat, t->F_mat, t->D_mat, t->J_mat,
+                  t->K_mat, t->X_mat, t->tmp_mat, t->Cocc_mat, t->eigval, t->ev_idx};
+    for (void *p : hp) free(p);
+}
+
+void die(const char *fn, int rc)
+{
+    fprintf(stderr, "[tinyscf] %s failed: %s\n", fn, TinySCF_status_string(rc));
+    abort();
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+TinySCF_t TinySCF_alloc(void)
+{
+    return (TinySCF_t) calloc(1, sizeof(struct TinySCF_struct));
+}
+
+size_t TinySCF_struct_size(void) { return sizeof(struct TinySCF_struct); }
+
+const char *TinySCF_status_string(int status)
+{
+    switch (status) {
+    case TINYSCF_OK: return "success";
+    case TINYSCF_ERR_CUDA: return "CUDA error";
+    case TINYSCF_ERR_FILEIO: return "cannot open input file";
+    case TINYSCF_ERR_INPUT: return "invalid input";
+    case TINYSCF_ERR_UNSUPPORTED: return "unsupported input";
+    case TINYSCF_ERR_ALLOC: return "device allocation failed";
+    case TINYSCF_ERR_NUMERIC: return "numerical failure";
+    case TINYSCF_ERR_STATE: return "call out of order";
+    default: return "unknown status";
+    }
+}
+
+#define STATUS_WRAP(name, call)            \
+    int name(TinySCF_t t)                  \
+    {                                      \
+        if (!t) return TINYSCF_ERR_STATE;  \
+        int rc = (call);                   \
+        t->status = rc;                    \
+        return rc;                         \
+    }
+
+int TinySCF_init_status(TinySCF_t t, const char *bas, const char *dfbas, const char *xyz, int niters)
+{
+    if (!t) return TINYSCF_ERR_STATE;
+    int rc = init_impl(t, bas, dfbas, xyz, niters);
+    t->status = rc;
+    return rc;
+}
+STATUS_WRAP(TinySCF_compute_Hcore_Ovlp_mat_status, hcore_impl(t))
+STATUS_WRAP(TinySCF_compute_sq_Schwarz_scrvals_status, schwarz_impl(t))
+STATUS_WRAP(TinySCF_prepare_sparsity_status, sparsity_impl(t))
+STATUS_WRAP(TinySCF_get_initial_guess_status, guess_impl(t))
+STATUS_WRAP(TinySCF_build_DF_tensor_status, df_impl(t))
+STATUS_WRAP(TinySCF_build_FockMat_status, fock_impl(t, true))
+STATUS_WRAP(TinySCF_DIIS_status, diis_impl(t, true))
+STATUS_WRAP(TinySCF_build_DenMat_status, density_impl(t, true))
+STATUS_WRAP(TinySCF_do_SCF_status, scf_impl(t))
+
+int TinySCF_free_status(TinySCF_t t)
+{
+    if (!t) return TINYSCF_ERR_STATE;
+    free_impl(t);
+    free(t);
+    return TINYSCF_OK;
+}
+
+int TinySCF_set_density(TinySCF_t t, const double *D, const double *Cocc)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (D && cudaMemcpy(e->D, D, sizeof(double) * e->nn, cudaMemcpyHostToDevice) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    if (Cocc && cudaMemcpy(e->Cocc, Cocc, sizeof(double) * t->nbasfuncs * t->n_occ, cudaMemcpyHostToDevice) != cudaSuccess)
+        return TINYSCF_ERR_CUDA;
+    if (D) memcpy(t->D_mat, D, sizeof(double) * e->nn);
+    if (Cocc) memcpy(t->Cocc_mat, Cocc, sizeof(double) * t->nbasfuncs * t->n_occ);
+    return TINYSCF_OK;
+}
+
+int TinySCF_set_fock(TinySCF_t t, const double *F, int orthogonal)
+{
+    if (!t || !t->dev || !F) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (cudaMemcpy(orthogonal ? e->Fp : e->F, F, sizeof(double) * e->nn, cudaMemcpyHostToDevice) != cudaSuccess)
+        return TINYSCF_ERR_CUDA;
+    e->F_is_orth = orthogonal != 0;
+    memcpy(t->F_mat, F, sizeof(double) * e->nn);
+    return TINYSCF_OK;
+}
+
+int TinySCF_sync_host(TinySCF_t t)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    return sync_host_impl(t);
+}
+
+int TinySCF_get_df_tensor(TinySCF_t t, double *out)
+{
+    if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (e->stage < 5) return TINYSCF_ERR_STATE;
+    const int naux = t->df_nbf;
+    // one row per ordered CSR entry, gathered from the unique-pair tensor
+    std::vector<int> cu(e->nnz);
+    cudaMemcpy(cu.data(), e->csr_u, sizeof(int) * e->nnz, cudaMemcpyDeviceToHost);
+    for (int k = 0; k < e->nnz; k++)
+        if (cudaMemcpy(out + (size_t) k * naux, e->B + (size_t) cu[k] * naux, sizeof(double) * naux,
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            return TINYSCF_ERR_CUDA;
+    return TINYSCF_OK;
+}
+
+int TinySCF_get_timings(TinySCF_t t, double *ms, int n)
+{
+    if (!t || !t->dev || !ms) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    for (int k = 0; k < n && k < TINYSCF_T_COUNT; k++) ms[k] = e->timers[k];
+    return TINYSCF_OK;
+}
+
+// ---- the reference's void API (abort on failure, like its asserts)
+void init_TinySCF(TinySCF_t t, char *bas, char *dfbas, char *xyz, const int niters)
+{
+    int rc = TinySCF_init_status(t, bas, dfbas, xyz, niters);
+    if (rc) die("init_TinySCF", rc);
+}
+void free_TinySCF(TinySCF_t t) { TinySCF_free_status(t); }
+void TinySCF_init_batch_dgemm_arrays(TinySCF_t t) { (void) t; }
+void TinySCF_free_batch_dgemm_arrays(TinySCF_t t) { (void) t; }
+void TinySCF_compute_Hcore_Ovlp_mat(TinySCF_t t)
+{
+    int rc = TinySCF_compute_Hcore_Ovlp_mat_status(t);
+    if (rc) die("TinySCF_compute_Hcore_Ovlp_mat", rc);
+}
+void TinySCF_compute_sq_Schwarz_scrvals(TinySCF_t t)
+{
+    int rc = TinySCF_compute_sq_Schwarz_scrvals_status(t);
+    if (rc) die("TinySCF_compute_sq_Schwarz_scrvals", rc);
+}
+void TinySCF_prepare_sparsity(TinySCF_t t)
+{
+    int rc = TinySCF_prepare_sparsity_status(t);
+    if (rc) die("TinySCF_prepare_sparsity", rc);
+}
+void TinySCF_get_initial_guess(TinySCF_t t)
+{
+    int rc = TinySCF_get_initial_guess_status(t);
+    if (rc) die("TinySCF_get_initial_guess", rc);
+}
+void TinySCF_build_DF_tensor(TinySCF_t t)
+{
+    int rc = TinySCF_build_DF_tensor_status(t);
+    if (rc) die("TinySCF_build_DF_tensor", rc);
+}
+void TinySCF_build_FockMat(TinySCF_t t)
+{
+    int rc = TinySCF_build_FockMat_status(t);
+    if (rc) die("TinySCF_build_FockMat", rc);
+}
+void TinySCF_DIIS(TinySCF_t t)
+{
+    int rc = TinySCF_DIIS_status(t);
+    if (rc) die("TinySCF_DIIS", rc);
+}
+void TinySCF_build_DenMat(TinySCF_t t)
+{
+    int rc = TinySCF_build_DenMat_status(t);
+    if (rc) die("TinySCF_build_DenMat", rc);
+}
+void TinySCF_do_SCF(TinySCF_t t)
+{
+    int rc = TinySCF_do_SCF_status(t);
+    if (rc) die("TinySCF_do_SCF", rc);
+}
+
+// build_density.c:12-35, the reference's host helper, behaviour kept as is.
+void quickSort_eigval(double *eigval, int *ev_idx, int l, int r)
+{
+    int i = l, j = r;
+    double mid = eigval[(i + j) / 2], dswap;
+    while (i <= j) {
+        while (eigval[i] < mid) i++;
+        while (eigval[j] > mid) j--;
+        if (i <= j) {
+            ev_idx[i] = ev_idx[j];
+            ev_idx[j] = ev_idx[i];
+            dswap = eigval[i];
+            eigval[i] = eigval[j];
+            eigval[j] = dswap;
+            i++;
+            j--;
+        }
+    }
+    if (i < r) quickSort_eigval(eigval, ev_idx, i, r);
+    if (j > l) quickSort_eigval(eigval, ev_idx, l, j);
+}
+
+}  // extern "C"

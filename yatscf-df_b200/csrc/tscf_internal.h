@@ -1,0 +1,175 @@
+// Internal declarations shared by the host driver (tinyscf.cpp) and the CUDA
+// modules. Nothing here is part of the public C ABI (include/*.h).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tscf {
+
+// ---------------------------------------------------------------- limits
+constexpr int MAX_L_ORB = 2;           // orbital shells up to d
+constexpr int MAX_L_AUX = 3;           // auxiliary shells up to f
+constexpr int MAXDIIS  = 10;          // TinySCF.h:8
+constexpr int BOYS_MMAX = 8;           // highest F_m needed: (dd|dd) Schwarz quartets
+constexpr int BOYS_TAYLOR = 7;         // Taylor terms of the tabulated Boys function
+constexpr double BOYS_DT = 0.05;       // grid spacing in T
+constexpr double BOYS_TMAX = 60.0;     // beyond: asymptotic form
+constexpr int BOYS_NGRID = 1201;       // BOYS_TMAX / BOYS_DT + 1
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int ncum(int l) { return l < 0 ? 0 : (l + 1) * (l + 2) * (l + 3) / 6; }
+
+// Status codes returned by the *_status entry points (0 = success).
+enum Status : int {
+    OK = 0,
+    ERR_CUDA = 1,
+    ERR_FILEIO = 2,
+    ERR_INPUT = 3,
+    ERR_UNSUPPORTED = 4,
+    ERR_ALLOC = 5,
+    ERR_NUMERIC = 6,
+    ERR_STATE = 7,
+};
+
+// Device view of a shell table (structure of arrays, all device pointers).
+struct DevShells {
+    int nsh;
+    const int *am;        // [nsh]
+    const int *nprim;     // [nsh]
+    const int *poff;      // [nsh] offset into alpha/coef
+    const int *bfoff;     // [nsh+1] first basis function of each shell
+    const double *cen;    // [3*nsh] Bohr
+    const double *alpha;  // [total prims]
+    const double *coef;   // [total prims], normalised (x^l component unit norm)
+};
+
+// ---------------------------------------------------------------- integrals (ints.cu)
+void boys_table_init(cudaStream_t s);   // uploads the Boys table once per process/device
+
+// Shell ids grouped by angular momentum: d_ids (device) lists the shells of
+// AM 0, then 1, ...; h_start (host) holds the group boundaries [maxL+2].
+
+// S and Hcore = T + V for all shell pairs; S, H row-major nbf x nbf.
+void launch_one_electron_grouped(const DevShells &sh, const int *d_ids, const int *h_start, int natoms,
+                                 const double *d_Z, const double *d_xyz, double *d_S, double *d_H, int nbf,
+                                 cudaStream_t s);
+
+// Schwarz screening values for every ordered shell pair (M,N):
+// bf_scr[(bfM+iM)*nbf + bfN+iN] = |(mn|mn)| read with the reference's index
+// (TinySCF.c:153), sp_scr[M*nsh+N] = max over the block.
+void launch_schwarz_grouped(const DevShells &sh, const int *d_ids, const int *h_start, double *d_sp_scr,
+                            double *d_bf_scr, int nbf, cudaStream_t s);
+
+// max_p (p|p) for each aux shell.
+void launch_df_scrval(const DevShells &aux, double *d_out, cudaStream_t s);
+
+// 3-centre integrals (mn|P) for the listed shell pairs into the unique-pair
+// tensor pqA_u[u][P] (u from upair_index[iM*nbf+iN], -1 = absent).
+struct ThreeCenterPlan {
+    const int2 *pairs;        // [npairs] shell pair (M,N), grouped by AM class
+    int npairs;
+    const int *class_start;   // host: [nclass+1] pair ranges of each (la,lb) class
+    const int *class_la, *class_lb;
+    int nclass;
+    const int *aux_by_am;     // device: aux shell ids grouped by AM
+    const int *aux_am_start;  // host: [MAX_L_AUX+2]
+    const double *sp_scr;     // device: [nsh*nsh]
+    const double *df_scr;     // device: [naux_sh]
+    double scrtol2;
+    const int *upair_index;   // device: [nbf*nbf]
+    int nbf, naux;
+};
+void launch_three_center(const DevShells &sh, const DevShells &aux, const ThreeCenterPlan &plan,
+                         double *d_pqA_u, cudaStream_t s);
+
+// (P|Q) for aux shell pairs with df_scr[P]*df_scr[Q] >= scrtol2, mirrored; Jpq row-major naux x naux.
+void launch_two_center_grouped(const DevShells &aux, const int *d_ids, const int *h_start, const double *d_df_scr,
+                               double scrtol2, double *d_Jpq, int naux, cudaStream_t s);
+
+// ---------------------------------------------------------------- dense FP64 (linalg.cu)
+// C = alpha * op(A) * op(B) + beta * C, row-major, op = transpose if ta/tb.
+void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
+           const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s);
+
+// Symmetric eigen-decomposition (ascending eigenvalues). A is row-major n x n
+// symmetric; on return V holds eigenvectors as ROWS (V[k*n + i] = i-th entry of
+// eigenvector k). Workspace is owned by the Eig object.
+struct Eig;
+Eig *eig_create(int n, cudaStream_t s);
+void eig_destroy(Eig *e);
+int  eig_run(Eig *e, const double *d_A, double *d_w, double *d_V, cudaStream_t s);
+
+// X = U diag(f(w)) U^T with f(w) = w^-1/2, U from eigenvectors in rows.
+void inv_sqrt_from_eig(const double *d_w, const double *d_V, double *d_X, double *d_tmp, int n, cudaStream_t s);
+
+// LAPACK dpstf2 semantics (unblocked pivoted Cholesky, lower, first-max pivot),
+// applied to a row-major symmetric matrix in place; rank to *d_rank.
+void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s);
+// TinySCF_D2Cocc's copy of the factor into Cocc (TinySCF.c:297-319).
+void d2cocc_copy(const double *d_chol, const int *d_rank, double *d_Cocc, int nbf, int nocc, cudaStream_t s);
+
+// Elementwise helpers.
+void fill(double *d, double v, size_t n, cudaStream_t s);
+void scale_copy(const double *src, double *dst, double a, size_t n, cudaStream_t s);
+
+// ---------------------------------------------------------------- Fock build (fock.cu)
+struct FockPlan {
+    int nbf, naux, nocc;
+    int nnz;                  // ordered screened pairs (reference CSR)
+    int nup;                  // ordered pairs (i, j>=i) used by J
+    const int *csr_j;         // [nnz] column j of each CSR entry
+    const int *csr_displs;    // [nbf+1]
+    const int *csr_u;         // [nnz] unique-pair row of each CSR entry
+    const int *up_i, *up_j;   // [nup] upper CSR entries (i <= j)
+    const int *up_u;          // [nup] their unique-pair rows
+    const double *B;          // DF tensor, [nu][naux] unique pairs
+};
+// J = symmetrised Coulomb matrix from D (build_Fock.c:37-130).
+// d_t (naux) and d_part (scratch, nblk*naux) are caller buffers.
+void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, double *d_part, int part_blocks,
+             double *d_w, cudaStream_t s);
+int  build_J_part_blocks(const FockPlan &p);
+// K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
+void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s);
+// ... then K = T T^T over upper 64x64 tiles (d_tiles: (bi,bj), bi <= bj), split-K, mirrored.
+void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_Kpart, int ksplit,
+                  const int2 *d_tiles, cudaStream_t s);
+size_t build_K_part_elems(const FockPlan &p, int ksplit);
+// F = H + 2J - K and e_part[b] = partial sums of D .* (F + H) (TinySCF.c:367-376).
+void build_F_energy(const double *d_H, const double *d_J, const double *d_K, const double *d_D,
+                    double *d_F, double *d_epart, int n, cudaStream_t s);
+constexpr int ENERGY_BLOCKS = 296;
+// ---------------------------------------------------------------- DIIS / density (scf.cu)
+struct DiisState {            // device-resident DIIS bookkeeping (DIIS.c:12-123)
+    int len;
+    int bmax_id;
+    int idx;
+    int pad;
+    double bmax;
+    double B[(MAXDIIS + 1) * (MAXDIIS + 1)];
+    double coef[MAXDIIS + 1];
+    double dots[MAXDIIS];
+};
+void diis_init(DiisState *d_st, cudaStream_t s);
+void diis_step(DiisState *d_st, int max_diis, const double *d_F, const double *d_D, const double *d_S,
+               const double *d_X, double *d_Fout, double *d_F0, double *d_R, double *d_tmp, double *d_tmp2,
+               int n, cudaStream_t s);
+void xtfx(const double *d_X, const double *d_F, double *d_out, double *d_tmp, int n, cudaStream_t s);
+void energy_reduce(const double *d_epart, double *d_E, cudaStream_t s);
+// Cocc = X * V[0:nocc]^T (eigenvectors in rows), D = Cocc Cocc^T.
+void density_from_eig(const double *d_X, const double *d_V, double *d_Cocc, double *d_D, int n, int nocc,
+                      cudaStream_t s);
+
+}  // namespace tscf
+
+#define TSCF_CUDA_CHECK(x)                                                            \
+    do {                                                                              \
+        cudaError_t e__ = (x);                                                        \
+        if (e__ != cudaSuccess) {                                                     \
+            fprintf(stderr, "[tinyscf] CUDA error %s at %s:%d: %s\n", #x, __FILE__,   \
+                    __LINE__, cudaGetErrorString(e__));                               \
+            return tscf::ERR_CUDA;                                                    \
+        }                                                                             \
+    } while (0)

@@ -1,0 +1,248 @@
+"""Python binding of the B200 TinySCF engine (libtinyscf_b200.so) via ctypes.
+
+Mirrors the reference's TinySCF C API (huanghua1994/YATSCF-DF, TinySCF.h:107-138,
+build_DF_tensor.h:6, build_Fock.h:6, build_density.h:6-8, DIIS.h:6) one call per
+function, in main.c's order, plus the engine's status-returning extensions
+(include/tinyscf_b200.h). Every call goes through the C ABI; there is no Python
+or CPU fallback: if the shared library or a CUDA device is missing, the calls
+raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libtinyscf_b200.so")
+
+MAX_DIIS = 10
+TIMERS = ["HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM", "J", "K_HT", "K_SYRK",
+          "FOCK", "DIIS", "DENSITY", "ITER", "SCF"]
+STATUS = {0: "success", 1: "CUDA error", 2: "cannot open input file", 3: "invalid input",
+          4: "unsupported input", 5: "device allocation failed", 6: "numerical failure",
+          7: "call out of order"}
+
+
+class TinySCFStruct(ctypes.Structure):
+    """struct TinySCF_struct of include/TinySCF.h, field for field."""
+    _fields_ = [
+        ("basis", ctypes.c_void_p), ("df_basis", ctypes.c_void_p),
+        ("natoms", ctypes.c_int), ("nshells", ctypes.c_int),
+        ("nbasfuncs", ctypes.c_int), ("n_occ", ctypes.c_int),
+        ("charge", ctypes.c_int), ("electron", ctypes.c_int),
+        ("df_nbf", ctypes.c_int), ("df_nshells", ctypes.c_int),
+        ("nshellpairs", ctypes.c_int), ("num_uniq_sp", ctypes.c_int),
+        ("mat_size", ctypes.c_int), ("max_dim", ctypes.c_int),
+        ("niters", ctypes.c_int), ("iter", ctypes.c_int),
+        ("nuc_energy", ctypes.c_double), ("HF_energy", ctypes.c_double), ("ene_tol", ctypes.c_double),
+        ("shell_scrtol2", ctypes.c_double), ("max_scrval", ctypes.c_double), ("max_df_scrval", ctypes.c_double),
+        ("sp_scrval", ctypes.POINTER(ctypes.c_double)), ("bf_pair_scrval", ctypes.POINTER(ctypes.c_double)),
+        ("uniq_sp_lid", ctypes.POINTER(ctypes.c_int)), ("uniq_sp_rid", ctypes.POINTER(ctypes.c_int)),
+        ("df_sp_scrval", ctypes.POINTER(ctypes.c_double)),
+        ("bf_pair_mask", ctypes.POINTER(ctypes.c_int)), ("bf_pair_j", ctypes.POINTER(ctypes.c_int)),
+        ("bf_pair_diag", ctypes.POINTER(ctypes.c_int)), ("bf_mask_displs", ctypes.POINTER(ctypes.c_int)),
+        ("num_bf_pair_scr", ctypes.c_int),
+        ("shell_bf_sind", ctypes.POINTER(ctypes.c_int)), ("shell_bf_num", ctypes.POINTER(ctypes.c_int)),
+        ("df_shell_bf_sind", ctypes.POINTER(ctypes.c_int)), ("df_shell_bf_num", ctypes.POINTER(ctypes.c_int)),
+        ("Hcore_mat", ctypes.POINTER(ctypes.c_double)), ("S_mat", ctypes.POINTER(ctypes.c_double)),
+        ("F_mat", ctypes.POINTER(ctypes.c_double)), ("D_mat", ctypes.POINTER(ctypes.c_double)),
+        ("J_mat", ctypes.POINTER(ctypes.c_double)), ("K_mat", ctypes.POINTER(ctypes.c_double)),
+        ("X_mat", ctypes.POINTER(ctypes.c_double)),
+        ("Cocc_mat", ctypes.POINTER(ctypes.c_double)), ("eigval", ctypes.POINTER(ctypes.c_double)),
+        ("ev_idx", ctypes.POINTER(ctypes.c_int)), ("tmp_mat", ctypes.POINTER(ctypes.c_double)),
+        ("DIIS_len", ctypes.c_int), ("DIIS_bmax_id", ctypes.c_int), ("DIIS_bmax", ctypes.c_double),
+        ("max_diis", ctypes.c_int),
+        ("mem_size", ctypes.c_double), ("init_time", ctypes.c_double),
+        ("S_Hcore_time", ctypes.c_double), ("shell_scr_time", ctypes.c_double),
+        ("status", ctypes.c_int), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
+        ("dev", ctypes.c_void_p),
+    ]
+
+
+TinySCF_t = ctypes.POINTER(TinySCFStruct)
+_lib = None
+
+
+def load_library(path=LIBPATH):
+    """Load libtinyscf_b200.so and declare every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libtinyscf_b200.so is not built (%s); run __graft_entry__.build()" % path)
+    lib = ctypes.CDLL(path)
+    T = TinySCF_t
+    cp, dp, ip = ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
+    sig = {
+        "TinySCF_alloc": ([], T),
+        "TinySCF_status_string": ([ip], ctypes.c_char_p),
+        "TinySCF_struct_size": ([], ctypes.c_size_t),
+        "TinySCF_init_status": ([T, cp, cp, cp, ip], ip),
+        "TinySCF_compute_Hcore_Ovlp_mat_status": ([T], ip),
+        "TinySCF_compute_sq_Schwarz_scrvals_status": ([T], ip),
+        "TinySCF_prepare_sparsity_status": ([T], ip),
+        "TinySCF_get_initial_guess_status": ([T], ip),
+        "TinySCF_build_DF_tensor_status": ([T], ip),
+        "TinySCF_build_FockMat_status": ([T], ip),
+        "TinySCF_DIIS_status": ([T], ip),
+        "TinySCF_build_DenMat_status": ([T], ip),
+        "TinySCF_do_SCF_status": ([T], ip),
+        "TinySCF_free_status": ([T], ip),
+        "TinySCF_set_density": ([T, dp, dp], ip),
+        "TinySCF_set_fock": ([T, dp, ip], ip),
+        "TinySCF_sync_host": ([T], ip),
+        "TinySCF_get_df_tensor": ([T, dp], ip),
+        "TinySCF_get_timings": ([T, dp, ip], ip),
+        "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+class TinySCFError(RuntimeError):
+    pass
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class TinySCF:
+    """One engine instance (one molecule) on one GPU."""
+
+    def __init__(self, bas_fname, df_bas_fname, xyz_fname, niters=30, verbose=0, max_diis=MAX_DIIS, device=None):
+        self.lib = load_library()
+        self.t = self.lib.TinySCF_alloc()
+        old = os.environ.get("TINYSCF_VERBOSE")
+        olddev = os.environ.get("TINYSCF_DEVICE")
+        os.environ["TINYSCF_VERBOSE"] = str(int(verbose))
+        if device is not None:
+            os.environ["TINYSCF_DEVICE"] = str(int(device))
+        try:
+            rc = self.lib.TinySCF_init_status(self.t, bas_fname.encode(), df_bas_fname.encode(),
+                                              xyz_fname.encode(), int(niters))
+        finally:
+            for k, v in (("TINYSCF_VERBOSE", old), ("TINYSCF_DEVICE", olddev)):
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        if rc:
+            self.lib.TinySCF_free_status(self.t)
+            self.t = None
+            raise TinySCFError("init_TinySCF: " + STATUS.get(rc, str(rc)))
+        self.s.max_diis = int(max_diis)
+
+    @property
+    def s(self):
+        return self.t.contents
+
+    def _call(self, name):
+        rc = getattr(self.lib, name + "_status")(self.t)
+        if rc:
+            raise TinySCFError("%s: %s" % (name, STATUS.get(rc, str(rc))))
+
+    # --- the reference's API, main.c:28-46 order
+    def compute_Hcore_Ovlp_mat(self):
+        self._call("TinySCF_compute_Hcore_Ovlp_mat")
+
+    def compute_sq_Schwarz_scrvals(self):
+        self._call("TinySCF_compute_sq_Schwarz_scrvals")
+
+    def prepare_sparsity(self):
+        self._call("TinySCF_prepare_sparsity")
+
+    def get_initial_guess(self):
+        self._call("TinySCF_get_initial_guess")
+
+    def build_DF_tensor(self):
+        self._call("TinySCF_build_DF_tensor")
+
+    def build_FockMat(self):
+        self._call("TinySCF_build_FockMat")
+
+    def DIIS(self):
+        self._call("TinySCF_DIIS")
+
+    def build_DenMat(self):
+        self._call("TinySCF_build_DenMat")
+
+    def do_SCF(self):
+        self._call("TinySCF_do_SCF")
+
+    def setup(self):
+        self.compute_Hcore_Ovlp_mat()
+        self.compute_sq_Schwarz_scrvals()
+        self.prepare_sparsity()
+        self.get_initial_guess()
+        self.build_DF_tensor()
+
+    # --- extensions
+    def set_density(self, D, Cocc=None):
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        C = None if Cocc is None else np.ascontiguousarray(Cocc, dtype=np.float64)
+        rc = self.lib.TinySCF_set_density(self.t, _dptr(D), None if C is None else _dptr(C))
+        if rc:
+            raise TinySCFError("set_density: " + STATUS.get(rc, str(rc)))
+
+    def set_fock(self, F, orthogonal=False):
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        rc = self.lib.TinySCF_set_fock(self.t, _dptr(F), int(bool(orthogonal)))
+        if rc:
+            raise TinySCFError("set_fock: " + STATUS.get(rc, str(rc)))
+
+    def sync_host(self):
+        rc = self.lib.TinySCF_sync_host(self.t)
+        if rc:
+            raise TinySCFError("sync_host: " + STATUS.get(rc, str(rc)))
+
+    def df_tensor(self):
+        out = np.empty((self.s.num_bf_pair_scr, self.s.df_nbf))
+        rc = self.lib.TinySCF_get_df_tensor(self.t, _dptr(out))
+        if rc:
+            raise TinySCFError("get_df_tensor: " + STATUS.get(rc, str(rc)))
+        return out
+
+    def timings(self):
+        ms = np.zeros(len(TIMERS))
+        self.lib.TinySCF_get_timings(self.t, _dptr(ms), len(TIMERS))
+        return dict(zip(TIMERS, ms))
+
+    # --- host mirrors as numpy copies
+    def _mat(self, name, shape):
+        p = getattr(self.s, name)
+        n = int(np.prod(shape))
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(shape).copy()
+
+    def mat(self, name):
+        n = self.s.nbasfuncs
+        if name == "Cocc_mat":
+            return self._mat(name, (n, self.s.n_occ))
+        if name == "eigval":
+            return self._mat(name, (n,))
+        return self._mat(name, (n, n))
+
+    def csr(self):
+        n = self.s.nbasfuncs
+        nnz = self.s.num_bf_pair_scr
+        return (self._mat("bf_pair_mask", (n, n)), self._mat("bf_pair_j", (nnz,)),
+                self._mat("bf_mask_displs", (n + 1,)))
+
+    @property
+    def energy(self):
+        return self.s.HF_energy + self.s.nuc_energy
+
+    def free(self):
+        if self.t is not None:
+            self.lib.TinySCF_free_status(self.t)
+            self.t = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
