@@ -1,0 +1,292 @@
+"""Benchmark of the DF-RHF hot path on B200: SCF time-to-converge.
+
+One step = one SCF solve of the workload molecule from the SAD guess to
+|dE| < 1e-8 Eh (J, K, F, energy, DIIS, density every iteration), with the
+integrals and the DF tensor resident in HBM (built once, untimed, reported
+separately). Timed on the device with CUDA events recorded by the engine on
+its own stream; max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c40h82] [--impl ours|reference]
+
+N > 1 runs independent replicas (one molecule per GPU, no data-path
+collective; torchrun, one process per GPU). --impl reference times the
+reference's own CPU code (oracle/_ref/ref_bench, compiled from the reference's
+sources) on this machine's host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "yatscf-df_b200")
+DATA = os.path.join(REPO, "tests", "golden", "data")
+BAS = os.path.join(DATA, "cc-pvdz", "cc-pvdz.gbs")
+DFBAS = os.path.join(DATA, "cc-pVDZ-RI", "cc-pVDZ-RI.gbs")
+REF_BENCH = os.path.join(REPO, "oracle", "_ref", "ref_bench")
+
+CONFIGS = {
+    "water": "H2O (O at origin, H at (0,+/-0.757,0.587) A)",
+    "c10h22": "C10H22 all-trans alkane, C-C 1.54 A, C-H 1.09 A",
+    "c20h42": "C20H42 all-trans alkane, C-C 1.54 A, C-H 1.09 A",
+    "c40h82": "C40H82 all-trans alkane, C-C 1.54 A, C-H 1.09 A",
+}
+METRIC = "SCF time-to-converge at 1e-8 Eh"
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(config, ene_tol, nsolves, threads):
+    """Run the reference's CPU code; returns (setup_s, [(iters, energy, seconds)])."""
+    if not os.path.exists(REF_BENCH):
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
+    out = subprocess.run([REF_BENCH, BAS, DFBAS, os.path.join(DATA, config + ".xyz"), "100", repr(ene_tol),
+                          str(nsolves)], capture_output=True, text=True, env=env)
+    if out.returncode != 0:
+        raise RuntimeError("ref_bench failed: " + out.stderr[-500:])
+    setup, solves = None, []
+    for line in out.stderr.splitlines():
+        tok = line.split()
+        if tok[:1] == ["SETUP"]:
+            setup = float(tok[1])
+        elif tok[:1] == ["SOLVE"]:
+            solves.append((int(tok[2]), float(tok[3]), float(tok[4])))
+    return setup, solves
+
+
+def k_flops(nbf, nocc, naux, nnz):
+    """Algorithmic K work: 2 nocc naux nnz (half-transform) + nbf(nbf+1) nocc naux (upper-triangle T T^T)."""
+    return 2.0 * nocc * naux * nnz, 1.0 * nbf * (nbf + 1) * nocc * naux
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    res = cpu_reference(args.config, args.ene_tol, args.warmup + args.steps, threads)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built"}))
+        return
+    setup, solves = res
+    timed = solves[args.warmup:]
+    t = statistics.mean(s[2] for s in timed)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": t, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config + ": " + CONFIGS[args.config] + ", cc-pVDZ / cc-pVDZ-RI (Cartesian)",
+                   "ene_tol": args.ene_tol, "iterations": timed[-1][0], "energy": timed[-1][1],
+                   "setup_s": setup, "parallelism": "replicas"},
+        "cpu_baseline": {"value": t, "unit": "s", "cores": threads, "kind": "reference",
+                         "sample": "%d full SCF solves of %s (reference C sources, OpenMP + OpenBLAS)"
+                                   % (args.steps, args.config)},
+        "e2e": {"value": setup + t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank):
+    sys.path.insert(0, PKG)
+    import tinyscf                                  # the engine's library first (CUDA libraries)
+    tinyscf.load_library()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local_rank)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist = dist_mod
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(v):
+        if dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    xyz = os.path.join(DATA, args.config + ".xyz")
+    t0 = time.perf_counter()
+    e = tinyscf.TinySCF(BAS, DFBAS, xyz, 100, device=local_rank)
+    e.setup()
+    setup_s = time.perf_counter() - t0
+    st = e.timings()
+    e.s.ene_tol = args.ene_tol
+    for _ in range(args.warmup):
+        e.reset_scf()
+        e.do_SCF()
+    e.reset_timing_stats()
+    launches0 = e.counters()[0]
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    times, iters, energies = [], [], []
+    for _ in range(args.steps):
+        e.reset_scf()                               # untimed: the device timer wraps do_SCF only
+        e.do_SCF()
+        times.append(e.timings()["SCF"])
+        iters.append(e.s.iter)
+        energies.append(e.energy)
+    barrier()
+    clk = clocks.stop()
+    launches = e.counters()[0] - launches0
+    stats = e.timing_stats()
+    ms_local = sum(times) / len(times)
+    ms = allmax(ms_local)
+    nbf, nocc, naux, nnz = e.s.nbasfuncs, e.s.n_occ, e.s.df_nbf, e.s.num_bf_pair_scr
+    e.free()
+
+    # end to end through the C ABI from files: parse, integrals, DF tensor, SCF,
+    # host mirrors of the results (S, H, X, F, D, J, K, Cocc) copied back.
+    e2e_times, h2d, d2h = [], 0, 0
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        e2 = tinyscf.TinySCF(BAS, DFBAS, xyz, 100, device=local_rank)
+        e2.setup()
+        e2.s.ene_tol = args.ene_tol
+        e2.do_SCF()
+        _ = e2.energy
+        c = e2.counters()
+        e2.free()
+        e2e_times.append(time.perf_counter() - t0)
+        h2d, d2h = c[1], c[2]
+    e2e = allmax(statistics.mean(e2e_times))
+
+    hbm, bf16, peak_kind = peaks()
+    fht, fsy = k_flops(nbf, nocc, naux, nnz)
+    ht_ms = stats["K_HT"][0] / max(1, stats["K_HT"][1])
+    sy_ms = stats["K_SYRK"][0] / max(1, stats["K_SYRK"][1])
+    dom = ("k_halftransform", fht, ht_ms) if ht_ms >= sy_ms else ("k_syrk_part", fsy, sy_ms)
+    achieved = dom[1] / (dom[2] * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(args.config, {}).get(dom[0])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        res = cpu_reference(args.config, args.ene_tol, 1, threads)
+        if res is not None:
+            setup_cpu, solves = res
+            cpu = {"value": solves[0][2], "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": "one full SCF solve of %s to 1e-8 Eh (reference C sources, OpenMP + OpenBLAS; "
+                             "its setup of %.1f s excluded)" % (args.config, setup_cpu)}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config + ": " + CONFIGS[args.config] + ", cc-pVDZ / cc-pVDZ-RI (Cartesian, "
+                                   "nbf %d, naux %d, n_occ %d, screened pairs %d)" % (nbf, naux, nocc, nnz),
+                       "ene_tol": args.ene_tol, "iterations": iters[-1], "energy": energies[-1],
+                       "precision": "plain FP64", "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (DF tensor resident in HBM)",
+                       "setup_s": setup_s, "setup_ms": {k: round(st[k], 3) for k in
+                                                        ("HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM")},
+                       "per_iteration_ms": {k: round(stats[k][0] / max(1, stats[k][1]), 4) for k in
+                                            ("J", "K_HT", "K_SYRK", "FOCK", "DIIS", "DENSITY", "ITER")}},
+            "roofline": {"bound": "tensor", "kernel": dom[0], "achieved": achieved, "peak": bf16,
+                         "unit": "TFLOP/s", "frac": achieved / bf16, "traffic": traffic,
+                         "peak_kind": peak_kind + " bf16 dense", "note": "K computed in FP64 on the CUDA cores"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "k_tflops": (fht + fsy) / ((ht_ms + sy_ms) * 1e-3) / 1e12,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c40h82")
+    ap.add_argument("--ene-tol", type=float, default=1e-8)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

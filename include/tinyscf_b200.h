@@ -75,8 +75,18 @@ TINYSCF_API int TinySCF_sync_host(TinySCF_t t);
 /* Copy the DF tensor in the reference's layout: rows in bf_pair CSR order
  * (nnz rows), df_nbf columns. out must hold num_bf_pair_scr * df_nbf doubles. */
 TINYSCF_API int TinySCF_get_df_tensor(TinySCF_t t, double *out);
-/* Timers: writes min(n, TINYSCF_T_COUNT) values in milliseconds. */
+/* Timers: writes min(n, TINYSCF_T_COUNT) values in milliseconds (last call). */
 TINYSCF_API int TinySCF_get_timings(TinySCF_t t, double *ms, int n);
+/* Accumulated timers since the last reset: total milliseconds and number of
+ * timed calls per phase (per SCF iteration for the per-iteration phases). */
+TINYSCF_API int TinySCF_get_timing_stats(TinySCF_t t, double *sum_ms, long long *count, int n);
+TINYSCF_API int TinySCF_reset_timing_stats(TinySCF_t t);
+/* Counters: [0] engine kernels launched by this process, [1] bytes copied
+ * host->device, [2] bytes copied device->host by this engine instance. */
+TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
+/* Back to the state right after TinySCF_get_initial_guess (SAD density, its
+ * factor, empty DIIS history), keeping integrals and the DF tensor. */
+TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,7 @@ int build_J_part_blocks(const FockPlan &p)
 void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, double *d_part, int nblk, double *d_w,
              cudaStream_t s)
 {
+    g_launches += 4;
     k_j_weights<<<(p.nup + 255) / 256, 256, 0, s>>>(p.up_i, p.up_j, d_D, d_w, p.nup, p.nbf);
     int rows_per_blk = (p.nup + nblk - 1) / nblk;
     k_j_tpart<<<nblk, JT_THREADS, 0, s>>>(p.B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
@@ -229,6 +230,7 @@ size_t build_K_part_elems(const FockPlan &p, int ksplit) { return (size_t) kspli
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s)
 {
     dim3 g1((p.naux + KT_N - 1) / KT_N, (p.nocc + KT_M - 1) / KT_M, p.nbf);
+    g_launches++;
     k_halftransform<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
 }
 
@@ -241,6 +243,7 @@ void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_K
     long long qchunk = (Q + ksplit - 1) / ksplit;
     qchunk = (qchunk + KT_K - 1) / KT_K * KT_K;
     dim3 g2(ntiles, ksplit);
+    g_launches += 2;
     k_syrk_part<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
     size_t nn = (size_t) p.nbf * p.nbf;
     k_syrk_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(d_Kpart, ksplit, p.nbf, d_K);
@@ -271,6 +274,7 @@ __global__ void k_fock_energy(const double *H, const double *J, const double *K,
 void build_F_energy(const double *d_H, const double *d_J, const double *d_K, const double *d_D, double *d_F,
                     double *d_epart, int n, cudaStream_t s)
 {
+    g_launches++;
     k_fock_energy<<<ENERGY_BLOCKS, 256, 0, s>>>(d_H, d_J, d_K, d_D, d_F, d_epart, (size_t) n * n);
 }
 

@@ -11,6 +11,8 @@
 
 namespace tscf {
 
+long long g_launches = 0;
+
 // ------------------------------------------------------------------ DGEMM
 // 64x64 output tile per 256-thread block, 4x4 outputs per thread, K step 16.
 // op(A) is m x k, op(B) is k x n, everything row-major.
@@ -77,6 +79,7 @@ void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
 {
     if (m <= 0 || n <= 0) return;
     dim3 grid((n + GB_N - 1) / GB_N, (m + GB_M - 1) / GB_M);
+    g_launches++;
     if (!ta && !tb) k_dgemm<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     else if (!ta && tb) k_dgemm<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     else if (ta && !tb) k_dgemm<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
@@ -146,6 +149,7 @@ __global__ void k_scale_rows_invsqrt(const double *w, const double *V, double *o
 void inv_sqrt_from_eig(const double *d_w, const double *d_V, double *d_X, double *d_tmp, int n, cudaStream_t s)
 {
     size_t nn = (size_t) n * n;
+    g_launches++;
     k_scale_rows_invsqrt<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(d_w, d_V, d_tmp, n);
     // X = V^T diag(w^-1/2) V
     dgemm(true, false, n, n, n, 1.0, d_V, n, d_tmp, n, 0.0, d_X, n, s);
@@ -274,6 +278,7 @@ __global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, in
 
 void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s)
 {
+    g_launches++;
     k_pstf2<<<1, 1024, 0, s>>>(d_A, n, tol, d_piv, d_rank, d_work);
 }
 
@@ -292,6 +297,7 @@ __global__ void k_d2cocc(const double *chol, const int *rank_p, double *C, int n
 void d2cocc_copy(const double *d_chol, const int *d_rank, double *d_Cocc, int nbf, int nocc, cudaStream_t s)
 {
     size_t n = (size_t) nbf * nocc;
+    g_launches++;
     k_d2cocc<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(d_chol, d_rank, d_Cocc, nbf, nocc);
 }
 
@@ -303,6 +309,7 @@ __global__ void k_fill(double *d, double v, size_t n)
 }
 void fill(double *d, double v, size_t n, cudaStream_t s)
 {
+    if (n) g_launches++;
     if (n) k_fill<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(d, v, n);
 }
 __global__ void k_scale_copy(const double *a, double *b, double f, size_t n)
@@ -312,6 +319,7 @@ __global__ void k_scale_copy(const double *a, double *b, double f, size_t n)
 }
 void scale_copy(const double *src, double *dst, double a, size_t n, cudaStream_t s)
 {
+    if (n) g_launches++;
     if (n) k_scale_copy<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(src, dst, a, n);
 }
 

@@ -259,6 +259,9 @@ struct Engine {
     cudaEvent_t ev0[TINYSCF_T_COUNT], ev1[TINYSCF_T_COUNT];
     bool ev_used[TINYSCF_T_COUNT];
     double timers[TINYSCF_T_COUNT];
+    double tsum[TINYSCF_T_COUNT];
+    long long tcnt[TINYSCF_T_COUNT];
+    long long h2d = 0, d2h = 0;       // bytes moved by explicit host<->device copies
     DevArrays dsh, dash;
     double *Z = nullptr, *xyz = nullptr;
     size_t nn = 0;
@@ -330,11 +333,18 @@ void dfree(Engine *e, void *p)
     if (it != e->allocs.end()) e->allocs.erase(it);
 }
 
+void d2h(Engine *e, void *dst, const void *src, size_t bytes)
+{
+    cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    e->d2h += (long long) bytes;
+}
+
 template <typename T>
 int upload(Engine *e, T **p, const std::vector<T> &v)
 {
     int rc = dalloc(e, p, v.size());
     if (rc) return rc;
+    e->h2d += (long long) (sizeof(T) * v.size());
     if (!v.empty() && cudaMemcpyAsync(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, e->s) != cudaSuccess)
         return ERR_CUDA;
     return OK;
@@ -354,7 +364,11 @@ void tcollect(Engine *e)
     for (int k = 0; k < TINYSCF_T_COUNT; k++)
         if (e->ev_used[k]) {
             float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, e->ev0[k], e->ev1[k]) == cudaSuccess) e->timers[k] = ms;
+            if (cudaEventElapsedTime(&ms, e->ev0[k], e->ev1[k]) == cudaSuccess) {
+                e->timers[k] = ms;
+                e->tsum[k] += ms;
+                e->tcnt[k]++;
+            }
             e->ev_used[k] = false;
         }
 }
@@ -521,6 +535,8 @@ int init_impl(TinySCF_t t, const char *bas_fname, const char *df_bas_fname, cons
         TSCF_CUDA_CHECK(cudaEventCreate(&e->ev1[k]));
         e->ev_used[k] = false;
         e->timers[k] = 0.0;
+        e->tsum[k] = 0.0;
+        e->tcnt[k] = 0;
     }
     boys_table_init(e->s);
     RC(upload_shells(e, e->sh, MAX_L_ORB, e->dsh));
@@ -580,9 +596,9 @@ int hcore_impl(TinySCF_t t)
     RC(sync_rc(e, "Hcore/S/X"));
     tcollect(e);
     t->S_Hcore_time = e->timers[TINYSCF_T_HCORE] * 1e-3;
-    cudaMemcpy(t->S_mat, e->S, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->Hcore_mat, e->H, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->X_mat, e->X, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    d2h(e, t->S_mat, e->S, sizeof(double) * e->nn);
+    d2h(e, t->Hcore_mat, e->H, sizeof(double) * e->nn);
+    d2h(e, t->X_mat, e->X, sizeof(double) * e->nn);
     if (t->verbose)
         printf("TinySCF precompute Hcore, S, and X matrices over,  elapsed time = %.3lf (s)\n", t->S_Hcore_time);
     e->stage = std::max(e->stage, 1);
@@ -603,9 +619,9 @@ int schwarz_impl(TinySCF_t t)
     RC(cuda_rc("Schwarz quartets"));
     RC(sync_rc(e, "Schwarz"));
     tcollect(e);
-    cudaMemcpy(t->sp_scrval, e->sp_scr, sizeof(double) * nsh * nsh, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->bf_pair_scrval, e->bf_scr, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->df_sp_scrval, e->df_scr, sizeof(double) * t->df_nshells, cudaMemcpyDeviceToHost);
+    d2h(e, t->sp_scrval, e->sp_scr, sizeof(double) * nsh * nsh);
+    d2h(e, t->bf_pair_scrval, e->bf_scr, sizeof(double) * e->nn);
+    d2h(e, t->df_sp_scrval, e->df_scr, sizeof(double) * t->df_nshells);
     double mx = 0.0, dmx = 0.0;
     for (int i = 0; i < nsh * nsh; i++) mx = std::max(mx, t->sp_scrval[i]);
     for (int i = 0; i < t->df_nshells; i++) dmx = std::max(dmx, t->df_sp_scrval[i]);
@@ -755,6 +771,7 @@ int guess_impl(TinySCF_t t)
     for (auto &v : D) v *= R;
     tstart(e, TINYSCF_T_GUESS);
     TSCF_CUDA_CHECK(cudaMemcpyAsync(e->D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, e->s));
+    e->h2d += (long long) (sizeof(double) * D.size());
     TSCF_CUDA_CHECK(cudaMemcpyAsync(e->tmp, e->D, sizeof(double) * D.size(), cudaMemcpyDeviceToDevice, e->s));
     pivoted_cholesky(e->tmp, nbf, 1e-12, e->piv, e->rank, e->pwork, e->s);
     d2cocc_copy(e->tmp, e->rank, e->Cocc, nbf, nocc, e->s);
@@ -763,7 +780,7 @@ int guess_impl(TinySCF_t t)
     RC(sync_rc(e, "initial guess"));
     tcollect(e);
     memcpy(t->D_mat, D.data(), sizeof(double) * D.size());
-    cudaMemcpy(t->Cocc_mat, e->Cocc, sizeof(double) * nbf * nocc, cudaMemcpyDeviceToHost);
+    d2h(e, t->Cocc_mat, e->Cocc, sizeof(double) * nbf * nocc);
     if (t->verbose)
         printf("TinySCF SAD initial guess: D mat / Cocc mat used %lf, %lf (s)\n", 0.0,
                e->timers[TINYSCF_T_GUESS] * 1e-3);
@@ -872,10 +889,10 @@ int fock_impl(TinySCF_t t, bool to_host)
     RC(sync_rc(e, "Fock build"));
     tcollect(e);
     if (to_host) {
-        cudaMemcpy(t->J_mat, e->J, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-        cudaMemcpy(t->K_mat, e->K, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-        cudaMemcpy(t->F_mat, e->F, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-        cudaMemcpy(&t->HF_energy, e->E, sizeof(double), cudaMemcpyDeviceToHost);
+        d2h(e, t->J_mat, e->J, sizeof(double) * e->nn);
+        d2h(e, t->K_mat, e->K, sizeof(double) * e->nn);
+        d2h(e, t->F_mat, e->F, sizeof(double) * e->nn);
+        d2h(e, &t->HF_energy, e->E, sizeof(double));
     }
     return OK;
 }
@@ -905,7 +922,7 @@ int diis_impl(TinySCF_t t, bool to_host)
     RC(diis_device(t));
     RC(sync_rc(e, "DIIS"));
     tcollect(e);
-    if (to_host) cudaMemcpy(t->F_mat, e->Fp, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
+    if (to_host) d2h(e, t->F_mat, e->Fp, sizeof(double) * e->nn);
     return OK;
 }
 
@@ -930,9 +947,9 @@ int density_impl(TinySCF_t t, bool to_host)
     RC(sync_rc(e, "density"));
     tcollect(e);
     if (to_host) {
-        cudaMemcpy(t->D_mat, e->D, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-        cudaMemcpy(t->Cocc_mat, e->Cocc, sizeof(double) * t->nbasfuncs * t->n_occ, cudaMemcpyDeviceToHost);
-        cudaMemcpy(t->eigval, e->w, sizeof(double) * t->nbasfuncs, cudaMemcpyDeviceToHost);
+        d2h(e, t->D_mat, e->D, sizeof(double) * e->nn);
+        d2h(e, t->Cocc_mat, e->Cocc, sizeof(double) * t->nbasfuncs * t->n_occ);
+        d2h(e, t->eigval, e->w, sizeof(double) * t->nbasfuncs);
     }
     return OK;
 }
@@ -943,17 +960,17 @@ int sync_host_impl(TinySCF_t t)
     if (!e) return ERR_STATE;
     RC(sync_rc(e, "sync"));
     const int nbf = t->nbasfuncs;
-    cudaMemcpy(t->S_mat, e->S, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->Hcore_mat, e->H, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->X_mat, e->X, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->F_mat, e->F_is_orth ? e->Fp : e->F, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->D_mat, e->D, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->J_mat, e->J, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->K_mat, e->K, sizeof(double) * e->nn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->Cocc_mat, e->Cocc, sizeof(double) * nbf * t->n_occ, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t->eigval, e->w, sizeof(double) * nbf, cudaMemcpyDeviceToHost);
+    d2h(e, t->S_mat, e->S, sizeof(double) * e->nn);
+    d2h(e, t->Hcore_mat, e->H, sizeof(double) * e->nn);
+    d2h(e, t->X_mat, e->X, sizeof(double) * e->nn);
+    d2h(e, t->F_mat, e->F_is_orth ? e->Fp : e->F, sizeof(double) * e->nn);
+    d2h(e, t->D_mat, e->D, sizeof(double) * e->nn);
+    d2h(e, t->J_mat, e->J, sizeof(double) * e->nn);
+    d2h(e, t->K_mat, e->K, sizeof(double) * e->nn);
+    d2h(e, t->Cocc_mat, e->Cocc, sizeof(double) * nbf * t->n_occ);
+    d2h(e, t->eigval, e->w, sizeof(double) * nbf);
     DiisState st;
-    cudaMemcpy(&st, e->diis, sizeof(st), cudaMemcpyDeviceToHost);
+    d2h(e, &st, e->diis, sizeof(st));
     t->DIIS_len = st.len;
     t->DIIS_bmax_id = st.bmax_id;
     t->DIIS_bmax = st.bmax;
@@ -984,6 +1001,7 @@ int scf_impl(TinySCF_t t)
         tstop(e, TINYSCF_T_ITER);
         double E = 0.0;
         TSCF_CUDA_CHECK(cudaMemcpyAsync(&E, e->E, sizeof(double), cudaMemcpyDeviceToHost, e->s));
+        e->d2h += (long long) sizeof(double);
         RC(sync_rc(e, "SCF iteration"));
         tcollect(e);
         t->HF_energy = E;
@@ -1149,11 +1167,62 @@ int TinySCF_get_df_tensor(TinySCF_t t, double *out)
     const int naux = t->df_nbf;
     // one row per ordered CSR entry, gathered from the unique-pair tensor
     std::vector<int> cu(e->nnz);
-    cudaMemcpy(cu.data(), e->csr_u, sizeof(int) * e->nnz, cudaMemcpyDeviceToHost);
+    d2h(e, cu.data(), e->csr_u, sizeof(int) * e->nnz);
     for (int k = 0; k < e->nnz; k++)
         if (cudaMemcpy(out + (size_t) k * naux, e->B + (size_t) cu[k] * naux, sizeof(double) * naux,
                        cudaMemcpyDeviceToHost) != cudaSuccess)
             return TINYSCF_ERR_CUDA;
+    return TINYSCF_OK;
+}
+
+int TinySCF_reset_scf(TinySCF_t t)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (e->stage < 4) return TINYSCF_ERR_STATE;
+    int verbose = t->verbose;
+    t->verbose = 0;
+    int rc = guess_impl(t);
+    t->verbose = verbose;
+    if (rc) return rc;
+    diis_init(e->diis, e->s);
+    cudaMemsetAsync(e->F0, 0, sizeof(double) * e->nn * MAX_DIIS, e->s);
+    cudaMemsetAsync(e->R, 0, sizeof(double) * e->nn * MAX_DIIS, e->s);
+    t->iter = 0;
+    t->DIIS_len = 0;
+    t->DIIS_bmax_id = 0;
+    t->DIIS_bmax = -DBL_MAX;
+    return sync_rc(e, "reset");
+}
+
+int TinySCF_get_timing_stats(TinySCF_t t, double *sum_ms, long long *count, int n)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    for (int k = 0; k < n && k < TINYSCF_T_COUNT; k++) {
+        if (sum_ms) sum_ms[k] = e->tsum[k];
+        if (count) count[k] = e->tcnt[k];
+    }
+    return TINYSCF_OK;
+}
+
+int TinySCF_reset_timing_stats(TinySCF_t t)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    for (int k = 0; k < TINYSCF_T_COUNT; k++) {
+        e->tsum[k] = 0.0;
+        e->tcnt[k] = 0;
+    }
+    return TINYSCF_OK;
+}
+
+int TinySCF_get_counters(TinySCF_t t, long long *out, int n)
+{
+    if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    long long v[3] = {g_launches, e->h2d, e->d2h};
+    for (int k = 0; k < n && k < 3; k++) out[k] = v[k];
     return TINYSCF_OK;
 }
 

@@ -8,6 +8,10 @@
 
 namespace tscf {
 
+// Number of engine kernels launched by this process (host-side count, read by
+// the benchmark; library kernels such as cuSOLVER's are not included).
+extern long long g_launches;
+
 // ---------------------------------------------------------------- limits
 constexpr int MAX_L_ORB = 2;           // orbital shells up to d
 constexpr int MAX_L_AUX = 3;           // auxiliary shells up to f

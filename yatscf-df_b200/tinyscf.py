@@ -93,6 +93,10 @@ def load_library(path=LIBPATH):
         "TinySCF_sync_host": ([T], ip),
         "TinySCF_get_df_tensor": ([T, dp], ip),
         "TinySCF_get_timings": ([T, dp, ip], ip),
+        "TinySCF_get_timing_stats": ([T, dp, ctypes.POINTER(ctypes.c_longlong), ip], ip),
+        "TinySCF_reset_timing_stats": ([T], ip),
+        "TinySCF_get_counters": ([T, ctypes.POINTER(ctypes.c_longlong), ip], ip),
+        "TinySCF_reset_scf": ([T], ip),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -206,6 +210,27 @@ class TinySCF:
         if rc:
             raise TinySCFError("get_df_tensor: " + STATUS.get(rc, str(rc)))
         return out
+
+    def reset_scf(self):
+        rc = self.lib.TinySCF_reset_scf(self.t)
+        if rc:
+            raise TinySCFError("reset_scf: " + STATUS.get(rc, str(rc)))
+
+    def timing_stats(self):
+        """{phase: (total ms, number of timed calls)} since the last reset_timing_stats()."""
+        ms = np.zeros(len(TIMERS))
+        cnt = (ctypes.c_longlong * len(TIMERS))()
+        self.lib.TinySCF_get_timing_stats(self.t, _dptr(ms), cnt, len(TIMERS))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(TIMERS)}
+
+    def reset_timing_stats(self):
+        self.lib.TinySCF_reset_timing_stats(self.t)
+
+    def counters(self):
+        """(engine kernel launches in this process, bytes host->device, bytes device->host)."""
+        out = (ctypes.c_longlong * 3)()
+        self.lib.TinySCF_get_counters(self.t, out, 3)
+        return tuple(int(v) for v in out)
 
     def timings(self):
         ms = np.zeros(len(TIMERS))
