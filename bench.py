@@ -6,7 +6,7 @@ integrals and the DF tensor resident in HBM (built once, untimed, reported
 separately). Timed on the device with CUDA events recorded by the engine on
 its own stream; max over ranks.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c40h82] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c20h42] [--impl ours|reference]
 
 N > 1 runs independent replicas (one molecule per GPU, no data-path
 collective; torchrun, one process per GPU). --impl reference times the
@@ -217,7 +217,7 @@ def run_ours(args, rank, world, local_rank):
         e2.free()
         e2e_times.append(time.perf_counter() - t0)
         h2d, d2h = c[1], c[2]
-    e2e = allmax(statistics.mean(e2e_times))
+    e2e = allmax(statistics.mean(e2e_times)) if e2e_times else None
 
     hbm, bf16, peak_kind = peaks()
     fht, fsy = k_flops(nbf, nocc, naux, nnz)
@@ -258,7 +258,8 @@ def run_ours(args, rank, world, local_rank):
                          "unit": "TFLOP/s", "frac": achieved / bf16, "traffic": traffic,
                          "peak_kind": peak_kind + " bf16 dense", "note": "K computed in FP64 on the CUDA cores"},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": ({"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+                    if e2e is not None else None),
             "gpu_launches": launches,
             "clocks": clk,
             "k_tflops": (fht + fsy) / ((ht_ms + sy_ms) * 1e-3) / 1e12,
@@ -274,7 +275,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="c40h82")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c20h42")
     ap.add_argument("--ene-tol", type=float, default=1e-8)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
