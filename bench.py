@@ -4,7 +4,10 @@ One step = one SCF solve of the workload molecule from the SAD guess to
 |dE| < 1e-8 Eh (J, K, F, energy, DIIS, density every iteration), with the
 integrals and the DF tensor resident in HBM (built once, untimed, reported
 separately). Timed on the device with CUDA events recorded by the engine on
-its own stream; max over ranks.
+its own stream; max over ranks. The headline value is the mixed-precision
+form (tensor-core incremental K, final FP64 Fock build); the plain FP64 form
+is timed in the same run and reported beside it (--precision fp64 makes it
+the headline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config c20h42] [--impl ours|reference]
 
@@ -179,27 +182,36 @@ def run_ours(args, rank, world, local_rank):
     setup_s = time.perf_counter() - t0
     st = e.timings()
     e.s.ene_tol = args.ene_tol
-    for _ in range(args.warmup):
-        e.reset_scf()
-        e.do_SCF()
-    e.reset_timing_stats()
-    launches0 = e.counters()[0]
-    clocks = ClockSampler(local_rank)
-    barrier()
-    clocks.start()
-    times, iters, energies = [], [], []
-    for _ in range(args.steps):
-        e.reset_scf()                               # untimed: the device timer wraps do_SCF only
-        e.do_SCF()
-        times.append(e.timings()["SCF"])
-        iters.append(e.s.iter)
-        energies.append(e.energy)
-    barrier()
-    clk = clocks.stop()
-    launches = e.counters()[0] - launches0
-    stats = e.timing_stats()
-    ms_local = sum(times) / len(times)
-    ms = allmax(ms_local)
+
+    def timed_solves(mode, steps, warmup, sample_clocks):
+        e.set_k_precision(mode)
+        for _ in range(warmup):
+            e.reset_scf()
+            e.do_SCF()
+        e.reset_timing_stats()
+        launches0 = e.counters()[0]
+        clocks = ClockSampler(local_rank) if sample_clocks else None
+        barrier()
+        if clocks:
+            clocks.start()
+        times, iters, energies = [], [], []
+        for _ in range(steps):
+            e.reset_scf()                           # untimed: the device timer wraps do_SCF only
+            e.do_SCF()
+            times.append(e.timings()["SCF"])
+            iters.append(e.s.iter)
+            energies.append(e.energy)
+        barrier()
+        clk = clocks.stop() if clocks else None
+        return dict(ms=sum(times) / len(times), iters=iters[-1], energy=energies[-1], clk=clk,
+                    launches=e.counters()[0] - launches0, stats=e.timing_stats())
+
+    plain = timed_solves(tinyscf.K_FP64, args.steps if args.precision == "fp64" else max(1, args.steps // 2),
+                         args.warmup if args.precision == "fp64" else 1, args.precision == "fp64")
+    fast = plain if args.precision == "fp64" else timed_solves(tinyscf.K_MIXED, args.steps, args.warmup, True)
+    ms = allmax(fast["ms"])
+    ms_plain = allmax(plain["ms"])
+    stats, clk, launches = fast["stats"], fast["clk"], fast["launches"]
     nbf, nocc, naux, nnz = e.s.nbasfuncs, e.s.n_occ, e.s.df_nbf, e.s.num_bf_pair_scr
     e.free()
 
@@ -211,6 +223,8 @@ def run_ours(args, rank, world, local_rank):
         e2 = tinyscf.TinySCF(BAS, DFBAS, xyz, 100, device=local_rank)
         e2.setup()
         e2.s.ene_tol = args.ene_tol
+        if args.precision == "mixed":
+            e2.set_k_precision(tinyscf.K_MIXED)
         e2.do_SCF()
         _ = e2.energy
         c = e2.counters()
@@ -221,15 +235,26 @@ def run_ours(args, rank, world, local_rank):
 
     hbm, bf16, peak_kind = peaks()
     fht, fsy = k_flops(nbf, nocc, naux, nnz)
-    ht_ms = stats["K_HT"][0] / max(1, stats["K_HT"][1])
-    sy_ms = stats["K_SYRK"][0] / max(1, stats["K_SYRK"][1])
-    dom = ("k_halftransform", fht, ht_ms) if ht_ms >= sy_ms else ("k_syrk_part", fsy, sy_ms)
-    achieved = dom[1] / (dom[2] * 1e-3) / 1e12
+    if args.precision == "fp64":
+        ht_ms = stats["K_HT"][0] / max(1, stats["K_HT"][1])
+        sy_ms = stats["K_SYRK"][0] / max(1, stats["K_SYRK"][1])
+        dom = ("k_halftransform", fht, ht_ms) if ht_ms >= sy_ms else ("k_syrk_part", fsy, sy_ms)
+        achieved = dom[1] / (dom[2] * 1e-3) / 1e12
+        k_ms = ht_ms + sy_ms
+        note = "K computed in FP64 on the CUDA cores"
+    else:
+        # incremental K per iteration: half-transform (2 nocc naux nnz) + dT S^T (2 nbf^2 nocc naux)
+        k_ms = stats["K_MIXED"][0] / max(1, stats["K_MIXED"][1])
+        fk = fht + 2.0 * nbf * nbf * nocc * naux
+        dom = ("k_gemm+k_half (tcgen05 split-BF16)", fk, k_ms)
+        achieved = fk / (k_ms * 1e-3) / 1e12
+        note = ("algorithmic FP64-equivalent flops of the incremental K (half-transform + dT S^T) over the "
+                "device time of the whole mixed K step; the tensor cores execute 3-4 BF16 products per flop")
     traffic = None
     tp = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get(args.config, {}).get(dom[0])
+            traffic = json.load(f).get(args.config, {}).get(dom[0].split()[0])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -244,25 +269,32 @@ def run_ours(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x2-split/f32/f64",
+            "data": "synthetic",
             "config": {"workload": args.config + ": " + CONFIGS[args.config] + ", cc-pVDZ / cc-pVDZ-RI (Cartesian, "
                                    "nbf %d, naux %d, n_occ %d, screened pairs %d)" % (nbf, naux, nocc, nnz),
-                       "ene_tol": args.ene_tol, "iterations": iters[-1], "energy": energies[-1],
-                       "precision": "plain FP64", "parallelism": "replicas" if world > 1 else "single GPU",
+                       "ene_tol": args.ene_tol, "iterations": fast["iters"], "energy": fast["energy"],
+                       "precision": ("plain FP64" if args.precision == "fp64" else
+                                     "mixed: incremental split-BF16 tcgen05 K, FP64 J/DIIS/density, final FP64 Fock build"),
+                       "plain_fp64": {"s": ms_plain * 1e-3, "iterations": plain["iters"], "energy": plain["energy"]},
+                       "speedup_vs_plain_fp64": ms_plain / ms,
+                       "energy_diff_vs_plain_fp64": fast["energy"] - plain["energy"],
+                       "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (DF tensor resident in HBM)",
                        "setup_s": setup_s, "setup_ms": {k: round(st[k], 3) for k in
                                                         ("HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM")},
                        "per_iteration_ms": {k: round(stats[k][0] / max(1, stats[k][1]), 4) for k in
-                                            ("J", "K_HT", "K_SYRK", "FOCK", "DIIS", "DENSITY", "ITER")}},
+                                            ("J", "K_HT", "K_SYRK", "K_MIXED", "FOCK", "DIIS", "DENSITY", "ITER",
+                                             "FINAL")}},
             "roofline": {"bound": "tensor", "kernel": dom[0], "achieved": achieved, "peak": bf16,
                          "unit": "TFLOP/s", "frac": achieved / bf16, "traffic": traffic,
-                         "peak_kind": peak_kind + " bf16 dense", "note": "K computed in FP64 on the CUDA cores"},
+                         "peak_kind": peak_kind + " bf16 dense", "note": note},
             "cpu_baseline": cpu,
             "e2e": ({"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
                     if e2e is not None else None),
             "gpu_launches": launches,
             "clocks": clk,
-            "k_tflops": (fht + fsy) / ((ht_ms + sy_ms) * 1e-3) / 1e12,
+            "k_tflops": (fht + fsy) / (k_ms * 1e-3) / 1e12,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -279,6 +311,7 @@ def main():
     ap.add_argument("--ene-tol", type=float, default=1e-8)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

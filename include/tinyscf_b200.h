@@ -40,6 +40,8 @@ enum {
     TINYSCF_T_DENSITY,       /* eigensolve + density                 */
     TINYSCF_T_ITER,          /* one SCF iteration                    */
     TINYSCF_T_SCF,           /* the whole TinySCF_do_SCF             */
+    TINYSCF_T_K_MIXED,       /* mixed-precision incremental K        */
+    TINYSCF_T_FINAL,         /* final FP64 Fock build (mixed mode)   */
     TINYSCF_T_COUNT
 };
 
@@ -99,6 +101,15 @@ TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
 TINYSCF_API int TinySCF_build_J_noalloc(const double *B, int naux, const int *up_i, const int *up_j,
                                         const int *up_u, int nup, int nbf, const double *D, double *J,
                                         void *stream);
+/* Precision of the exchange build. TINYSCF_K_FP64 (default): FP64 on the CUDA
+ * cores, the reference's arithmetic. TINYSCF_K_MIXED: incremental builds from
+ * the change of the occupied orbitals on the tcgen05 tensor cores (split-BF16
+ * operands, FP32 accumulation, FP64 K), then one FP64 Fock build at
+ * convergence whose energy is the result. In mixed mode each Fock build
+ * updates K from the previous build's orbitals; TinySCF_reset_scf restarts. */
+#define TINYSCF_K_FP64  0
+#define TINYSCF_K_MIXED 1
+TINYSCF_API int TinySCF_set_k_precision(TinySCF_t t, int mode);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

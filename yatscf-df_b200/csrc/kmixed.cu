@@ -1,0 +1,832 @@
+// Mixed-precision exchange (K) on the 5th-generation tensor cores (tcgen05).
+//
+// Both K contractions run as one warp-specialised UMMA GEMM kernel with
+// K-major BF16 operands staged by TMA (128-byte swizzle) and an FP32
+// accumulator in tensor memory. Every FP64/FP32 operand x is split into
+// x_hi = bf16(x), x_lo = bf16(x - x_hi); each product uses three MMAs
+// (hi*hi + hi*lo + lo*hi), which keeps ~16 significant bits per operand.
+//
+// The K build is incremental (build_Fock.c:244-347 restated on differences):
+//   C'_n  = C_n R,  R = polar(C_n^T S C_{n-1})       (align the occupied orbitals)
+//   dC    = C'_n - C_{n-1}
+//   dT    = half-transform(dC)                         (mode 0, per CSR row i)
+//   T_n   = T_{n-1} + dT,  S_T = T_n + T_{n-1}
+//   K_n   = K_{n-1} + sym(dT S_T^T)                    (mode 1, split-K)
+// so that T_n T_n^T - T_{n-1} T_{n-1}^T is formed from dT: the low-precision
+// error of each increment scales with |dC| ~ |dD| and vanishes as the SCF
+// converges. K_n is accumulated in FP64.
+//
+// Warp roles (192 threads): warp 0 issues TMA loads, warp 1 allocates tensor
+// memory and issues the MMAs, warps 2-5 drain the accumulator (each warp reads
+// the TMEM lane quadrant warp_id % 4). All mbarrier waits are bounded; a
+// timeout sets an error flag instead of hanging.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <vector>
+
+#include "tscf_internal.h"
+
+namespace tscf {
+
+namespace {
+
+constexpr int UM = 128;          // UMMA M (rows of A per CTA)
+constexpr int BK = 64;           // K per pipeline stage (one 128-byte swizzle row of BF16)
+constexpr int UK = 16;           // K per tcgen05.mma.kind::f16
+constexpr long long WAIT_CYCLES = 4000000000LL;   // ~2 s at 2 GHz
+
+__device__ int g_umma_error;     // set to a nonzero code when a bounded wait times out
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait on an mbarrier phase. Returns false (and records code) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, int code)
+{
+    const uint32_t addr = smem_u32(bar);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > WAIT_CYCLES) {
+            atomicExch(&g_umma_error, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"((uint64_t) map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle: rows of 128 B, 8-row atoms 1024 B apart.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t) ((addr >> 4) & 0x3FFF);   // start address
+    d |= (uint64_t) 1 << 16;                  // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t) (1024 >> 4) << 32;        // stride byte offset: next 8-row atom
+    d |= (uint64_t) 1 << 46;                  // descriptor version (sm_100)
+    d |= (uint64_t) 2 << 61;                  // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) | ((uint32_t) (UM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    hi = __float2bfloat16_rn(x);
+    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+struct HalfArgs {            // half-transform of one CSR row per blockIdx.y
+    const int *row_chunk0;   // [nbf+1] first 64-chunk of each padded CSR row
+    float *Tm;               // T master [nbf][Qp] FP32
+    __nv_bfloat16 *dTh, *dTl, *Sh, *Sl;   // [nbf][Qp]
+    int nocc, naux;
+    long long Qp;
+};
+struct GArgs {               // split-K partial of dT S^T
+    double *part;            // [ksplit][nbf][nbf]
+    int nbf;
+    int chunks_per_split;
+    int total_chunks;
+};
+
+constexpr int EPI_WARPS = 8;                  // two warps per TMEM lane quadrant
+constexpr int THREADS = 64 + 32 * EPI_WARPS;  // TMA warp, MMA warp, epilogue warps
+constexpr int SEG_CHUNKS = 4;                 // G: drain the accumulator every 256 K
+constexpr int FLUSH_SEGS = 8;                 // G: fold the FP32 register sums into FP64 every 2048 K
+
+// One k-chunk (64 K) of split-BF16 MMAs: hi*hi into acc_main, hi*lo + lo*hi
+// into acc_corr. Keeping the small correction terms apart means the large
+// accumulator takes one FP32 addition per 16 K instead of three.
+template <bool LOLO>
+__device__ __forceinline__ void mma_chunk(uint32_t a_hi, uint32_t a_lo, uint32_t b_hi, uint32_t b_lo, uint32_t acc_main,
+                                          uint32_t acc_corr, uint32_t idesc, bool first)
+{
+#pragma unroll
+    for (int kk = 0; kk < BK / UK; kk++) {
+        const uint32_t off = kk * UK * 2;   // bytes along K inside the 128-byte row
+        const uint64_t dah = desc_sw128(a_hi + off), dal = desc_sw128(a_lo + off);
+        const uint64_t dbh = desc_sw128(b_hi + off), dbl = desc_sw128(b_lo + off);
+        const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+        umma_bf16(acc_main, dah, dbh, idesc, acc);
+        umma_bf16(acc_corr, dah, dbl, idesc, acc);
+        umma_bf16(acc_corr, dal, dbh, idesc, 1u);
+        if (LOLO) umma_bf16(acc_corr, dal, dbl, idesc, 1u);
+    }
+}
+
+__device__ __forceinline__ void tmem_alloc_warp(uint32_t *slot, uint32_t cols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+// ------------------------------------------------------------------ half-transform
+// CTA (x, y): rows P = 128x..128x+127 of the aux index, CSR row i = y.
+// D[P][s] = sum_r BpT[P][r] CgT[s][r] over the padded CSR row i.
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(THREADS, 1)
+k_half(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+       const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, HalfArgs ha)
+{
+    constexpr int A_BYTES = UM * BK * 2;
+    constexpr int B_BYTES = BN * BK * 2;
+    constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    constexpr uint32_t ACC_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;   // main + corrections
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    uint64_t *full = (uint64_t *) (smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *accum = empty + STAGES;
+    uint32_t *tmem_slot = (uint32_t *) (accum + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * UM, i = blockIdx.y;
+    const int kc0 = ha.row_chunk0[i], nk = ha.row_chunk0[i + 1] - kc0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accum, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc_warp(tmem_slot, TMEM_COLS);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        bool ok = true;
+        for (int kb = 0; kb < nk && ok; kb++) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES) ok = mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, 1);
+            if (!ok) break;
+            unsigned char *st = smem + s * STAGE_BYTES;
+            mbar_expect_tx(&full[s], STAGE_BYTES);
+            const int kx = (kc0 + kb) * BK;
+            tma_load_2d(st, &mAh, &full[s], kx, m0);
+            tma_load_2d(st + A_BYTES, &mAl, &full[s], kx, m0);
+            tma_load_2d(st + 2 * A_BYTES, &mBh, &full[s], kx, 0);
+            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, &full[s], kx, 0);
+        }
+        for (int kb = (nk > STAGES ? nk - STAGES : 0); kb < nk; kb++)
+            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, 2);
+    } else if (warp == 1 && lane == 0) {
+        constexpr uint32_t idesc = idesc_bf16(BN);
+        bool ok = true;
+        for (int kb = 0; kb < nk && ok; kb++) {
+            const int s = kb % STAGES;
+            ok = mbar_wait(&full[s], (kb / STAGES) & 1, 3);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
+            // the half-transform is bandwidth-bound: the fourth (lo*lo) product is free
+            mma_chunk<true>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + B_BYTES, tmem,
+                            tmem + ACC_COLS, idesc, kb == 0);
+            umma_commit(&empty[s]);
+        }
+        umma_commit(accum);
+    } else if (warp >= 2) {
+        const bool ok = (nk > 0) ? mbar_wait(accum, 0, 4) : true;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int row = quad * 32 + lane;
+        const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16);
+        const int P = m0 + row;
+        const size_t base = (size_t) i * ha.Qp + P;
+        uint32_t rm[32];
+        float dtv[32];
+        for (int c0 = half * 32; c0 < BN; c0 += 64) {
+            if (nk > 0 && ok) {
+                tmem_ld32(tq + c0, rm);
+#pragma unroll
+                for (int q = 0; q < 32; q++) dtv[q] = __uint_as_float(rm[q]);
+                tmem_ld32(tq + ACC_COLS + c0, rm);
+#pragma unroll
+                for (int q = 0; q < 32; q++) dtv[q] += __uint_as_float(rm[q]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 32; q++) dtv[q] = 0.f;
+            }
+            if (P >= ha.naux) continue;
+#pragma unroll
+            for (int h16 = 0; h16 < 32; h16 += 16) {
+            float told[16];
+#pragma unroll
+            for (int q = h16; q < h16 + 16; q++) {   // loads first: 16 in flight per thread
+                const int s = c0 + q;
+                told[q - h16] = (s < ha.nocc) ? ha.Tm[base + (size_t) s * ha.naux] : 0.f;
+            }
+#pragma unroll
+            for (int q = h16; q < h16 + 16; q++) {
+                const int s = c0 + q;
+                if (s < ha.nocc) {
+                    const size_t idx = base + (size_t) s * ha.naux;
+                    const float dt = dtv[q];
+                    const float tnew = told[q - h16] + dt;
+                    ha.Tm[idx] = tnew;
+                    __nv_bfloat16 h, l;
+                    split_bf16(dt, h, l);
+                    ha.dTh[idx] = h;
+                    ha.dTl[idx] = l;
+                    split_bf16(told[q - h16] + tnew, h, l);
+                    ha.Sh[idx] = h;
+                    ha.Sl[idx] = l;
+                }
+            }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// ------------------------------------------------------------------ G = dT S^T, split-K
+// CTA (x, y, z): output tile rows 128x.., cols 128y.., K chunks of split z.
+// The K range is cut into segments of SEG_CHUNKS chunks; each segment
+// accumulates in one of two TMEM buffers (main 128 cols + corrections 128
+// cols each, 512 cols in all) while the epilogue warps drain the other one
+// into FP64 registers, so no FP32 accumulation runs longer than 256 K.
+template <int STAGES>
+__global__ void __launch_bounds__(THREADS, 1)
+k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+       const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, GArgs ga)
+{
+    constexpr int BN = 128;
+    constexpr int A_BYTES = UM * BK * 2, B_BYTES = BN * BK * 2;
+    constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    constexpr uint32_t TMEM_COLS = 512;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    uint64_t *full = (uint64_t *) (smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;    // [2] accumulator buffer ready
+    uint64_t *tempty = tfull + 2;        // [2] accumulator buffer drained
+    uint32_t *tmem_slot = (uint32_t *) (tempty + 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * UM, n0 = blockIdx.y * BN;
+    const int kc0 = blockIdx.z * ga.chunks_per_split;
+    const int nk = max(0, min(ga.total_chunks, kc0 + ga.chunks_per_split) - kc0);
+    const int nseg = (nk + SEG_CHUNKS - 1) / SEG_CHUNKS;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], EPI_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc_warp(tmem_slot, TMEM_COLS);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        bool ok = true;
+        for (int kb = 0; kb < nk && ok; kb++) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES) ok = mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, 11);
+            if (!ok) break;
+            unsigned char *st = smem + s * STAGE_BYTES;
+            mbar_expect_tx(&full[s], STAGE_BYTES);
+            const int kx = (kc0 + kb) * BK;
+            tma_load_2d(st, &mAh, &full[s], kx, m0);
+            tma_load_2d(st + A_BYTES, &mAl, &full[s], kx, m0);
+            tma_load_2d(st + 2 * A_BYTES, &mBh, &full[s], kx, n0);
+            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, &full[s], kx, n0);
+        }
+        for (int kb = (nk > STAGES ? nk - STAGES : 0); kb < nk; kb++)
+            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, 12);
+    } else if (warp == 1 && lane == 0) {
+        constexpr uint32_t idesc = idesc_bf16(BN);
+        bool ok = true;
+        int kb = 0;
+        for (int seg = 0; seg < nseg && ok; seg++) {
+            const int b = seg & 1;
+            if (seg >= 2) ok = mbar_wait(&tempty[b], ((seg >> 1) - 1) & 1, 13);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t acc_main = tmem + b * 256, acc_corr = acc_main + 128;
+            const int kend = min(nk, (seg + 1) * SEG_CHUNKS);
+            for (; kb < kend && ok; kb++) {
+                const int s = kb % STAGES;
+                ok = mbar_wait(&full[s], (kb / STAGES) & 1, 14);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
+                mma_chunk<false>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + B_BYTES, acc_main,
+                                 acc_corr, idesc, kb == seg * SEG_CHUNKS);
+                umma_commit(&empty[s]);
+            }
+            umma_commit(&tfull[b]);
+        }
+    } else if (warp >= 2) {
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int row = quad * 32 + lane;
+        const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16) + half * 64;
+        const int gi = m0 + row;
+        const int lim = ga.nbf - (n0 + half * 64);
+        double *o = ga.part + (size_t) blockIdx.z * ga.nbf * ga.nbf + (size_t) gi * ga.nbf + n0 + half * 64;
+        const bool own = gi < ga.nbf;
+        // FP32 sums of at most FLUSH_SEGS segment results (round-to-nearest adds),
+        // folded into the split's FP64 partial, which this thread alone owns
+        float acc[64];
+#pragma unroll
+        for (int c = 0; c < 64; c++) acc[c] = 0.f;
+        uint32_t r[32];
+        bool ok = true, wrote = false;
+        for (int seg = 0; seg < nseg && ok; seg++) {
+            const int b = seg & 1;
+            ok = mbar_wait(&tfull[b], (seg >> 1) & 1, 15);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int c0 = 0; c0 < 64; c0 += 32) {
+                tmem_ld32(tq + b * 256 + c0, r);
+                float t[32];
+#pragma unroll
+                for (int q = 0; q < 32; q++) t[q] = __uint_as_float(r[q]);
+                tmem_ld32(tq + b * 256 + 128 + c0, r);
+#pragma unroll
+                for (int q = 0; q < 32; q++) acc[c0 + q] += t[q] + __uint_as_float(r[q]);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[b])) : "memory");
+            if ((seg + 1) % FLUSH_SEGS == 0 || seg + 1 == nseg) {
+                if (own) {
+#pragma unroll
+                    for (int c = 0; c < 64; c++)
+                        if (c < lim) o[c] = (wrote ? o[c] : 0.0) + (double) acc[c];
+                }
+                wrote = true;
+#pragma unroll
+                for (int c = 0; c < 64; c++) acc[c] = 0.f;
+            }
+        }
+        if (!wrote && own) {
+#pragma unroll
+            for (int c = 0; c < 64; c++)
+                if (c < lim) o[c] = 0.0;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+template <int BN, int STAGES>
+constexpr int half_smem_bytes()
+{
+    return STAGES * (2 * UM * BK * 2 + 2 * BN * BK * 2) + 1024 + 8 * (2 * STAGES + 1) + 16;
+}
+template <int STAGES>
+constexpr int gemm_smem_bytes()
+{
+    return STAGES * (4 * UM * BK * 2) + 1024 + 8 * (2 * STAGES + 4) + 16;
+}
+
+// ---------------------------------------------------------------- TMA descriptors
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn) p;
+    }
+    return fn;
+}
+
+// 2D BF16 matrix rows x cols (cols contiguous, pitch in elements), box 64 cols x box_rows.
+int make_map(CUtensorMap *m, const void *base, long long rows, long long cols, long long pitch, int box_rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return ERR_CUDA;
+    cuuint64_t dims[2] = {(cuuint64_t) cols, (cuuint64_t) rows};
+    cuuint64_t strides[1] = {(cuuint64_t) pitch * 2};
+    cuuint32_t box[2] = {(cuuint32_t) BK, (cuuint32_t) box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? OK : ERR_CUDA;
+}
+
+}  // namespace
+
+// N of the half-transform GEMM: the occupied orbitals padded to a multiple of 16.
+int kmix_half_bn(int nocc) { return (nocc + 15) / 16 * 16; }
+
+// ---------------------------------------------------------------- kernels around the GEMMs
+// Transposed, row-padded copy of the DF tensor for the half-transform's A
+// operand: BpT[P][r] = B(CSR entry of padded position r, P), zero in padding.
+__global__ void k_build_bpt(const double *Bu, const int *pad_entry, const int *csr_u, int naux, long long rp,
+                            __nv_bfloat16 *Bh, __nv_bfloat16 *Bl)
+{
+    __shared__ float tile[32][33];
+    const long long r0 = (long long) blockIdx.x * 32;
+    const int p0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8 threads
+    for (int k = ty; k < 32; k += 8) {
+        const long long r = r0 + k;
+        const int e = (r < rp) ? pad_entry[r] : -1;
+        const int p = p0 + tx;
+        tile[k][tx] = (e >= 0 && p < naux) ? (float) Bu[(size_t) csr_u[e] * naux + p] : 0.f;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int p = p0 + k;
+        const long long r = r0 + tx;
+        if (p < naux && r < rp) {
+            __nv_bfloat16 h, l;
+            split_bf16(tile[tx][k], h, l);
+            Bh[(size_t) p * rp + r] = h;
+            Bl[(size_t) p * rp + r] = l;
+        }
+    }
+}
+
+// CgT[s][r] = dC(j of padded position r, s): the half-transform's B operand.
+__global__ void k_gather_dc(const double *dC, const int *pad_entry, const int *csr_j, int nocc, long long rp,
+                            __nv_bfloat16 *Ch, __nv_bfloat16 *Cl)
+{
+    const long long r = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (r >= rp) return;
+    const int e = pad_entry[r];
+    const float v = (e >= 0 && s < nocc) ? (float) dC[(size_t) csr_j[e] * nocc + s] : 0.f;
+    __nv_bfloat16 h, l;
+    split_bf16(v, h, l);
+    Ch[(size_t) s * rp + r] = h;
+    Cl[(size_t) s * rp + r] = l;
+}
+
+// K[i][j] = (reset ? 0 : K[i][j]) + (G_ij + G_ji) / 2, G summed over splits in FP64.
+__global__ void k_kmix_reduce(const double *part, int ksplit, int nbf, int reset, double *K)
+{
+    const size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t) nbf * nbf) return;
+    const int i = (int) (idx / nbf), j = (int) (idx % nbf);
+    const size_t tdx = (size_t) j * nbf + i;
+    const size_t nn = (size_t) nbf * nbf;
+    double gij = 0.0, gji = 0.0;
+    for (int k = 0; k < ksplit; k++) {
+        gij += part[k * nn + idx];
+        gji += part[k * nn + tdx];
+    }
+    const double d = 0.5 * (gij + gji);
+    K[idx] = reset ? d : K[idx] + d;
+}
+
+// Newton-Schulz step helper: Z = 1.5 I - 0.5 Y
+__global__ void k_ns_z(const double *Y, double *Z, int n)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * n) return;
+    const int i = idx / n, j = idx % n;
+    Z[idx] = (i == j ? 1.5 : 0.0) - 0.5 * Y[idx];
+}
+
+// R = X if max|X^T X - I| <= tol (Y holds X^T X) else I.
+__global__ void k_select_r(const double *X, const double *Y, double *R, int n, double tol)
+{
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx % n;
+        const double e = Y[idx] - (i == j ? 1.0 : 0.0);
+        if (!(fabs(e) <= tol)) bad = 1;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx % n;
+        R[idx] = bad ? (i == j ? 1.0 : 0.0) : X[idx];
+    }
+}
+
+// dC = C' - Cprev; Cprev = C'
+__global__ void k_delta_c(const double *Cn, double *Cprev, double *dC, size_t n)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double c = Cn[i];
+    dC[i] = c - Cprev[i];
+    Cprev[i] = c;
+}
+
+// ---------------------------------------------------------------- plan
+struct KMix {
+    int nbf = 0, naux = 0, nocc = 0, bn_half = 0, ksplit = 1, chunks_per_split = 1, total_chunks = 0;
+    long long rp = 0, Qp = 0;
+    int *row_chunk0 = nullptr, *pad_entry = nullptr;
+    const int *csr_j = nullptr;
+    __nv_bfloat16 *Bh = nullptr, *Bl = nullptr, *Ch = nullptr, *Cl = nullptr;
+    float *Tm = nullptr;
+    double *G = nullptr;
+    __nv_bfloat16 *dTh = nullptr, *dTl = nullptr, *Sh = nullptr, *Sl = nullptr;
+    double *Cprev = nullptr, *Cal = nullptr, *dC = nullptr, *SC = nullptr, *M = nullptr, *X = nullptr,
+           *Y = nullptr, *Z = nullptr, *R = nullptr;
+    CUtensorMap mBh, mBl, mCh, mCl, mdTh, mdTl, mSh, mSl;
+    bool first = true;
+    std::vector<void *> mem;
+};
+
+static int kalloc(KMix *k, void **p, size_t bytes)
+{
+    if (cudaMalloc(p, bytes ? bytes : 16) != cudaSuccess) {
+        cudaGetLastError();
+        return ERR_ALLOC;
+    }
+    k->mem.push_back(*p);
+    return OK;
+}
+
+#define KRC(x)                  \
+    do {                        \
+        int rc__ = (x);         \
+        if (rc__) return rc__;  \
+    } while (0)
+
+void kmix_destroy(KMix *k)
+{
+    if (!k) return;
+    for (void *p : k->mem) cudaFree(p);
+    delete k;
+}
+
+int kmix_create(KMix **out, const FockPlan &p, const int *h_displs, cudaStream_t s)
+{
+    *out = nullptr;
+    if (p.nocc > 256) return ERR_UNSUPPORTED;
+    KMix *k = new KMix();
+    k->nbf = p.nbf;
+    k->naux = p.naux;
+    k->nocc = p.nocc;
+    k->bn_half = kmix_half_bn(p.nocc);
+    k->csr_j = p.csr_j;
+    // padded CSR rows: each row starts at a multiple of 64 positions
+    std::vector<int> chunk0(p.nbf + 1), pad;
+    long long pos = 0;
+    for (int i = 0; i < p.nbf; i++) {
+        chunk0[i] = (int) (pos / BK);
+        const int len = h_displs[i + 1] - h_displs[i];
+        const int plen = (len + BK - 1) / BK * BK;
+        for (int q = 0; q < plen; q++) pad.push_back(q < len ? h_displs[i] + q : -1);
+        pos += plen;
+    }
+    chunk0[p.nbf] = (int) (pos / BK);
+    k->rp = pos;
+    k->Qp = ((long long) p.nocc * p.naux + BK - 1) / BK * BK;
+    k->total_chunks = (int) (k->Qp / BK);
+    const int mt = (p.nbf + UM - 1) / UM;
+    const int tiles = mt * mt;
+    int ks = (4 * 148 + tiles - 1) / tiles;
+    ks = std::max(1, std::min(ks, k->total_chunks / 4 > 0 ? k->total_chunks / 4 : 1));
+    if (const char *ev = getenv("TINYSCF_KMIX_KSPLIT"))
+        if (atoi(ev) > 0) ks = std::min(atoi(ev), k->total_chunks);
+    k->chunks_per_split = (k->total_chunks + ks - 1) / ks;
+    k->ksplit = (k->total_chunks + k->chunks_per_split - 1) / k->chunks_per_split;
+    const size_t nbq = (size_t) p.nbf * k->Qp;
+    const int nocc_pad = k->bn_half;
+    int rc = OK;
+    do {
+        if ((rc = kalloc(k, (void **) &k->row_chunk0, sizeof(int) * chunk0.size()))) break;
+        if ((rc = kalloc(k, (void **) &k->pad_entry, sizeof(int) * pad.size()))) break;
+        if ((rc = kalloc(k, (void **) &k->Bh, 2 * (size_t) p.naux * k->rp))) break;
+        if ((rc = kalloc(k, (void **) &k->Bl, 2 * (size_t) p.naux * k->rp))) break;
+        if ((rc = kalloc(k, (void **) &k->Ch, 2 * (size_t) nocc_pad * k->rp))) break;
+        if ((rc = kalloc(k, (void **) &k->Cl, 2 * (size_t) nocc_pad * k->rp))) break;
+        if ((rc = kalloc(k, (void **) &k->Tm, 4 * nbq))) break;
+        if ((rc = kalloc(k, (void **) &k->dTh, 2 * nbq))) break;
+        if ((rc = kalloc(k, (void **) &k->dTl, 2 * nbq))) break;
+        if ((rc = kalloc(k, (void **) &k->Sh, 2 * nbq))) break;
+        if ((rc = kalloc(k, (void **) &k->Sl, 2 * nbq))) break;
+        if ((rc = kalloc(k, (void **) &k->G, 8 * (size_t) k->ksplit * p.nbf * p.nbf))) break;
+        const size_t nc = (size_t) p.nbf * p.nocc, oo = (size_t) p.nocc * p.nocc;
+        if ((rc = kalloc(k, (void **) &k->Cprev, 8 * nc))) break;
+        if ((rc = kalloc(k, (void **) &k->Cal, 8 * nc))) break;
+        if ((rc = kalloc(k, (void **) &k->dC, 8 * nc))) break;
+        if ((rc = kalloc(k, (void **) &k->SC, 8 * nc))) break;
+        if ((rc = kalloc(k, (void **) &k->M, 8 * oo))) break;
+        if ((rc = kalloc(k, (void **) &k->X, 8 * oo))) break;
+        if ((rc = kalloc(k, (void **) &k->Y, 8 * oo))) break;
+        if ((rc = kalloc(k, (void **) &k->Z, 8 * oo))) break;
+        if ((rc = kalloc(k, (void **) &k->R, 8 * oo))) break;
+    } while (0);
+    if (rc) {
+        kmix_destroy(k);
+        return rc;
+    }
+    cudaMemcpyAsync(k->row_chunk0, chunk0.data(), sizeof(int) * chunk0.size(), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(k->pad_entry, pad.data(), sizeof(int) * pad.size(), cudaMemcpyHostToDevice, s);
+    // padded tails of the K dimension stay zero forever
+    cudaMemsetAsync(k->dTh, 0, 2 * nbq, s);
+    cudaMemsetAsync(k->dTl, 0, 2 * nbq, s);
+    cudaMemsetAsync(k->Sh, 0, 2 * nbq, s);
+    cudaMemsetAsync(k->Sl, 0, 2 * nbq, s);
+    dim3 gb((unsigned) ((k->rp + 31) / 32), (unsigned) ((p.naux + 31) / 32));
+    k_build_bpt<<<gb, dim3(32, 8), 0, s>>>(p.B, k->pad_entry, p.csr_u, p.naux, k->rp, k->Bh, k->Bl);
+    g_launches++;
+    if (make_map(&k->mBh, k->Bh, p.naux, k->rp, k->rp, UM) || make_map(&k->mBl, k->Bl, p.naux, k->rp, k->rp, UM) ||
+        make_map(&k->mCh, k->Ch, nocc_pad, k->rp, k->rp, nocc_pad) ||
+        make_map(&k->mCl, k->Cl, nocc_pad, k->rp, k->rp, nocc_pad) ||
+        make_map(&k->mdTh, k->dTh, p.nbf, k->Qp, k->Qp, UM) || make_map(&k->mdTl, k->dTl, p.nbf, k->Qp, k->Qp, UM) ||
+        make_map(&k->mSh, k->Sh, p.nbf, k->Qp, k->Qp, UM) || make_map(&k->mSl, k->Sl, p.nbf, k->Qp, k->Qp, UM)) {
+        kmix_destroy(k);
+        return ERR_CUDA;
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        kmix_destroy(k);
+        return ERR_CUDA;
+    }
+    *out = k;
+    return OK;
+}
+
+void kmix_reset(KMix *k, cudaStream_t s)
+{
+    cudaMemsetAsync(k->Tm, 0, 4 * (size_t) k->nbf * k->Qp, s);
+    cudaMemsetAsync(k->Cprev, 0, 8 * (size_t) k->nbf * k->nocc, s);
+    k->first = true;
+}
+
+template <int BN>
+static int launch_half(const KMix *k, const HalfArgs &ha, cudaStream_t s)
+{
+    constexpr int STAGES = 2;
+    constexpr int SMEM = half_smem_bytes<BN, STAGES>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(k_half<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+            return ERR_CUDA;
+        attr_set = true;
+    }
+    dim3 grid((k->naux + UM - 1) / UM, k->nbf);
+    k_half<BN, STAGES><<<grid, THREADS, SMEM, s>>>(k->mBh, k->mBl, k->mCh, k->mCl, ha);
+    g_launches++;
+    return OK;
+}
+
+static int launch_gemm(const KMix *k, const GArgs &ga, dim3 grid, cudaStream_t s)
+{
+    constexpr int STAGES = 3;
+    constexpr int SMEM = gemm_smem_bytes<STAGES>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(k_gemm<STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+            return ERR_CUDA;
+        attr_set = true;
+    }
+    k_gemm<STAGES><<<grid, THREADS, SMEM, s>>>(k->mdTh, k->mdTl, k->mSh, k->mSl, ga);
+    g_launches++;
+    return OK;
+}
+
+// One incremental K build from the new occupied factor Cocc (nbf x nocc).
+int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s)
+{
+    const int n = k->nbf, o = k->nocc;
+    // align C_n to C_{n-1}: R = polar(C_n^T S C_{n-1}) by Newton-Schulz; R = I if it does not converge
+    dgemm(false, false, n, o, n, 1.0, S, n, k->Cprev, o, 0.0, k->SC, o, s);
+    dgemm(true, false, o, o, n, 1.0, Cocc, o, k->SC, o, 0.0, k->X, o, s);
+    for (int it = 0; it < 12; it++) {
+        dgemm(true, false, o, o, o, 1.0, k->X, o, k->X, o, 0.0, k->Y, o, s);
+        k_ns_z<<<(o * o + 255) / 256, 256, 0, s>>>(k->Y, k->Z, o);
+        dgemm(false, false, o, o, o, 1.0, k->X, o, k->Z, o, 0.0, k->M, o, s);
+        std::swap(k->X, k->M);
+        g_launches++;
+    }
+    dgemm(true, false, o, o, o, 1.0, k->X, o, k->X, o, 0.0, k->Y, o, s);
+    k_select_r<<<1, 1024, 0, s>>>(k->X, k->Y, k->R, o, 1e-12);
+    dgemm(false, false, n, o, o, 1.0, Cocc, o, k->R, o, 0.0, k->Cal, o, s);
+    const size_t nc = (size_t) n * o;
+    k_delta_c<<<(unsigned) ((nc + 255) / 256), 256, 0, s>>>(k->Cal, k->Cprev, k->dC, nc);
+    dim3 gg((unsigned) ((k->rp + 255) / 256), k->bn_half);
+    k_gather_dc<<<gg, 256, 0, s>>>(k->dC, k->pad_entry, k->csr_j, o, k->rp, k->Ch, k->Cl);
+    g_launches += 3;
+    HalfArgs ha{k->row_chunk0, k->Tm, k->dTh, k->dTl, k->Sh, k->Sl, o, k->naux, k->Qp};
+    int rc;
+    switch (k->bn_half) {
+    case 16: rc = launch_half<16>(k, ha, s); break;
+    case 32: rc = launch_half<32>(k, ha, s); break;
+    case 48: rc = launch_half<48>(k, ha, s); break;
+    case 64: rc = launch_half<64>(k, ha, s); break;
+    case 80: rc = launch_half<80>(k, ha, s); break;
+    case 96: rc = launch_half<96>(k, ha, s); break;
+    case 112: rc = launch_half<112>(k, ha, s); break;
+    case 128: rc = launch_half<128>(k, ha, s); break;
+    case 144: rc = launch_half<144>(k, ha, s); break;
+    case 160: rc = launch_half<160>(k, ha, s); break;
+    case 176: rc = launch_half<176>(k, ha, s); break;
+    case 192: rc = launch_half<192>(k, ha, s); break;
+    case 208: rc = launch_half<208>(k, ha, s); break;
+    case 224: rc = launch_half<224>(k, ha, s); break;
+    case 240: rc = launch_half<240>(k, ha, s); break;
+    case 256: rc = launch_half<256>(k, ha, s); break;
+    default: rc = ERR_UNSUPPORTED;
+    }
+    if (rc) return rc;
+    const int mt = (n + UM - 1) / UM;
+    GArgs ga{k->G, n, k->chunks_per_split, k->total_chunks};
+    rc = launch_gemm(k, ga, dim3(mt, mt, k->ksplit), s);
+    if (rc) return rc;
+    const size_t nn = (size_t) n * n;
+    k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, k->ksplit, n, k->first ? 1 : 0, K);
+    g_launches++;
+    k->first = false;
+    return OK;
+}
+
+int kmix_error_flag()
+{
+    int v = 0;
+    cudaMemcpyFromSymbol(&v, g_umma_error, sizeof(int));
+    return v;
+}
+
+}  // namespace tscf

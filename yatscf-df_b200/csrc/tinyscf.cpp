@@ -286,6 +286,9 @@ struct Engine {
     int jblk = 1;
     double *epart = nullptr, *E = nullptr;
     Eig *eig = nullptr;
+    int kprec = TINYSCF_K_FP64;
+    KMix *kmix = nullptr;
+    double *Kmix = nullptr;
     int stage = 0;            // 1 hcore, 2 schwarz, 3 sparsity, 4 guess, 5 df
     bool F_is_orth = false;   // which buffer currently plays the reference's F_mat
     std::vector<void *> allocs;
@@ -859,7 +862,7 @@ int df_impl(TinySCF_t t)
 }
 
 // ------------------------------------------------------------------ Fock (build_Fock.c:349-396)
-int fock_device(TinySCF_t t)
+int fock_device(TinySCF_t t, bool force_fp64 = false)
 {
     Engine *e = E_(t);
     FockPlan p = e->plan();
@@ -867,12 +870,22 @@ int fock_device(TinySCF_t t)
     tstart(e, TINYSCF_T_J);
     build_J(p, e->D, e->J, e->Jt, e->Jpart, e->jblk, e->Jw, e->s);
     tstop(e, TINYSCF_T_J);
-    tstart(e, TINYSCF_T_K_HT);
-    build_K_halftransform(p, e->Cocc, e->T, e->s);
-    tstop(e, TINYSCF_T_K_HT);
-    tstart(e, TINYSCF_T_K_SYRK);
-    build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->tiles, e->s);
-    tstop(e, TINYSCF_T_K_SYRK);
+    const double *Kuse = e->K;
+    if (e->kprec == TINYSCF_K_MIXED && !force_fp64) {
+        tstart(e, TINYSCF_T_K_MIXED);
+        RC(kmix_build(e->kmix, e->Cocc, e->S, e->Kmix, e->s));
+        tstop(e, TINYSCF_T_K_MIXED);
+        Kuse = e->Kmix;
+    } else {
+        tstart(e, TINYSCF_T_K_HT);
+        build_K_halftransform(p, e->Cocc, e->T, e->s);
+        tstop(e, TINYSCF_T_K_HT);
+        tstart(e, TINYSCF_T_K_SYRK);
+        build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->tiles, e->s);
+        tstop(e, TINYSCF_T_K_SYRK);
+    }
+    if (Kuse != e->K)
+        cudaMemcpyAsync(e->K, Kuse, sizeof(double) * e->nn, cudaMemcpyDeviceToDevice, e->s);
     tstart(e, TINYSCF_T_FOCK);
     build_F_energy(e->H, e->J, e->K, e->D, e->F, e->epart, t->nbasfuncs, e->s);
     energy_reduce(e->epart, e->E, e->s);
@@ -1027,6 +1040,26 @@ int scf_impl(TinySCF_t t)
         if (t->iter == 0) energy_delta = 223;
         t->iter++;
     }
+    if (e->kprec == TINYSCF_K_MIXED) {
+        // one FP64 Fock build on the converged density; its energy is the result
+        tstart(e, TINYSCF_T_FINAL);
+        RC(fock_device(t, true));
+        tstop(e, TINYSCF_T_FINAL);
+        double E = 0.0;
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(&E, e->E, sizeof(double), cudaMemcpyDeviceToHost, e->s));
+        e->d2h += (long long) sizeof(double);
+        RC(sync_rc(e, "final FP64 Fock build"));
+        tcollect(e);
+        if (t->verbose)
+            printf("* Final FP64 Fock build: Energy = %.10lf (%.10lf), mixed-precision energy was %.10lf\n",
+                   E + t->nuc_energy, E, t->HF_energy + t->nuc_energy);
+        t->HF_energy = E;
+        int fl = kmix_error_flag();
+        if (fl) {
+            fprintf(stderr, "[tinyscf] tensor-core K: a bounded wait timed out (code %d)\n", fl);
+            return ERR_CUDA;
+        }
+    }
     cudaEventRecord(scf1, e->s);
     cudaEventSynchronize(scf1);
     float ms = 0;
@@ -1044,6 +1077,7 @@ void free_impl(TinySCF_t t)
     if (e) {
         if (e->s) cudaStreamSynchronize(e->s);
         eig_destroy(e->eig);
+        kmix_destroy(e->kmix);
         for (void *p : e->allocs) cudaFree(p);
         e->allocs.clear();
         if (e->s) {
@@ -1175,6 +1209,28 @@ int TinySCF_get_df_tensor(TinySCF_t t, double *out)
     return TINYSCF_OK;
 }
 
+int TinySCF_set_k_precision(TinySCF_t t, int mode)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (mode != TINYSCF_K_FP64 && mode != TINYSCF_K_MIXED) return TINYSCF_ERR_INPUT;
+    if (mode == TINYSCF_K_MIXED) {
+        if (e->stage < 5) return TINYSCF_ERR_STATE;   // needs the DF tensor
+        if (!e->kmix) {
+            FockPlan p = e->plan();
+            p.nocc = t->n_occ;
+            int rc = kmix_create(&e->kmix, p, t->bf_mask_displs, e->s);
+            if (rc) return rc;
+            rc = dalloc(e, &e->Kmix, e->nn);
+            if (rc) return rc;
+        }
+        kmix_reset(e->kmix, e->s);
+        if (sync_rc(e, "mixed K set-up")) return TINYSCF_ERR_CUDA;
+    }
+    e->kprec = mode;
+    return TINYSCF_OK;
+}
+
 int TinySCF_reset_scf(TinySCF_t t)
 {
     if (!t || !t->dev) return TINYSCF_ERR_STATE;
@@ -1188,6 +1244,7 @@ int TinySCF_reset_scf(TinySCF_t t)
     diis_init(e->diis, e->s);
     cudaMemsetAsync(e->F0, 0, sizeof(double) * e->nn * MAX_DIIS, e->s);
     cudaMemsetAsync(e->R, 0, sizeof(double) * e->nn * MAX_DIIS, e->s);
+    if (e->kmix) kmix_reset(e->kmix, e->s);
     t->iter = 0;
     t->DIIS_len = 0;
     t->DIIS_bmax_id = 0;

@@ -145,6 +145,16 @@ size_t build_K_part_elems(const FockPlan &p, int ksplit);
 void build_F_energy(const double *d_H, const double *d_J, const double *d_K, const double *d_D,
                     double *d_F, double *d_epart, int n, cudaStream_t s);
 constexpr int ENERGY_BLOCKS = 296;
+// ---------------------------------------------------------------- mixed-precision K (kmixed.cu)
+struct KMix;
+// Needs p.B, p.csr_j, p.csr_u, p.nbf, p.naux, p.nocc and the host CSR row starts.
+int  kmix_create(KMix **out, const FockPlan &p, const int *h_displs, cudaStream_t s);
+void kmix_destroy(KMix *k);
+void kmix_reset(KMix *k, cudaStream_t s);
+// K (FP64, accumulated across calls) from the occupied factor Cocc; S is the overlap.
+int  kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s);
+int  kmix_error_flag();
+
 // ---------------------------------------------------------------- DIIS / density (scf.cu)
 struct DiisState {            // device-resident DIIS bookkeeping (DIIS.c:12-123)
     int len;

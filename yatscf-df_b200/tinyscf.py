@@ -17,7 +17,8 @@ LIBPATH = os.path.join(HERE, "libtinyscf_b200.so")
 
 MAX_DIIS = 10
 TIMERS = ["HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM", "J", "K_HT", "K_SYRK",
-          "FOCK", "DIIS", "DENSITY", "ITER", "SCF"]
+          "FOCK", "DIIS", "DENSITY", "ITER", "SCF", "K_MIXED", "FINAL"]
+K_FP64, K_MIXED = 0, 1
 STATUS = {0: "success", 1: "CUDA error", 2: "cannot open input file", 3: "invalid input",
           4: "unsupported input", 5: "device allocation failed", 6: "numerical failure",
           7: "call out of order"}
@@ -97,6 +98,7 @@ def load_library(path=LIBPATH):
         "TinySCF_reset_timing_stats": ([T], ip),
         "TinySCF_get_counters": ([T, ctypes.POINTER(ctypes.c_longlong), ip], ip),
         "TinySCF_reset_scf": ([T], ip),
+        "TinySCF_set_k_precision": ([T, ip], ip),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -210,6 +212,12 @@ class TinySCF:
         if rc:
             raise TinySCFError("get_df_tensor: " + STATUS.get(rc, str(rc)))
         return out
+
+    def set_k_precision(self, mode):
+        """K_FP64 (the reference's arithmetic) or K_MIXED (tensor-core incremental K, final FP64 build)."""
+        rc = self.lib.TinySCF_set_k_precision(self.t, int(mode))
+        if rc:
+            raise TinySCFError("set_k_precision: " + STATUS.get(rc, str(rc)))
 
     def reset_scf(self):
         rc = self.lib.TinySCF_reset_scf(self.t)
