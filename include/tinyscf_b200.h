@@ -84,7 +84,9 @@ TINYSCF_API int TinySCF_get_timings(TinySCF_t t, double *ms, int n);
 TINYSCF_API int TinySCF_get_timing_stats(TinySCF_t t, double *sum_ms, long long *count, int n);
 TINYSCF_API int TinySCF_reset_timing_stats(TinySCF_t t);
 /* Counters: [0] engine kernels launched by this process, [1] bytes copied
- * host->device, [2] bytes copied device->host by this engine instance. */
+ * host->device, [2] bytes copied device->host by this engine instance,
+ * [3] full eigensolves and [4] occupied-subspace refinement steps taken by
+ * the density builds of this instance. */
 TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
 /* Coulomb matrix J from a density D without allocating anything: for callers
  * that cannot call cudaMalloc (a host framework that owns all device memory
@@ -110,6 +112,20 @@ TINYSCF_API int TinySCF_build_J_noalloc(const double *B, int naux, const int *up
 #define TINYSCF_K_FP64  0
 #define TINYSCF_K_MIXED 1
 TINYSCF_API int TinySCF_set_k_precision(TinySCF_t t, int mode);
+/* Density solver of the SCF loop. TINYSCF_DENSITY_EIG (default): a full
+ * eigendecomposition of X^T F X every iteration, as build_density.c:37-69.
+ * TINYSCF_DENSITY_REFINE: once a full eigensolve has been taken, later
+ * iterations refine the previous occupied subspace against the new Fock
+ * matrix (residual preconditioned with the last full eigenbasis, Loewdin
+ * re-orthonormalisation) until max|(I-P)F'U^T| < 1e-9 Eh, and fall back to a
+ * full eigensolve when that does not converge within a few steps. D is the
+ * same aufbau density as long as no orbital level crosses the HOMO-LUMO gap
+ * between full eigensolves; eigval and the columns of Cocc then hold the last
+ * full eigensolve's eigenvalues and an orthonormal (not canonical) occupied
+ * basis. */
+#define TINYSCF_DENSITY_EIG    0
+#define TINYSCF_DENSITY_REFINE 1
+TINYSCF_API int TinySCF_set_density_solver(TinySCF_t t, int mode);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

@@ -75,3 +75,40 @@ def test_mixed_scf_energy_matches_fp64(name):
     Em = em.energy
     em.free()
     assert abs(Em - E64) < 1e-8, (Em, E64)
+
+
+def test_refine_density_matches_full_eigensolves():
+    """Occupied-subspace refinement between full eigensolves converges to the
+    same SCF energy and density as a full eigensolve every iteration."""
+    e0 = engine("c10h22", tinyscf.K_FP64)
+    e0.s.ene_tol = 1e-10
+    e0.do_SCF()
+    E0, D0, it0 = e0.energy, e0.mat("D_mat"), e0.s.iter
+    e0.free()
+    e1 = engine("c10h22", tinyscf.K_FP64)
+    e1.set_density_solver(tinyscf.DENSITY_REFINE)
+    e1.s.ene_tol = 1e-10
+    c0 = e1.counters()
+    e1.do_SCF()
+    c1 = e1.counters()
+    E1, D1, it1 = e1.energy, e1.mat("D_mat"), e1.s.iter
+    e1.free()
+    n_eig, n_ref = c1[3] - c0[3], c1[4] - c0[4]
+    assert abs(E1 - E0) < 1e-9, (E1, E0)
+    assert np.abs(D1 - D0).max() < 1e-6
+    assert n_ref > 0 and n_eig < it1, (n_eig, n_ref, it1, it0)
+
+
+def test_mixed_refine_scf_energy_matches_fp64():
+    e64 = engine("c20h42", tinyscf.K_FP64)
+    e64.s.ene_tol = 1e-10
+    e64.do_SCF()
+    E64 = e64.energy
+    e64.free()
+    em = engine("c20h42", tinyscf.K_MIXED)
+    em.set_density_solver(tinyscf.DENSITY_REFINE)
+    em.s.ene_tol = 1e-10
+    em.do_SCF()
+    Em = em.energy
+    em.free()
+    assert abs(Em - E64) < 1e-8, (Em, E64)

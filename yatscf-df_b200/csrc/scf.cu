@@ -182,6 +182,136 @@ void diis_step(DiisState *st, int max_diis, const double *d_F, const double *d_D
     k_diis_combine<<<nb, 256, 0, s>>>(d_F0, st, d_Fout, nn);
 }
 
+// ------------------------------------------------------------------ occupied-subspace refinement
+// Between full eigensolves the occupied subspace of F' is refined from the
+// previous one: U (o x n, orthonormal rows in the orthogonal basis) moves along
+// the residual R = (I - U^T U) F' U^T, preconditioned with the last full
+// eigenbasis (virtual rows Vv, eigenvalues wv):
+//   U_i += sum_a Vv_a (Vv_a . R_i) / (eps_i - wv_a),   eps_i = (U F' U^T)_ii,
+// then Loewdin re-orthonormalisation. The fixed point is the invariant
+// subspace continuously connected to the previous occupied one, i.e. the
+// aufbau occupied space of build_density.c:37-69 as long as no level crosses
+// the gap.
+__global__ void k_sub(const double *A, double *R, size_t n)   // R = A - R
+{
+    size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) R[i] = A[i] - R[i];
+}
+
+__global__ void k_precond(double *Cv, const double *UA, const double *wv, int v, int o)
+{
+    size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t) v * o) return;
+    int a = (int) (idx / o), i = (int) (idx % o);
+    double d = UA[(size_t) i * o + i] - wv[a];
+    Cv[idx] = (fabs(d) > 1e-6) ? Cv[idx] / d : 0.0;
+}
+
+__global__ void k_add_transposed(double *U, const double *DT, int o, int n)   // U (o x n) += DT^T (DT: n x o)
+{
+    size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t) o * n) return;
+    int i = (int) (idx / n), k = (int) (idx % n);
+    U[idx] += DT[(size_t) k * o + i];
+}
+
+__global__ void k_absmax(const double *x, size_t n, double *out)
+{
+    __shared__ double sh[32];
+    double m = 0.0;
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+        m = fmax(m, fabs(x[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffff, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffff, m, o));
+        if (threadIdx.x == 0) {
+            unsigned long long *p = (unsigned long long *) out;
+            atomicMax(p, __double_as_longlong(m));   // m >= 0: integer order = float order
+        }
+    }
+}
+
+__global__ void k_ns_step(double *T, int n)   // T <- 1.5 I - 0.5 T
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * n) return;
+    T[idx] = (idx / n == idx % n ? 1.5 : 0.0) - 0.5 * T[idx];
+}
+
+__global__ void k_eye(double *A, int n)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < n * n) A[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+}
+
+// M^-1/2 of an SPD matrix close to I (coupled Newton-Schulz), result in Z.
+static void inv_sqrt_ns(const double *M, double *Y, double *Z, double *T, double *W, int o, int iters, cudaStream_t s)
+{
+    const unsigned nb = (unsigned) ((o * o + 255) / 256);
+    cudaMemcpyAsync(Y, M, sizeof(double) * o * o, cudaMemcpyDeviceToDevice, s);
+    k_eye<<<nb, 256, 0, s>>>(Z, o);
+    g_launches++;
+    for (int it = 0; it < iters; it++) {
+        dgemm(false, false, o, o, o, 1.0, Z, o, Y, o, 0.0, T, o, s);        // T = Z Y
+        k_ns_step<<<nb, 256, 0, s>>>(T, o);                                  // T = 1.5 I - 0.5 Z Y
+        dgemm(false, false, o, o, o, 1.0, Y, o, T, o, 0.0, W, o, s);        // Y <- Y T
+        cudaMemcpyAsync(Y, W, sizeof(double) * o * o, cudaMemcpyDeviceToDevice, s);
+        dgemm(false, false, o, o, o, 1.0, T, o, Z, o, 0.0, W, o, s);        // Z <- T Z
+        cudaMemcpyAsync(Z, W, sizeof(double) * o * o, cudaMemcpyDeviceToDevice, s);
+        g_launches++;
+    }
+}
+
+int subspace_refine(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n, int o,
+                    SubspaceWork &w, double tol, int max_steps, int *steps_out, double *res_out, cudaStream_t s)
+{
+    const int v = n - o;
+    const double *Vv = d_Vstale + (size_t) o * n;
+    const double *wv = d_wstale + o;
+    double res = 1e300, prev = 1e300;
+    int step = 0;
+    for (; step < max_steps; step++) {
+        dgemm(false, true, n, o, n, 1.0, d_Fp, n, d_U, n, 0.0, w.A, o, s);          // A = F' U^T (n x o)
+        dgemm(false, false, o, o, n, 1.0, d_U, n, w.A, o, 0.0, w.UA, o, s);        // UA = U F' U^T
+        dgemm(true, false, n, o, o, 1.0, d_U, n, w.UA, o, 0.0, w.R, o, s);         // R = U^T UA
+        k_sub<<<(unsigned) (((size_t) n * o + 255) / 256), 256, 0, s>>>(w.A, w.R, (size_t) n * o);   // R = A - R
+        cudaMemsetAsync(w.res, 0, sizeof(double), s);
+        k_absmax<<<148, 256, 0, s>>>(w.R, (size_t) n * o, w.res);
+        g_launches += 2;
+        cudaMemcpyAsync(&res, w.res, sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return ERR_CUDA;
+        if (res < tol) break;
+        // far from the last subspace, or contracting too slowly to reach tol in
+        // the steps left: leave it to a full eigensolve
+        if (step == 0 && res > 5e-2) break;
+        if (step > 0 && res * pow(res / prev, max_steps - step) > tol) break;
+        prev = res;
+        dgemm(false, false, v, o, n, 1.0, Vv, n, w.R, o, 0.0, w.Cv, o, s);        // Cv = Vv R
+        k_precond<<<(unsigned) (((size_t) v * o + 255) / 256), 256, 0, s>>>(w.Cv, w.UA, wv, v, o);
+        dgemm(true, false, n, o, v, 1.0, Vv, n, w.Cv, o, 0.0, w.A, o, s);         // A = Vv^T Cv (n x o)
+        k_add_transposed<<<(unsigned) (((size_t) o * n + 255) / 256), 256, 0, s>>>(d_U, w.A, o, n);
+        dgemm(false, true, o, o, n, 1.0, d_U, n, d_U, n, 0.0, w.M, o, s);         // M = U U^T
+        inv_sqrt_ns(w.M, w.Y, w.Z, w.T, w.W, o, 8, s);                              // Z = M^-1/2
+        dgemm(false, false, o, n, o, 1.0, w.Z, o, d_U, n, 0.0, w.A, n, s);        // U = Z U
+        cudaMemcpyAsync(d_U, w.A, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, s);
+        g_launches += 2;
+    }
+    *steps_out = step;
+    *res_out = res;
+    return OK;
+}
+
+// Cocc = X U^T (U: occupied rows in the orthogonal basis), D = Cocc Cocc^T
+void density_from_rows(const double *d_X, const double *d_U, double *d_Cocc, double *d_D, int n, int nocc,
+                       cudaStream_t s)
+{
+    dgemm(false, true, n, nocc, n, 1.0, d_X, n, d_U, n, 0.0, d_Cocc, nocc, s);
+    dgemm(false, true, n, n, nocc, 1.0, d_Cocc, nocc, d_Cocc, nocc, 0.0, d_D, n, s);
+}
+
 // ------------------------------------------------------------------ density
 void density_from_eig(const double *d_X, const double *d_V, double *d_Cocc, double *d_D, int n, int nocc,
                       cudaStream_t s)

@@ -30,6 +30,9 @@ namespace {
 
 const double A2BOHR = 1.0 / 0.52917720859;   // CMS_BasisSet.c:39
 const int ELEN = 50;
+// occupied-subspace refinement: residual bound (Eh) and step limit before a full eigensolve
+const double kRefineTol = 1e-9;
+const int kRefineSteps = 6;
 const char *ETABLE[ELEN] = {"H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg", "Al",
                             "Si", "P",  "S",  "Cl", "Ar", "K",  "Ca", "Sc", "Ti", "V",  "Cr", "Mn", "Fe",
                             "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",
@@ -287,6 +290,11 @@ struct Engine {
     double *epart = nullptr, *E = nullptr;
     Eig *eig = nullptr;
     int kprec = TINYSCF_K_FP64;
+    int dmode = TINYSCF_DENSITY_EIG;
+    double *U = nullptr;          // occupied rows (nocc x nbf) in the orthogonal basis
+    bool have_eig = false;        // V, w hold a full eigensolve of an earlier F'
+    SubspaceWork sw{};
+    long long n_eig = 0, n_refine = 0;
     KMix *kmix = nullptr;
     double *Kmix = nullptr;
     int stage = 0;            // 1 hcore, 2 schwarz, 3 sparsity, 4 guess, 5 df
@@ -943,11 +951,27 @@ int diis_impl(TinySCF_t t, bool to_host)
 int density_device(TinySCF_t t)
 {
     Engine *e = E_(t);
-    const int n = t->nbasfuncs;
+    const int n = t->nbasfuncs, o = t->n_occ;
     tstart(e, TINYSCF_T_DENSITY);
     const double *Fo = e->F_is_orth ? e->Fp : e->F;
+    if (e->dmode == TINYSCF_DENSITY_REFINE && e->have_eig && o > 0 && o < n) {
+        int steps = 0;
+        double res = 0.0;
+        RC(subspace_refine(Fo, e->V, e->w, e->U, n, o, e->sw, kRefineTol, kRefineSteps, &steps, &res, e->s));
+        e->n_refine += steps;
+        if (res < kRefineTol) {
+            density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, e->s);
+            tstop(e, TINYSCF_T_DENSITY);
+            return cuda_rc("density (subspace refinement)");
+        }
+    }
     RC(eig_run(e->eig, Fo, e->w, e->V, e->s));
-    density_from_eig(e->X, e->V, e->Cocc, e->D, n, t->n_occ, e->s);
+    density_from_eig(e->X, e->V, e->Cocc, e->D, n, o, e->s);
+    e->n_eig++;
+    if (e->dmode == TINYSCF_DENSITY_REFINE && o > 0) {
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(e->U, e->V, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, e->s));
+        e->have_eig = true;
+    }
     tstop(e, TINYSCF_T_DENSITY);
     return cuda_rc("density");
 }
@@ -1231,6 +1255,28 @@ int TinySCF_set_k_precision(TinySCF_t t, int mode)
     return TINYSCF_OK;
 }
 
+int TinySCF_set_density_solver(TinySCF_t t, int mode)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (mode != TINYSCF_DENSITY_EIG && mode != TINYSCF_DENSITY_REFINE) return TINYSCF_ERR_INPUT;
+    if (e->stage < 1) return TINYSCF_ERR_STATE;
+    const int n = t->nbasfuncs, o = t->n_occ;
+    if (mode == TINYSCF_DENSITY_REFINE && !e->U && o > 0) {
+        const size_t no = (size_t) n * o, oo = (size_t) o * o;
+        double **bufs[] = {&e->U, &e->sw.A, &e->sw.R, &e->sw.Cv};
+        for (double **b : bufs)
+            if (dalloc(e, b, no)) return TINYSCF_ERR_ALLOC;
+        double **small[] = {&e->sw.UA, &e->sw.M, &e->sw.Y, &e->sw.Z, &e->sw.T, &e->sw.W};
+        for (double **b : small)
+            if (dalloc(e, b, oo)) return TINYSCF_ERR_ALLOC;
+        if (dalloc(e, &e->sw.res, 1)) return TINYSCF_ERR_ALLOC;
+    }
+    e->dmode = mode;
+    e->have_eig = false;
+    return TINYSCF_OK;
+}
+
 int TinySCF_reset_scf(TinySCF_t t)
 {
     if (!t || !t->dev) return TINYSCF_ERR_STATE;
@@ -1245,6 +1291,7 @@ int TinySCF_reset_scf(TinySCF_t t)
     cudaMemsetAsync(e->F0, 0, sizeof(double) * e->nn * MAX_DIIS, e->s);
     cudaMemsetAsync(e->R, 0, sizeof(double) * e->nn * MAX_DIIS, e->s);
     if (e->kmix) kmix_reset(e->kmix, e->s);
+    e->have_eig = false;
     t->iter = 0;
     t->DIIS_len = 0;
     t->DIIS_bmax_id = 0;
@@ -1278,8 +1325,8 @@ int TinySCF_get_counters(TinySCF_t t, long long *out, int n)
 {
     if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
-    long long v[3] = {g_launches, e->h2d, e->d2h};
-    for (int k = 0; k < n && k < 3; k++) out[k] = v[k];
+    long long v[5] = {g_launches, e->h2d, e->d2h, e->n_eig, e->n_refine};
+    for (int k = 0; k < n && k < 5; k++) out[k] = v[k];
     return TINYSCF_OK;
 }
 

@@ -172,6 +172,14 @@ void diis_step(DiisState *d_st, int max_diis, const double *d_F, const double *d
                int n, cudaStream_t s);
 void xtfx(const double *d_X, const double *d_F, double *d_out, double *d_tmp, int n, cudaStream_t s);
 void energy_reduce(const double *d_epart, double *d_E, cudaStream_t s);
+// Occupied-subspace refinement between full eigensolves (scf.cu).
+struct SubspaceWork {
+    double *A, *UA, *R, *Cv, *M, *Y, *Z, *T, *W, *res;
+};
+int subspace_refine(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n, int o,
+                    SubspaceWork &w, double tol, int max_steps, int *steps_out, double *res_out, cudaStream_t s);
+void density_from_rows(const double *d_X, const double *d_U, double *d_Cocc, double *d_D, int n, int nocc,
+                       cudaStream_t s);
 // Cocc = X * V[0:nocc]^T (eigenvectors in rows), D = Cocc Cocc^T.
 void density_from_eig(const double *d_X, const double *d_V, double *d_Cocc, double *d_D, int n, int nocc,
                       cudaStream_t s);

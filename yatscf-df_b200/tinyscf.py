@@ -19,6 +19,7 @@ MAX_DIIS = 10
 TIMERS = ["HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM", "J", "K_HT", "K_SYRK",
           "FOCK", "DIIS", "DENSITY", "ITER", "SCF", "K_MIXED", "FINAL"]
 K_FP64, K_MIXED = 0, 1
+DENSITY_EIG, DENSITY_REFINE = 0, 1
 STATUS = {0: "success", 1: "CUDA error", 2: "cannot open input file", 3: "invalid input",
           4: "unsupported input", 5: "device allocation failed", 6: "numerical failure",
           7: "call out of order"}
@@ -99,6 +100,7 @@ def load_library(path=LIBPATH):
         "TinySCF_get_counters": ([T, ctypes.POINTER(ctypes.c_longlong), ip], ip),
         "TinySCF_reset_scf": ([T], ip),
         "TinySCF_set_k_precision": ([T, ip], ip),
+        "TinySCF_set_density_solver": ([T, ip], ip),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -219,6 +221,12 @@ class TinySCF:
         if rc:
             raise TinySCFError("set_k_precision: " + STATUS.get(rc, str(rc)))
 
+    def set_density_solver(self, mode):
+        """DENSITY_EIG (full eigensolve every iteration, the reference's) or DENSITY_REFINE."""
+        rc = self.lib.TinySCF_set_density_solver(self.t, int(mode))
+        if rc:
+            raise TinySCFError("set_density_solver: " + STATUS.get(rc, str(rc)))
+
     def reset_scf(self):
         rc = self.lib.TinySCF_reset_scf(self.t)
         if rc:
@@ -235,9 +243,10 @@ class TinySCF:
         self.lib.TinySCF_reset_timing_stats(self.t)
 
     def counters(self):
-        """(engine kernel launches in this process, bytes host->device, bytes device->host)."""
-        out = (ctypes.c_longlong * 3)()
-        self.lib.TinySCF_get_counters(self.t, out, 3)
+        """(engine kernel launches in this process, bytes host->device, bytes device->host,
+        full eigensolves, subspace refinement steps)."""
+        out = (ctypes.c_longlong * 5)()
+        self.lib.TinySCF_get_counters(self.t, out, 5)
         return tuple(int(v) for v in out)
 
     def timings(self):
