@@ -186,6 +186,7 @@ def run_ours(args, rank, world, local_rank):
     def timed_solves(mode, steps, warmup, sample_clocks):
         e.set_k_precision(mode)
         e.set_density_solver(tinyscf.DENSITY_REFINE if mode == tinyscf.K_MIXED else tinyscf.DENSITY_EIG)
+        e.set_graph(mode == tinyscf.K_MIXED)
         for _ in range(warmup):
             e.reset_scf()
             e.do_SCF()
@@ -230,6 +231,7 @@ def run_ours(args, rank, world, local_rank):
         if args.precision == "mixed":
             e2.set_k_precision(tinyscf.K_MIXED)
             e2.set_density_solver(tinyscf.DENSITY_REFINE)
+            e2.set_graph(True)
         e2.do_SCF()
         _ = e2.energy
         c = e2.counters()
@@ -281,7 +283,8 @@ def run_ours(args, rank, world, local_rank):
                        "ene_tol": args.ene_tol, "iterations": fast["iters"], "energy": fast["energy"],
                        "precision": ("plain FP64" if args.precision == "fp64" else
                                      "mixed: incremental split-BF16 tcgen05 K, FP64 J/DIIS, occupied-subspace "
-                                     "refinement between full eigensolves, final FP64 Fock build"),
+                                     "refinement between full eigensolves, CUDA-graph iterations from the DIIS start, "
+                                     "final FP64 Fock build"),
                        "density_per_solve": {"full_eigensolves": fast["eigensolves"],
                                              "refinement_steps": fast["refine_steps"]},
                        "plain_fp64": {"s": ms_plain * 1e-3, "iterations": plain["iters"], "energy": plain["energy"]},

@@ -126,6 +126,14 @@ TINYSCF_API int TinySCF_set_k_precision(TinySCF_t t, int mode);
 #define TINYSCF_DENSITY_EIG    0
 #define TINYSCF_DENSITY_REFINE 1
 TINYSCF_API int TinySCF_set_density_solver(TinySCF_t t, int mode);
+/* CUDA-graph SCF iterations. With on = 1, TinySCF_do_SCF captures one
+ * iteration once DIIS is active (iteration 2 on) into a CUDA graph: J, K,
+ * Fock and energy, DIIS and, with TINYSCF_DENSITY_REFINE, the density with its
+ * refinement loop as a device-controlled conditional (WHILE) node; each later
+ * iteration is one graph launch. The full eigensolve of TINYSCF_DENSITY_EIG
+ * (and the refinement's fallback) runs outside the graph. The graph is
+ * recaptured when the K precision or density solver changes. */
+TINYSCF_API int TinySCF_set_graph(TinySCF_t t, int on);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

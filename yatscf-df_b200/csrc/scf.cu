@@ -265,43 +265,120 @@ static void inv_sqrt_ns(const double *M, double *Y, double *Z, double *T, double
     }
 }
 
-int subspace_refine(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n, int o,
-                    SubspaceWork &w, double tol, int max_steps, int *steps_out, double *res_out, cudaStream_t s)
+// res = max|R|, R = (I - U^T U) F' U^T; UA = U F' U^T
+static void refine_residual(const double *d_Fp, const double *d_U, int n, int o, SubspaceWork &w, cudaStream_t s)
+{
+    dgemm(false, true, n, o, n, 1.0, d_Fp, n, d_U, n, 0.0, w.A, o, s);          // A = F' U^T (n x o)
+    dgemm(false, false, o, o, n, 1.0, d_U, n, w.A, o, 0.0, w.UA, o, s);        // UA = U F' U^T
+    dgemm(true, false, n, o, o, 1.0, d_U, n, w.UA, o, 0.0, w.R, o, s);         // R = U^T UA
+    k_sub<<<(unsigned) (((size_t) n * o + 255) / 256), 256, 0, s>>>(w.A, w.R, (size_t) n * o);   // R = A - R
+    cudaMemsetAsync(w.res, 0, sizeof(double), s);
+    k_absmax<<<148, 256, 0, s>>>(w.R, (size_t) n * o, w.res);
+    g_launches += 2;
+}
+
+// one preconditioned step on U followed by Loewdin re-orthonormalisation
+static void refine_update(const double *d_Vstale, const double *d_wstale, double *d_U, int n, int o, SubspaceWork &w,
+                          cudaStream_t s)
 {
     const int v = n - o;
     const double *Vv = d_Vstale + (size_t) o * n;
     const double *wv = d_wstale + o;
+    dgemm(false, false, v, o, n, 1.0, Vv, n, w.R, o, 0.0, w.Cv, o, s);        // Cv = Vv R
+    k_precond<<<(unsigned) (((size_t) v * o + 255) / 256), 256, 0, s>>>(w.Cv, w.UA, wv, v, o);
+    dgemm(true, false, n, o, v, 1.0, Vv, n, w.Cv, o, 0.0, w.A, o, s);         // A = Vv^T Cv (n x o)
+    k_add_transposed<<<(unsigned) (((size_t) o * n + 255) / 256), 256, 0, s>>>(d_U, w.A, o, n);
+    dgemm(false, true, o, o, n, 1.0, d_U, n, d_U, n, 0.0, w.M, o, s);         // M = U U^T
+    inv_sqrt_ns(w.M, w.Y, w.Z, w.T, w.W, o, 5, s);                              // Z = M^-1/2
+    dgemm(false, false, o, n, o, 1.0, w.Z, o, d_U, n, 0.0, w.A, n, s);        // U = Z U
+    cudaMemcpyAsync(d_U, w.A, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, s);
+    g_launches += 2;
+}
+
+// Stop rule shared by the host loop and the graph's device-side loop: stop when
+// converged, when the first residual shows F' far from the last subspace, or
+// when the observed contraction cannot reach tol within the steps left.
+__host__ __device__ inline bool refine_continue(double res, double prev, int step, int max_steps, double tol)
+{
+    if (res < tol || step >= max_steps) return false;
+    if (step == 0) return res <= 5e-2;
+    return res * pow(res / prev, max_steps - step) <= tol;
+}
+
+int subspace_refine(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n, int o,
+                    SubspaceWork &w, double tol, int max_steps, int *steps_out, double *res_out, cudaStream_t s)
+{
     double res = 1e300, prev = 1e300;
     int step = 0;
-    for (; step < max_steps; step++) {
-        dgemm(false, true, n, o, n, 1.0, d_Fp, n, d_U, n, 0.0, w.A, o, s);          // A = F' U^T (n x o)
-        dgemm(false, false, o, o, n, 1.0, d_U, n, w.A, o, 0.0, w.UA, o, s);        // UA = U F' U^T
-        dgemm(true, false, n, o, o, 1.0, d_U, n, w.UA, o, 0.0, w.R, o, s);         // R = U^T UA
-        k_sub<<<(unsigned) (((size_t) n * o + 255) / 256), 256, 0, s>>>(w.A, w.R, (size_t) n * o);   // R = A - R
-        cudaMemsetAsync(w.res, 0, sizeof(double), s);
-        k_absmax<<<148, 256, 0, s>>>(w.R, (size_t) n * o, w.res);
-        g_launches += 2;
+    for (;; step++) {
+        refine_residual(d_Fp, d_U, n, o, w, s);
         cudaMemcpyAsync(&res, w.res, sizeof(double), cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) return ERR_CUDA;
-        if (res < tol) break;
-        // far from the last subspace, or contracting too slowly to reach tol in
-        // the steps left: leave it to a full eigensolve
-        if (step == 0 && res > 5e-2) break;
-        if (step > 0 && res * pow(res / prev, max_steps - step) > tol) break;
+        if (!refine_continue(res, prev, step, max_steps, tol)) break;
         prev = res;
-        dgemm(false, false, v, o, n, 1.0, Vv, n, w.R, o, 0.0, w.Cv, o, s);        // Cv = Vv R
-        k_precond<<<(unsigned) (((size_t) v * o + 255) / 256), 256, 0, s>>>(w.Cv, w.UA, wv, v, o);
-        dgemm(true, false, n, o, v, 1.0, Vv, n, w.Cv, o, 0.0, w.A, o, s);         // A = Vv^T Cv (n x o)
-        k_add_transposed<<<(unsigned) (((size_t) o * n + 255) / 256), 256, 0, s>>>(d_U, w.A, o, n);
-        dgemm(false, true, o, o, n, 1.0, d_U, n, d_U, n, 0.0, w.M, o, s);         // M = U U^T
-        inv_sqrt_ns(w.M, w.Y, w.Z, w.T, w.W, o, 8, s);                              // Z = M^-1/2
-        dgemm(false, false, o, n, o, 1.0, w.Z, o, d_U, n, 0.0, w.A, n, s);        // U = Z U
-        cudaMemcpyAsync(d_U, w.A, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, s);
-        g_launches += 2;
+        refine_update(d_Vstale, d_wstale, d_U, n, o, w, s);
     }
     *steps_out = step;
     *res_out = res;
     return OK;
+}
+
+// Device-side loop control for the captured iteration: reads the residual the
+// preceding kernels produced and sets the WHILE node's condition.
+__global__ void k_refine_decide(RefineCtl *c, const double *res, cudaGraphConditionalHandle h, int first)
+{
+    const double r = *res;
+    if (first) {
+        c->step = 0;
+        c->prev = 1e300;
+    } else {
+        c->step++;
+    }
+    c->res = r;
+    c->converged = r < c->tol;
+    const bool cont = refine_continue(r, c->prev, c->step, c->max_steps, c->tol);
+    c->prev = r;
+    cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+int subspace_refine_capture(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n,
+                            int o, SubspaceWork &w, RefineCtl *d_ctl, cudaStream_t s, cudaStream_t s_body,
+                            long long *body_launches)
+{
+    refine_residual(d_Fp, d_U, n, o, w, s);
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps) != cudaSuccess || st != cudaStreamCaptureStatusActive)
+        return ERR_CUDA;
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return ERR_CUDA;
+    k_refine_decide<<<1, 1, 0, s>>>(d_ctl, w.res, h, 1);
+    g_launches++;
+    if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps) != cudaSuccess) return ERR_CUDA;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, deps, ndeps, &cp) != cudaSuccess) return ERR_CUDA;
+    if (cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+        return ERR_CUDA;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(s_body, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+        return ERR_CUDA;
+    const long long l0 = g_launches;
+    refine_update(d_Vstale, d_wstale, d_U, n, o, w, s_body);
+    refine_residual(d_Fp, d_U, n, o, w, s_body);
+    k_refine_decide<<<1, 1, 0, s_body>>>(d_ctl, w.res, h, 0);
+    g_launches++;
+    *body_launches = g_launches - l0;
+    g_launches = l0;
+    cudaGraph_t out = nullptr;
+    if (cudaStreamEndCapture(s_body, &out) != cudaSuccess) return ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA;
 }
 
 // Cocc = X U^T (U: occupied rows in the orthogonal basis), D = Cocc Cocc^T

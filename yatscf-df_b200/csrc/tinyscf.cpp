@@ -295,6 +295,18 @@ struct Engine {
     bool have_eig = false;        // V, w hold a full eigensolve of an earlier F'
     SubspaceWork sw{};
     long long n_eig = 0, n_refine = 0;
+    // CUDA-graph iteration (Fock, DIIS and, with the refinement solver, the density)
+    bool use_graph = false;
+    bool capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_key = -1;
+    bool gev_used[TINYSCF_T_COUNT];
+    long long g_top = 0, g_body = 0;  // kernels per launch outside / per step inside the refinement loop
+    cudaStream_t s_body = nullptr;
+    RefineCtl *rctl = nullptr;        // device
+    RefineCtl *h_rctl = nullptr;      // pinned host copy written by the graph
+    double *h_E = nullptr;            // pinned host copy of the energy written by the graph
     KMix *kmix = nullptr;
     double *Kmix = nullptr;
     int stage = 0;            // 1 hcore, 2 schwarz, 3 sparsity, 4 guess, 5 df
@@ -361,14 +373,22 @@ int upload(Engine *e, T **p, const std::vector<T> &v)
     return OK;
 }
 
+// Inside a stream capture the timer events become event-record nodes of the
+// graph, so each graph launch times its phases like an eager iteration.
 void tstart(Engine *e, int k)
 {
-    cudaEventRecord(e->ev0[k], e->s);
+    if (e->capturing) cudaEventRecordWithFlags(e->ev0[k], e->s, cudaEventRecordExternal);
+    else cudaEventRecord(e->ev0[k], e->s);
 }
 void tstop(Engine *e, int k)
 {
-    cudaEventRecord(e->ev1[k], e->s);
-    e->ev_used[k] = true;
+    if (e->capturing) {
+        cudaEventRecordWithFlags(e->ev1[k], e->s, cudaEventRecordExternal);
+        e->gev_used[k] = true;
+    } else {
+        cudaEventRecord(e->ev1[k], e->s);
+        e->ev_used[k] = true;
+    }
 }
 void tcollect(Engine *e)
 {
@@ -1014,6 +1034,113 @@ int sync_host_impl(TinySCF_t t)
     return cuda_rc("sync to host");
 }
 
+// ------------------------------------------------------------------ CUDA-graph iteration
+void graph_release(Engine *e)
+{
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->gexec = nullptr;
+    e->graph = nullptr;
+    e->graph_key = -1;
+}
+
+// Capture one SCF iteration past the DIIS start (t->iter >= 2): J, K (FP64 or
+// mixed), Fock + energy, DIIS, and with the refinement solver the density with
+// its step loop as a device-controlled WHILE node. The full-eigensolve density
+// stays outside the graph (the eigensolver library is not captured).
+int graph_capture(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    const int n = t->nbasfuncs, o = t->n_occ;
+    graph_release(e);
+    if (!e->s_body) TSCF_CUDA_CHECK(cudaStreamCreateWithFlags(&e->s_body, cudaStreamNonBlocking));
+    if (!e->h_rctl) {
+        TSCF_CUDA_CHECK(cudaMallocHost(&e->h_rctl, sizeof(RefineCtl)));
+        TSCF_CUDA_CHECK(cudaMallocHost(&e->h_E, sizeof(double)));
+        RC(dalloc(e, &e->rctl, 1));
+    }
+    const bool refine = e->dmode == TINYSCF_DENSITY_REFINE && o > 0 && o < n;
+    if (refine) {
+        RefineCtl c{};
+        c.tol = kRefineTol;
+        c.max_steps = kRefineSteps;
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(e->rctl, &c, sizeof(c), cudaMemcpyHostToDevice, e->s));
+        TSCF_CUDA_CHECK(cudaStreamSynchronize(e->s));
+    }
+    for (int k = 0; k < TINYSCF_T_COUNT; k++) e->gev_used[k] = false;
+    TSCF_CUDA_CHECK(cudaStreamBeginCapture(e->s, cudaStreamCaptureModeRelaxed));
+    e->capturing = true;
+    const long long l0 = g_launches;
+    int rc = fock_device(t);
+    if (!rc) rc = diis_device(t);
+    if (!rc && refine) {
+        tstart(e, TINYSCF_T_DENSITY);
+        rc = subspace_refine_capture(e->Fp, e->V, e->w, e->U, n, o, e->sw, e->rctl, e->s, e->s_body, &e->g_body);
+        if (!rc) {
+            density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, e->s);
+            cudaMemcpyAsync(e->h_rctl, e->rctl, sizeof(RefineCtl), cudaMemcpyDeviceToHost, e->s);
+        }
+        tstop(e, TINYSCF_T_DENSITY);
+    }
+    if (!rc) cudaMemcpyAsync(e->h_E, e->E, sizeof(double), cudaMemcpyDeviceToHost, e->s);
+    e->g_top = g_launches - l0;
+    g_launches = l0;
+    e->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(e->s, &g);
+    if (rc || ce != cudaSuccess) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        fprintf(stderr, "[tinyscf] capture of the SCF iteration failed: %s\n",
+                ce != cudaSuccess ? cudaGetErrorString(ce) : TinySCF_status_string(rc));
+        return rc ? rc : ERR_CUDA;
+    }
+    e->graph = g;
+    TSCF_CUDA_CHECK(cudaGraphInstantiate(&e->gexec, g, 0));
+    e->graph_key = e->kprec * 2 + e->dmode;
+    return OK;
+}
+
+// One SCF iteration (t->iter >= 2) through the captured graph; E receives the
+// energy. Falls back to a full eigensolve when the refinement loop stopped
+// without converging.
+int graph_iteration(TinySCF_t t, double *E)
+{
+    Engine *e = E_(t);
+    const int n = t->nbasfuncs, o = t->n_occ;
+    if (!e->gexec || e->graph_key != e->kprec * 2 + e->dmode) RC(graph_capture(t));
+    const bool refine = e->dmode == TINYSCF_DENSITY_REFINE && o > 0 && o < n;
+    cudaEventRecord(e->ev0[TINYSCF_T_ITER], e->s);
+    TSCF_CUDA_CHECK(cudaGraphLaunch(e->gexec, e->s));
+    for (int k = 0; k < TINYSCF_T_COUNT; k++)
+        if (e->gev_used[k]) e->ev_used[k] = true;
+    e->F_is_orth = true;
+    if (!refine) {
+        RC(density_device(t));
+    } else {
+        TSCF_CUDA_CHECK(cudaStreamSynchronize(e->s));
+        const RefineCtl c = *e->h_rctl;
+        e->n_refine += c.step;
+        g_launches += e->g_body * c.step;
+        if (!c.converged) {
+            // same as the eager solver's fallback: full eigensolve of this F'
+            // (the DENSITY timer keeps the start the graph recorded)
+            RC(eig_run(e->eig, e->Fp, e->w, e->V, e->s));
+            density_from_eig(e->X, e->V, e->Cocc, e->D, n, o, e->s);
+            TSCF_CUDA_CHECK(cudaMemcpyAsync(e->U, e->V, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, e->s));
+            e->n_eig++;
+            tstop(e, TINYSCF_T_DENSITY);
+        }
+    }
+    g_launches += e->g_top;
+    cudaEventRecord(e->ev1[TINYSCF_T_ITER], e->s);
+    e->ev_used[TINYSCF_T_ITER] = true;
+    RC(sync_rc(e, "SCF iteration (graph)"));
+    *E = *e->h_E;
+    e->d2h += (long long) sizeof(double);
+    return OK;
+}
+
 // ------------------------------------------------------------------ SCF loop (TinySCF.c:378-435)
 int scf_impl(TinySCF_t t)
 {
@@ -1031,15 +1158,19 @@ int scf_impl(TinySCF_t t)
     double prev_energy = 0, energy_delta = 223;
     while ((t->iter < t->niters) && (energy_delta >= t->ene_tol)) {
         if (t->verbose) printf("--------------- Iteration %d ---------------\n", t->iter);
-        tstart(e, TINYSCF_T_ITER);
-        RC(fock_device(t));
-        RC(diis_device(t));
-        RC(density_device(t));
-        tstop(e, TINYSCF_T_ITER);
         double E = 0.0;
-        TSCF_CUDA_CHECK(cudaMemcpyAsync(&E, e->E, sizeof(double), cudaMemcpyDeviceToHost, e->s));
-        e->d2h += (long long) sizeof(double);
-        RC(sync_rc(e, "SCF iteration"));
+        if (e->use_graph && t->iter >= 2) {
+            RC(graph_iteration(t, &E));
+        } else {
+            tstart(e, TINYSCF_T_ITER);
+            RC(fock_device(t));
+            RC(diis_device(t));
+            RC(density_device(t));
+            tstop(e, TINYSCF_T_ITER);
+            TSCF_CUDA_CHECK(cudaMemcpyAsync(&E, e->E, sizeof(double), cudaMemcpyDeviceToHost, e->s));
+            e->d2h += (long long) sizeof(double);
+            RC(sync_rc(e, "SCF iteration"));
+        }
         tcollect(e);
         t->HF_energy = E;
         energy_delta = fabs(t->HF_energy - prev_energy);
@@ -1100,6 +1231,10 @@ void free_impl(TinySCF_t t)
     Engine *e = E_(t);
     if (e) {
         if (e->s) cudaStreamSynchronize(e->s);
+        graph_release(e);
+        if (e->s_body) cudaStreamDestroy(e->s_body);
+        if (e->h_rctl) cudaFreeHost(e->h_rctl);
+        if (e->h_E) cudaFreeHost(e->h_E);
         eig_destroy(e->eig);
         kmix_destroy(e->kmix);
         for (void *p : e->allocs) cudaFree(p);
@@ -1274,6 +1409,19 @@ int TinySCF_set_density_solver(TinySCF_t t, int mode)
     }
     e->dmode = mode;
     e->have_eig = false;
+    return TINYSCF_OK;
+}
+
+int TinySCF_set_graph(TinySCF_t t, int on)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (on != 0 && on != 1) return TINYSCF_ERR_INPUT;
+    if (!on) {
+        cudaStreamSynchronize(e->s);
+        graph_release(e);
+    }
+    e->use_graph = on != 0;
     return TINYSCF_OK;
 }
 

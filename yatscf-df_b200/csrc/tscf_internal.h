@@ -178,6 +178,16 @@ struct SubspaceWork {
 };
 int subspace_refine(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n, int o,
                     SubspaceWork &w, double tol, int max_steps, int *steps_out, double *res_out, cudaStream_t s);
+// Refinement inside a stream capture: the steps run in a WHILE conditional
+// node whose condition a device kernel sets from the residual. d_ctl->tol and
+// ->max_steps are inputs; ->step, ->res and ->converged are written.
+struct RefineCtl {
+    double res, prev, tol;
+    int step, max_steps, converged;
+};
+int subspace_refine_capture(const double *d_Fp, const double *d_Vstale, const double *d_wstale, double *d_U, int n,
+                            int o, SubspaceWork &w, RefineCtl *d_ctl, cudaStream_t s, cudaStream_t s_body,
+                            long long *body_launches);
 void density_from_rows(const double *d_X, const double *d_U, double *d_Cocc, double *d_D, int n, int nocc,
                        cudaStream_t s);
 // Cocc = X * V[0:nocc]^T (eigenvectors in rows), D = Cocc Cocc^T.

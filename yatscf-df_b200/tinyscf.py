@@ -101,6 +101,7 @@ def load_library(path=LIBPATH):
         "TinySCF_reset_scf": ([T], ip),
         "TinySCF_set_k_precision": ([T, ip], ip),
         "TinySCF_set_density_solver": ([T, ip], ip),
+        "TinySCF_set_graph": ([T, ip], ip),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -226,6 +227,12 @@ class TinySCF:
         rc = self.lib.TinySCF_set_density_solver(self.t, int(mode))
         if rc:
             raise TinySCFError("set_density_solver: " + STATUS.get(rc, str(rc)))
+
+    def set_graph(self, on):
+        """Run SCF iterations from the DIIS start as CUDA-graph launches."""
+        rc = self.lib.TinySCF_set_graph(self.t, int(bool(on)))
+        if rc:
+            raise TinySCFError("set_graph: " + STATUS.get(rc, str(rc)))
 
     def reset_scf(self):
         rc = self.lib.TinySCF_reset_scf(self.t)
