@@ -134,6 +134,40 @@ TINYSCF_API int TinySCF_set_density_solver(TinySCF_t t, int mode);
  * (and the refinement's fallback) runs outside the graph. The graph is
  * recaptured when the K precision or density solver changes. */
 TINYSCF_API int TinySCF_set_graph(TinySCF_t t, int on);
+/* Initial guess. TINYSCF_GUESS_SAD (default): the reference's superposition
+ * of atomic densities with its pivoted-Cholesky Cocc (TinySCF.c:282-364).
+ * TINYSCF_GUESS_LEARNED: atom-pair density blocks predicted by the MLPs in the
+ * weights file (block types: diagonal H / C,N,O; off-diagonal pairs closer
+ * than 4 A), assembled and projected onto the idempotent density of the n_occ
+ * leading natural orbitals; molecules with other elements or shell layouts
+ * fall back to SAD. weights may be NULL to keep a loaded network. Takes effect
+ * at the next TinySCF_get_initial_guess / TinySCF_reset_scf. */
+#define TINYSCF_GUESS_SAD     0
+#define TINYSCF_GUESS_LEARNED 1
+/* The SAD density put through the same projection as the learned one (the
+ * ablation that isolates what the network adds). */
+#define TINYSCF_GUESS_SAD_PROJECTED 2
+TINYSCF_API int TinySCF_set_guess(TinySCF_t t, int mode, const char *weights);
+/* Which guess the last TinySCF_get_initial_guess used (or -status). */
+TINYSCF_API int TinySCF_guess_used(TinySCF_t t);
+/* Training data from a density D (host, nbf x nbf, e.g. a converged one):
+ * for every atom pair of the molecule its 128 features, its target block in
+ * the pair's local frame (225 floats, row-major nf_a x nf_b) and its block
+ * type. With feat == NULL returns the number of pairs; else fills up to cap
+ * pairs and returns the count (negative status on error). */
+TINYSCF_API long long TinySCF_guess_dataset(TinySCF_t t, const double *D, float *feat, float *target, int *type,
+                                            long long cap);
+/* Train the five block-type MLPs (128-192-192-out, SiLU) with Adam on the GPU
+ * from host arrays as TinySCF_guess_dataset writes them and save the weights
+ * file at path; final_loss (5 floats) receives each type's last-epoch MSE in
+ * normalised units. */
+TINYSCF_API int TinySCF_guess_train(const float *feat, const float *target, const int *type, long long n, int epochs,
+                                    int batch, float lr, unsigned seed, const char *path, float *final_loss);
+/* Mean-squared-error loss and its gradient for one MLP (parameters laid out
+ * W1[din][hid], b1, W2[hid][hid], b2, W3[hid][dout], b3) on n rows, computed
+ * by the training kernels: host in, host out. */
+TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *params, const float *X, const float *T,
+                                       int n, float *grad, float *loss);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

@@ -23,6 +23,7 @@
 #include "build_density.h"
 #include "tinyscf_b200.h"
 #include "tscf_internal.h"
+#include "guess.h"
 
 using namespace tscf;
 
@@ -307,6 +308,10 @@ struct Engine {
     RefineCtl *rctl = nullptr;        // device
     RefineCtl *h_rctl = nullptr;      // pinned host copy written by the graph
     double *h_E = nullptr;            // pinned host copy of the energy written by the graph
+    // learned initial guess
+    int guess_mode = TINYSCF_GUESS_SAD;
+    int guess_used = TINYSCF_GUESS_SAD;
+    GuessNet *gnet = nullptr;
     KMix *kmix = nullptr;
     double *Kmix = nullptr;
     int stage = 0;            // 1 hcore, 2 schwarz, 3 sparsity, 4 guess, 5 df
@@ -783,12 +788,11 @@ int sparsity_impl(TinySCF_t t)
 }
 
 // ------------------------------------------------------------------ guess (TinySCF.c:282-364)
-int guess_impl(TinySCF_t t)
+// SAD density (TinySCF.c:324-364): atomic blocks from the .dat files, scaled
+// by 0.5 (and by the charge factor for ions).
+void sad_blocks(Engine *e, TinySCF_t t, std::vector<double> &D)
 {
-    Engine *e = E_(t);
-    if (!e) return ERR_STATE;
-    const int nbf = t->nbasfuncs, nocc = t->n_occ;
-    std::vector<double> D((size_t) nbf * nbf, 0.0);
+    const int nbf = t->nbasfuncs;
     for (int a = 0; a < t->natoms; a++) {
         int el = e->mol.eid[a];
         int b0 = e->sh.atom_bf0[a], b1 = e->sh.atom_bf1[a], nf = b1 - b0;
@@ -800,7 +804,80 @@ int guess_impl(TinySCF_t t)
     if (t->charge != 0 && t->electron != 0) R = (double) (t->electron - t->charge) / (double) t->electron;
     R *= 0.5;
     for (auto &v : D) v *= R;
-    tstart(e, TINYSCF_T_GUESS);
+}
+
+GuessAtoms guess_atoms(Engine *e)
+{
+    GuessAtoms g;
+    g.natoms = e->mol.natoms;
+    g.eid = e->mol.eid.data();
+    g.xyz = e->mol.xyz.data();
+    g.bf0 = e->sh.atom_bf0.data();
+    g.shell_am.assign(g.natoms, {});
+    for (int k = 0; k < e->sh.nsh; k++) g.shell_am[e->sh.atom_of[k]].push_back(e->sh.am[k]);
+    return g;
+}
+
+// Predicted density blocks, then the idempotent density closest in the
+// orthogonal basis: the n_occ leading eigenvectors U of S^1/2 D S^1/2
+// (S^1/2 = S X), Cocc = X U^T, D = Cocc Cocc^T. Returns ERR_UNSUPPORTED when
+// an atom is not covered by the network (the caller then uses SAD).
+int learned_guess(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    const int n = t->nbasfuncs, o = t->n_occ;
+    if (o <= 0 || o > n) return ERR_UNSUPPORTED;
+    tstart(e, TINYSCF_T_GUESS);   // the timer spans the host-side features too
+    std::vector<GuessPair> pairs;
+    if (e->guess_mode == TINYSCF_GUESS_LEARNED) {
+        GuessAtoms g = guess_atoms(e);
+        if (guess_pairs(g, pairs)) return ERR_UNSUPPORTED;
+        RC(guessnet_predict(e->gnet, pairs, g, e->D, n, e->s));
+    } else {
+        std::vector<double> D((size_t) n * n, 0.0);
+        sad_blocks(e, t, D);
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(e->D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, e->s));
+        e->h2d += (long long) (sizeof(double) * D.size());
+    }
+    dgemm(false, false, n, n, n, 1.0, e->S, n, e->X, n, 0.0, e->tmp, n, e->s);      // S^1/2
+    dgemm(false, false, n, n, n, 1.0, e->tmp, n, e->D, n, 0.0, e->tmp2, n, e->s);
+    dgemm(false, false, n, n, n, 1.0, e->tmp2, n, e->tmp, n, 0.0, e->F, n, e->s);   // S^1/2 D S^1/2
+    RC(eig_run(e->eig, e->F, e->w, e->V, e->s));
+    density_from_eig(e->X, e->V + (size_t) (n - o) * n, e->Cocc, e->D, n, o, e->s);
+    tstop(e, TINYSCF_T_GUESS);
+    RC(cuda_rc("learned initial guess"));
+    RC(sync_rc(e, "learned initial guess"));
+    tcollect(e);
+    d2h(e, t->D_mat, e->D, sizeof(double) * e->nn);
+    d2h(e, t->Cocc_mat, e->Cocc, sizeof(double) * n * o);
+    if (t->verbose)
+        printf("TinySCF %s initial guess: %zu atom-pair blocks, %.3lf (s)\n",
+               e->guess_mode == TINYSCF_GUESS_LEARNED ? "learned" : "projected SAD", pairs.size(),
+               e->timers[TINYSCF_T_GUESS] * 1e-3);
+    return OK;
+}
+
+int guess_impl(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!e) return ERR_STATE;
+    const int nbf = t->nbasfuncs, nocc = t->n_occ;
+    e->have_eig = false;
+    if ((e->guess_mode == TINYSCF_GUESS_LEARNED && e->gnet && e->stage >= 1) ||
+        (e->guess_mode == TINYSCF_GUESS_SAD_PROJECTED && e->stage >= 1)) {
+        int rc = learned_guess(t);
+        if (rc == OK) {
+            e->guess_used = e->guess_mode;
+            e->stage = std::max(e->stage, 4);
+            return OK;
+        }
+        if (rc != ERR_UNSUPPORTED) return rc;
+        if (t->verbose) printf("TinySCF learned initial guess: an atom is not covered, using SAD\n");
+    }
+    e->guess_used = TINYSCF_GUESS_SAD;
+    tstart(e, TINYSCF_T_GUESS);   // the timer spans reading the SAD blocks too
+    std::vector<double> D((size_t) nbf * nbf, 0.0);
+    sad_blocks(e, t, D);
     TSCF_CUDA_CHECK(cudaMemcpyAsync(e->D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, e->s));
     e->h2d += (long long) (sizeof(double) * D.size());
     TSCF_CUDA_CHECK(cudaMemcpyAsync(e->tmp, e->D, sizeof(double) * D.size(), cudaMemcpyDeviceToDevice, e->s));
@@ -1235,6 +1312,7 @@ void free_impl(TinySCF_t t)
         if (e->s_body) cudaStreamDestroy(e->s_body);
         if (e->h_rctl) cudaFreeHost(e->h_rctl);
         if (e->h_E) cudaFreeHost(e->h_E);
+        guessnet_free(e->gnet);
         eig_destroy(e->eig);
         kmix_destroy(e->kmix);
         for (void *p : e->allocs) cudaFree(p);
@@ -1423,6 +1501,77 @@ int TinySCF_set_graph(TinySCF_t t, int on)
     }
     e->use_graph = on != 0;
     return TINYSCF_OK;
+}
+
+int TinySCF_set_guess(TinySCF_t t, int mode, const char *weights)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (mode != TINYSCF_GUESS_SAD && mode != TINYSCF_GUESS_LEARNED && mode != TINYSCF_GUESS_SAD_PROJECTED)
+        return TINYSCF_ERR_INPUT;
+    if (weights) {
+        GuessNet *net = nullptr;
+        int rc = guessnet_load(&net, weights);
+        if (rc) {
+            fprintf(stderr, "[tinyscf] cannot load guess network weights from %s: %s\n", weights,
+                    TinySCF_status_string(rc));
+            return rc;
+        }
+        guessnet_free(e->gnet);
+        e->gnet = net;
+    }
+    if (mode == TINYSCF_GUESS_LEARNED && !e->gnet) return TINYSCF_ERR_STATE;
+    e->guess_mode = mode;
+    return TINYSCF_OK;
+}
+
+int TinySCF_guess_used(TinySCF_t t)
+{
+    if (!t || !t->dev) return -TINYSCF_ERR_STATE;
+    return E_(t)->guess_used;
+}
+
+long long TinySCF_guess_dataset(TinySCF_t t, const double *D, float *feat, float *target, int *type, long long cap)
+{
+    if (!t || !t->dev || !D) return -TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    GuessAtoms g = guess_atoms(e);
+    std::vector<GuessPair> pairs;
+    if (guess_pairs(g, pairs)) return -TINYSCF_ERR_UNSUPPORTED;
+    if (!feat) return (long long) pairs.size();
+    if ((long long) pairs.size() > cap) return -TINYSCF_ERR_INPUT;
+    for (size_t k = 0; k < pairs.size(); k++) {
+        std::memcpy(feat + k * G_DIN, pairs[k].feat, sizeof(float) * G_DIN);
+        float *o = target + k * G_MAXF * G_MAXF;
+        std::memset(o, 0, sizeof(float) * G_MAXF * G_MAXF);
+        guess_local_block(g, pairs[k], D, t->nbasfuncs, o);
+        type[k] = pairs[k].type;
+    }
+    return (long long) pairs.size();
+}
+
+int TinySCF_guess_train(const float *feat, const float *target, const int *type, long long n, int epochs, int batch,
+                        float lr, unsigned seed, const char *path, float *final_loss)
+{
+    if (!feat || !target || !type || n <= 0 || epochs <= 0 || batch <= 0 || !path) return TINYSCF_ERR_INPUT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return TINYSCF_ERR_CUDA;
+    }
+    return guessnet_train(feat, target, type, n, epochs, batch, lr, seed, path, final_loss);
+}
+
+int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *params, const float *X, const float *T, int n,
+                           float *grad, float *loss)
+{
+    if (!params || !X || !T || !grad || !loss || din <= 0 || hid <= 0 || dout <= 0 || n <= 0) return TINYSCF_ERR_INPUT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return TINYSCF_ERR_CUDA;
+    }
+    return guessnet_grad(din, hid, dout, params, X, T, n, grad, loss);
 }
 
 int TinySCF_reset_scf(TinySCF_t t)

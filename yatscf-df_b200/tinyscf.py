@@ -20,6 +20,9 @@ TIMERS = ["HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM", "J", "K_
           "FOCK", "DIIS", "DENSITY", "ITER", "SCF", "K_MIXED", "FINAL"]
 K_FP64, K_MIXED = 0, 1
 DENSITY_EIG, DENSITY_REFINE = 0, 1
+GUESS_SAD, GUESS_LEARNED, GUESS_SAD_PROJECTED = 0, 1, 2
+GUESS_DIN, GUESS_MAXF = 128, 15
+GUESS_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "guess_weights.bin")
 STATUS = {0: "success", 1: "CUDA error", 2: "cannot open input file", 3: "invalid input",
           4: "unsupported input", 5: "device allocation failed", 6: "numerical failure",
           7: "call out of order"}
@@ -75,6 +78,7 @@ def load_library(path=LIBPATH):
     lib = ctypes.CDLL(path)
     T = TinySCF_t
     cp, dp, ip = ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
+    fp = ctypes.POINTER(ctypes.c_float)
     sig = {
         "TinySCF_alloc": ([], T),
         "TinySCF_status_string": ([ip], ctypes.c_char_p),
@@ -102,6 +106,12 @@ def load_library(path=LIBPATH):
         "TinySCF_set_k_precision": ([T, ip], ip),
         "TinySCF_set_density_solver": ([T, ip], ip),
         "TinySCF_set_graph": ([T, ip], ip),
+        "TinySCF_set_guess": ([T, ip, ctypes.c_char_p], ip),
+        "TinySCF_guess_used": ([T], ip),
+        "TinySCF_guess_dataset": ([T, dp, fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong], ctypes.c_longlong),
+        "TinySCF_guess_train": ([fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ip, ip, ctypes.c_float,
+                                 ctypes.c_uint, ctypes.c_char_p, fp], ip),
+        "TinySCF_guess_mlp_grad": ([ip, ip, ip, fp, fp, fp, ip, fp, fp], ip),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -114,6 +124,39 @@ def load_library(path=LIBPATH):
 
 class TinySCFError(RuntimeError):
     pass
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def guess_train(feat, target, types, path, epochs=40, batch=512, lr=2e-3, seed=0):
+    """Train the guess networks on the GPU (the engine's kernels); returns the per-type final MSE."""
+    lib = load_library()
+    feat = np.ascontiguousarray(feat, dtype=np.float32)
+    target = np.ascontiguousarray(target, dtype=np.float32)
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    loss = np.zeros(5, dtype=np.float32)
+    rc = lib.TinySCF_guess_train(_fptr(feat), _fptr(target), types.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 len(types), epochs, batch, lr, seed, path.encode(), _fptr(loss))
+    if rc:
+        raise TinySCFError("guess_train: " + STATUS.get(rc, str(rc)))
+    return loss
+
+
+def guess_mlp_grad(params, X, T, din, hid, dout):
+    """(loss, gradient) of one guess MLP computed by the training kernels."""
+    lib = load_library()
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    g = np.zeros_like(params)
+    loss = np.zeros(1, dtype=np.float32)
+    rc = lib.TinySCF_guess_mlp_grad(din, hid, dout, _fptr(params), _fptr(X), _fptr(T), X.shape[0], _fptr(g),
+                                    _fptr(loss))
+    if rc:
+        raise TinySCFError("guess_mlp_grad: " + STATUS.get(rc, str(rc)))
+    return float(loss[0]), g
 
 
 def _dptr(a):
@@ -183,10 +226,13 @@ class TinySCF:
     def do_SCF(self):
         self._call("TinySCF_do_SCF")
 
-    def setup(self):
+    def setup(self, guess=None):
+        """main.c's set-up sequence; guess selects the initial guess (default: SAD)."""
         self.compute_Hcore_Ovlp_mat()
         self.compute_sq_Schwarz_scrvals()
         self.prepare_sparsity()
+        if guess is not None:
+            self.set_guess(guess)
         self.get_initial_guess()
         self.build_DF_tensor()
 
@@ -233,6 +279,32 @@ class TinySCF:
         rc = self.lib.TinySCF_set_graph(self.t, int(bool(on)))
         if rc:
             raise TinySCFError("set_graph: " + STATUS.get(rc, str(rc)))
+
+    def set_guess(self, mode, weights=None):
+        """GUESS_SAD (the reference's) or GUESS_LEARNED (weights file; default: the packaged one)."""
+        if mode == GUESS_LEARNED and weights is None:
+            weights = GUESS_WEIGHTS
+        rc = self.lib.TinySCF_set_guess(self.t, int(mode), None if weights is None else weights.encode())
+        if rc:
+            raise TinySCFError("set_guess: " + STATUS.get(rc, str(rc)))
+
+    def guess_used(self):
+        return int(self.lib.TinySCF_guess_used(self.t))
+
+    def guess_dataset(self, D):
+        """(features [n,128], local target blocks [n,225], block types [n]) for density D."""
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        n = self.lib.TinySCF_guess_dataset(self.t, _dptr(D), None, None, None, 0)
+        if n < 0:
+            raise TinySCFError("guess_dataset: " + STATUS.get(-n, str(-n)))
+        feat = np.zeros((n, GUESS_DIN), dtype=np.float32)
+        tgt = np.zeros((n, GUESS_MAXF * GUESS_MAXF), dtype=np.float32)
+        typ = np.zeros(n, dtype=np.int32)
+        got = self.lib.TinySCF_guess_dataset(self.t, _dptr(D), _fptr(feat), _fptr(tgt),
+                                            typ.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+        if got != n:
+            raise TinySCFError("guess_dataset: %d" % got)
+        return feat, tgt, typ
 
     def reset_scf(self):
         rc = self.lib.TinySCF_reset_scf(self.t)
