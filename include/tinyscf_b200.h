@@ -168,6 +168,22 @@ TINYSCF_API int TinySCF_guess_train(const float *feat, const float *target, cons
  * by the training kernels: host in, host out. */
 TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *params, const float *X, const float *T,
                                        int n, float *grad, float *loss);
+/* Batched SCF over many molecules of uneven size. Each molecule is a handle
+ * set up through the single-molecule calls (up to TinySCF_build_DF_tensor,
+ * any initial guess; FP64 exchange). TinySCF_batch_do_SCF then iterates all of
+ * them together: every SCF phase (J, K, Fock + energy, DIIS, density) is one
+ * launch over all molecules still iterating, the eigensolves one batched
+ * cuSOLVER call per group of equal basis size. Each molecule follows its own
+ * reference loop (ene_tol, niters, iteration count, DIIS history) and ends
+ * with its host mirrors filled as after TinySCF_do_SCF. The handles must stay
+ * alive until TinySCF_batch_free (which frees only the batch). */
+typedef struct TinySCF_batch_struct *TinySCF_batch_t;
+TINYSCF_API int TinySCF_batch_create(TinySCF_batch_t *out, TinySCF_t *mols, int nmol);
+TINYSCF_API int TinySCF_batch_do_SCF(TinySCF_batch_t b);
+/* Device time of the last TinySCF_batch_do_SCF (ms), its number of batched
+ * iterations (the slowest molecule's count) and the kernels it launched. */
+TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long long *launches);
+TINYSCF_API int TinySCF_batch_free(TinySCF_batch_t b);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

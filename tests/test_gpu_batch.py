@@ -1,0 +1,60 @@
+"""Batched SCF (one launch per phase over many molecules of uneven size)
+against the same molecules solved one by one: the same iteration counts,
+energies and densities."""
+import numpy as np
+import pytest
+
+import geometry
+import tinyscf
+from conftest import BAS, DFBAS, xyz
+
+pytestmark = pytest.mark.gpu
+
+
+def _molecules(tmp_path):
+    paths = [xyz("water"), xyz("c10h22")]
+    for seed in range(4):
+        p = str(tmp_path / ("w%d.xyz" % seed))
+        geometry.write_xyz(p, geometry.water_cluster(seed, nmax=6))
+        paths.append(p)
+    # the same cluster twice (rotated): two members of one eigensolver group
+    atoms = geometry.water_cluster(1, nmax=6)
+    q = np.array([0.2, 0.9, -0.3, 0.1])
+    q /= np.linalg.norm(q)
+    rot = np.array([a[1:] for a in atoms]) @ geometry._rotation(q).T
+    p = str(tmp_path / "w1r.xyz")
+    geometry.write_xyz(p, [(a[0], *map(float, r)) for a, r in zip(atoms, rot)])
+    paths.append(p)
+    return paths
+
+
+def _engine(p, guess=None, ene_tol=1e-10):
+    e = tinyscf.TinySCF(BAS, DFBAS, p, 60)
+    e.setup(guess=guess)
+    e.s.ene_tol = ene_tol
+    return e
+
+
+@pytest.mark.parametrize("guess", [None, tinyscf.GUESS_LEARNED])
+def test_batch_matches_single_molecule_scf(tmp_path, guess):
+    paths = _molecules(tmp_path)
+    single = []
+    for p in paths:
+        e = _engine(p, guess)
+        e.do_SCF()
+        single.append((e.energy, e.s.iter, e.mat("D_mat")))
+        e.free()
+    engines = [_engine(p, guess) for p in paths]
+    b = tinyscf.TinySCFBatch(engines)
+    b.do_SCF()
+    ms, iters, launches = b.stats()
+    for e, (E, it, D) in zip(engines, single):
+        assert e.s.iter == it, (e.s.iter, it)
+        assert abs(e.energy - E) < 1e-9, (e.energy, E)
+        assert np.abs(e.mat("D_mat") - D).max() < 1e-8
+    assert iters == max(s[1] for s in single)
+    # phases are batched: far fewer launches than one solve per molecule would need
+    assert launches < 80 * iters + 40 * len(paths), launches
+    b.free()
+    for e in engines:
+        e.free()

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 
+#include "tiles.cuh"
 #include "tscf_internal.h"
 
 namespace tscf {
@@ -25,30 +26,13 @@ __global__ void k_j_weights(const int *up_i, const int *up_j, const double *D, d
 }
 
 // Each block streams a contiguous range of upper rows and keeps its partial
-// t(P) for every column in registers: thread x owns columns x, x+512, ...
-constexpr int JT_THREADS = 512, JT_COLS = 16;   // naux <= 8192
+// t(P) for every column in registers (jt_rows).
 __global__ void __launch_bounds__(JT_THREADS) k_j_tpart(const double *__restrict__ B, const int *__restrict__ up_u,
                                                         const double *__restrict__ w, int nup, int naux, int rows_per_blk,
                                                         double *__restrict__ part)
 {
-    double acc[JT_COLS];
-#pragma unroll
-    for (int c = 0; c < JT_COLS; c++) acc[c] = 0.0;
     const int r0 = blockIdx.x * rows_per_blk, r1 = min(nup, r0 + rows_per_blk);
-    for (int r = r0; r < r1; r++) {
-        const double wr = w[r];
-        const double *row = B + (size_t) up_u[r] * naux;
-#pragma unroll
-        for (int c = 0; c < JT_COLS; c++) {
-            int p = threadIdx.x + c * JT_THREADS;
-            if (p < naux) acc[c] = fma(wr, __ldg(row + p), acc[c]);
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < JT_COLS; c++) {
-        int p = threadIdx.x + c * JT_THREADS;
-        if (p < naux) part[(size_t) blockIdx.x * naux + p] = acc[c];
-    }
+    jt_rows(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
 }
 
 __global__ void k_j_treduce(const double *part, int nblk, int naux, double *t)
@@ -103,61 +87,12 @@ void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, dou
 
 // ------------------------------------------------------------------ K, FP64
 // T[i][s][P]: block tile 64 (s) x 64 (P), K-step 16 rows of CSR row i.
-constexpr int KT_M = 64, KT_N = 64, KT_K = 16;
 __global__ void __launch_bounds__(256) k_halftransform(const double *__restrict__ B, const double *__restrict__ C,
                                                        const int *__restrict__ csr_j, const int *__restrict__ csr_u,
                                                        const int *__restrict__ displs, int nocc, int naux,
                                                        double *__restrict__ T)
 {
-    __shared__ double As[KT_K][KT_M + 1];
-    __shared__ double Bs[KT_K][KT_N + 1];
-    __shared__ int rj[KT_K], ru[KT_K];
-    const int i = blockIdx.z;
-    const int s0 = blockIdx.y * KT_M, p0 = blockIdx.x * KT_N;
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    const int r_beg = displs[i], r_end = displs[i + 1];
-    double acc[4][4] = {};
-    for (int r0 = r_beg; r0 < r_end; r0 += KT_K) {
-        if (tid < KT_K) {
-            int r = r0 + tid;
-            rj[tid] = (r < r_end) ? csr_j[r] : -1;
-            ru[tid] = (r < r_end) ? csr_u[r] : -1;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            int l = tid + 256 * q;
-            int kk = l / KT_M, c = l % KT_M;
-            int j = rj[kk], u = ru[kk];
-            int sg = s0 + c, pg = p0 + c;
-            As[kk][c] = (j >= 0 && sg < nocc) ? C[(size_t) j * nocc + sg] : 0.0;
-            Bs[kk][c] = (u >= 0 && pg < naux) ? B[(size_t) u * naux + pg] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < KT_K; kk++) {
-            double a[4], b[4];
-#pragma unroll
-            for (int x = 0; x < 4; x++) a[x] = As[kk][ty + 16 * x];
-#pragma unroll
-            for (int y = 0; y < 4; y++) b[y] = Bs[kk][tx + 16 * y];
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int x = 0; x < 4; x++) {
-        int sg = s0 + ty + 16 * x;
-        if (sg >= nocc) continue;
-#pragma unroll
-        for (int y = 0; y < 4; y++) {
-            int pg = p0 + tx + 16 * y;
-            if (pg < naux) T[((size_t) i * nocc + sg) * naux + pg] = acc[x][y];
-        }
-    }
+    half_tile(B, C, csr_j, csr_u, displs, nocc, naux, T, blockIdx.z, blockIdx.y * KT_M, blockIdx.x * KT_N);
 }
 
 // K partial tiles: upper tile pairs (bi <= bj) of 64x64, split over the
@@ -165,50 +100,10 @@ __global__ void __launch_bounds__(256) k_halftransform(const double *__restrict_
 __global__ void __launch_bounds__(256) k_syrk_part(const double *__restrict__ T, int nbf, long long Q, long long qchunk,
                                                    const int2 *__restrict__ tiles, double *__restrict__ Kpart)
 {
-    __shared__ double As[KT_K][KT_M + 1];
-    __shared__ double Bs[KT_K][KT_N + 1];
     const int2 tl = tiles[blockIdx.x];
     const int split = blockIdx.y;
-    const int i0 = tl.x * KT_M, j0 = tl.y * KT_N;
     const long long q_beg = (long long) split * qchunk, q_end = min(Q, q_beg + qchunk);
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    double acc[4][4] = {};
-    for (long long q0 = q_beg; q0 < q_end; q0 += KT_K) {
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-            int l = tid + 256 * r;
-            int row = l / KT_K, kk = l % KT_K;
-            long long q = q0 + kk;
-            int gi = i0 + row, gj = j0 + row;
-            As[kk][row] = (gi < nbf && q < q_end) ? T[(size_t) gi * Q + q] : 0.0;
-            Bs[kk][row] = (gj < nbf && q < q_end) ? T[(size_t) gj * Q + q] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < KT_K; kk++) {
-            double a[4], b[4];
-#pragma unroll
-            for (int x = 0; x < 4; x++) a[x] = As[kk][ty + 16 * x];
-#pragma unroll
-            for (int y = 0; y < 4; y++) b[y] = Bs[kk][tx + 16 * y];
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-        }
-        __syncthreads();
-    }
-    double *out = Kpart + (size_t) split * nbf * nbf;
-#pragma unroll
-    for (int x = 0; x < 4; x++) {
-        int gi = i0 + ty + 16 * x;
-        if (gi >= nbf) continue;
-#pragma unroll
-        for (int y = 0; y < 4; y++) {
-            int gj = j0 + tx + 16 * y;
-            if (gj < nbf) out[(size_t) gi * nbf + gj] = acc[x][y];
-        }
-    }
+    syrk_tile(T, nbf, Q, q_beg, q_end, tl.x * KT_M, tl.y * KT_N, Kpart + (size_t) split * nbf * nbf);
 }
 
 // K[i][j] = K[j][i] = sum_split Kpart[split][i][j] for i <= j (TinySCF keeps
@@ -253,22 +148,10 @@ void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_K
 __global__ void k_fock_energy(const double *H, const double *J, const double *K, const double *D, double *F,
                               double *epart, size_t n)
 {
-    __shared__ double sh[32];
-    double e = 0.0;
-    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x) {
-        double h = H[i];
-        double f = h + 2.0 * J[i] - K[i];
-        F[i] = f;
-        e += D[i] * (f + h);
-    }
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffff, e, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = e;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        e = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffff, e, o);
-        if (threadIdx.x == 0) epart[blockIdx.x] = e;
-    }
+    double e = fock_energy_range(H, J, K, D, F, (size_t) blockIdx.x * blockDim.x + threadIdx.x, n,
+                                 (size_t) gridDim.x * blockDim.x);
+    e = block_sum(e);
+    if (threadIdx.x == 0) epart[blockIdx.x] = e;
 }
 
 void build_F_energy(const double *d_H, const double *d_J, const double *d_K, const double *d_D, double *d_F,

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cusolverDn.h>
 
+#include "tiles.cuh"
 #include "tscf_internal.h"
 
 namespace tscf {
@@ -14,64 +15,12 @@ namespace tscf {
 long long g_launches = 0;
 
 // ------------------------------------------------------------------ DGEMM
-// 64x64 output tile per 256-thread block, 4x4 outputs per thread, K step 16.
-// op(A) is m x k, op(B) is k x n, everything row-major.
-constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
-
+// 64x64 output tile per 256-thread block (dgemm_tile).
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256) k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
                                                const double *__restrict__ B, int ldb, double beta, double *C, int ldc)
 {
-    __shared__ double As[GB_K][GB_M + 1];
-    __shared__ double Bs[GB_K][GB_N + 1];
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    const int m0 = blockIdx.y * GB_M, n0 = blockIdx.x * GB_N;
-    double acc[4][4] = {};
-    for (int k0 = 0; k0 < k; k0 += GB_K) {
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-            int l = tid + 256 * r;
-            int row, kk;
-            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / GB_M; row = l % GB_M; }
-            int gi = m0 + row, gk = k0 + kk;
-            double v = 0.0;
-            if (gi < m && gk < k) v = TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk];
-            As[kk][row] = v;
-            int col;
-            if (!TB) { kk = l / GB_N; col = l % GB_N; } else { col = l / GB_K; kk = l % GB_K; }
-            int gj = n0 + col;
-            gk = k0 + kk;
-            double w = 0.0;
-            if (gj < n && gk < k) w = TB ? B[(size_t) gj * ldb + gk] : B[(size_t) gk * ldb + gj];
-            Bs[kk][col] = w;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < GB_K; kk++) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        int gi = m0 + ty + 16 * i;
-        if (gi >= m) continue;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            int gj = n0 + tx + 16 * j;
-            if (gj >= n) continue;
-            double *c = C + (size_t) gi * ldc + gj;
-            *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * *c;
-        }
-    }
+    dgemm_tile<TA, TB>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, blockIdx.y * GB_M, blockIdx.x * GB_N);
 }
 
 void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda, const double *B, int ldb,

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 
+#include "batch.h"
 #include "tscf_internal.h"
 
 namespace tscf {
@@ -100,7 +101,7 @@ __global__ void k_diis_dots(const double *R, DiisState *st, size_t nn)
 // DIIS.c:76-110: update B, track the historically largest residual, and
 // solve the (len+1) bordered system by Gaussian elimination with partial
 // pivoting (first maximum, as LAPACK dgesv/idamax).
-__global__ void k_diis_solve(DiisState *st)
+__device__ void diis_solve_body(DiisState *st)
 {
     const int ld = MAXDIIS + 1;
     const int len = st->len, idx = st->idx;
@@ -148,6 +149,21 @@ __global__ void k_diis_solve(DiisState *st)
         b[i] = s / a[i * n + i];
     }
     for (int i = 0; i < n; i++) st->coef[i] = b[i];
+}
+
+__global__ void k_diis_solve(DiisState *st) { diis_solve_body(st); }
+
+// one thread per molecule of a batch
+__global__ void k_diis_solve_batched(const MolDev *mols, const int *active, int nmol)
+{
+    const int mol = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mol < nmol && active[mol]) diis_solve_body(mols[mol].diis);
+}
+
+void diis_solve_batched(const MolDev *d_mols, const int *d_active, int nmol, cudaStream_t s)
+{
+    g_launches++;
+    k_diis_solve_batched<<<(nmol + 63) / 64, 64, 0, s>>>(d_mols, d_active, nmol);
 }
 
 // F = sum_{i<len} coef_i F0_i (DIIS.c:112-122)

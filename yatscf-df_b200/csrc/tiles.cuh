@@ -1,0 +1,226 @@
+// Tile bodies shared by the single-molecule kernels and the batched
+// (many-molecule) kernels: the same arithmetic in the same order, so a batched
+// SCF reproduces the single-molecule one.
+#pragma once
+#include "tscf_internal.h"
+
+namespace tscf {
+
+// ---- FP64 GEMM tile: 64x64 outputs per 256 threads, 4x4 per thread, K step 16.
+// op(A) is m x k, op(B) is k x n, row-major; C = alpha op(A) op(B) + beta C.
+constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
+
+template <bool TA, bool TB>
+__device__ __forceinline__ void dgemm_tile(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
+                                           const double *__restrict__ B, int ldb, double beta, double *C, int ldc,
+                                           int m0, int n0)
+{
+    __shared__ double As[GB_K][GB_M + 1];
+    __shared__ double Bs[GB_K][GB_N + 1];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    double acc[4][4] = {};
+    for (int k0 = 0; k0 < k; k0 += GB_K) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            int l = tid + 256 * r;
+            int row, kk;
+            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / GB_M; row = l % GB_M; }
+            int gi = m0 + row, gk = k0 + kk;
+            double v = 0.0;
+            if (gi < m && gk < k) v = TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk];
+            As[kk][row] = v;
+            int col;
+            if (!TB) { kk = l / GB_N; col = l % GB_N; } else { col = l / GB_K; kk = l % GB_K; }
+            int gj = n0 + col;
+            gk = k0 + kk;
+            double w = 0.0;
+            if (gj < n && gk < k) w = TB ? B[(size_t) gj * ldb + gk] : B[(size_t) gk * ldb + gj];
+            Bs[kk][col] = w;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GB_K; kk++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int gi = m0 + ty + 16 * i;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            int gj = n0 + tx + 16 * j;
+            if (gj >= n) continue;
+            double *c = C + (size_t) gi * ldc + gj;
+            *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * *c;
+        }
+    }
+}
+
+// ---- K half-transform tile: T[i][s0:s0+64][p0:p0+64] = sum_{r in CSR row i} C[j_r][s] B[u_r][p]
+constexpr int KT_M = 64, KT_N = 64, KT_K = 16;
+
+__device__ __forceinline__ void half_tile(const double *__restrict__ B, const double *__restrict__ C,
+                                          const int *__restrict__ csr_j, const int *__restrict__ csr_u,
+                                          const int *__restrict__ displs, int nocc, int naux, double *__restrict__ T,
+                                          int i, int s0, int p0)
+{
+    __shared__ double As[KT_K][KT_M + 1];
+    __shared__ double Bs[KT_K][KT_N + 1];
+    __shared__ int rj[KT_K], ru[KT_K];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int r_beg = displs[i], r_end = displs[i + 1];
+    double acc[4][4] = {};
+    for (int r0 = r_beg; r0 < r_end; r0 += KT_K) {
+        if (tid < KT_K) {
+            int r = r0 + tid;
+            rj[tid] = (r < r_end) ? csr_j[r] : -1;
+            ru[tid] = (r < r_end) ? csr_u[r] : -1;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int l = tid + 256 * q;
+            int kk = l / KT_M, c = l % KT_M;
+            int j = rj[kk], u = ru[kk];
+            int sg = s0 + c, pg = p0 + c;
+            As[kk][c] = (j >= 0 && sg < nocc) ? C[(size_t) j * nocc + sg] : 0.0;
+            Bs[kk][c] = (u >= 0 && pg < naux) ? B[(size_t) u * naux + pg] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < KT_K; kk++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[kk][ty + 16 * x];
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[kk][tx + 16 * y];
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        int sg = s0 + ty + 16 * x;
+        if (sg >= nocc) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            int pg = p0 + tx + 16 * y;
+            if (pg < naux) T[((size_t) i * nocc + sg) * naux + pg] = acc[x][y];
+        }
+    }
+}
+
+// ---- K = T T^T partial tile over q in [q_beg, q_end) of the flattened (s,P) index
+__device__ __forceinline__ void syrk_tile(const double *__restrict__ T, int nbf, long long Q, long long q_beg,
+                                          long long q_end, int i0, int j0, double *__restrict__ out)
+{
+    __shared__ double As[KT_K][KT_M + 1];
+    __shared__ double Bs[KT_K][KT_N + 1];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    double acc[4][4] = {};
+    for (long long q0 = q_beg; q0 < q_end; q0 += KT_K) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            int l = tid + 256 * r;
+            int row = l / KT_K, kk = l % KT_K;
+            long long q = q0 + kk;
+            int gi = i0 + row, gj = j0 + row;
+            As[kk][row] = (gi < nbf && q < q_end) ? T[(size_t) gi * Q + q] : 0.0;
+            Bs[kk][row] = (gj < nbf && q < q_end) ? T[(size_t) gj * Q + q] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < KT_K; kk++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[kk][ty + 16 * x];
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[kk][tx + 16 * y];
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        int gi = i0 + ty + 16 * x;
+        if (gi >= nbf) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            int gj = j0 + tx + 16 * y;
+            if (gj < nbf) out[(size_t) gi * nbf + gj] = acc[x][y];
+        }
+    }
+}
+
+// ---- J first pass: partial t(P) of upper rows [r0, r1), weights (2 - d_ij) D_ij.
+// Thread x owns columns x, x + 512, ... (naux <= 8192).
+constexpr int JT_THREADS = 512, JT_COLS = 16;
+
+__device__ __forceinline__ void jt_rows(const double *__restrict__ B, const int *__restrict__ up_u,
+                                        const double *__restrict__ w, int naux, int r0, int r1,
+                                        double *__restrict__ part_row)
+{
+    double acc[JT_COLS];
+#pragma unroll
+    for (int c = 0; c < JT_COLS; c++) acc[c] = 0.0;
+    for (int r = r0; r < r1; r++) {
+        const double wr = w[r];
+        const double *row = B + (size_t) up_u[r] * naux;
+#pragma unroll
+        for (int c = 0; c < JT_COLS; c++) {
+            int p = threadIdx.x + c * JT_THREADS;
+            if (p < naux) acc[c] = fma(wr, __ldg(row + p), acc[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < JT_COLS; c++) {
+        int p = threadIdx.x + c * JT_THREADS;
+        if (p < naux) part_row[p] = acc[c];
+    }
+}
+
+// ---- F = H + 2J - K and the partial energy sum D (F + H) of one strided range
+__device__ __forceinline__ double fock_energy_range(const double *H, const double *J, const double *K,
+                                                    const double *D, double *F, size_t beg, size_t n, size_t stride)
+{
+    double e = 0.0;
+    for (size_t i = beg; i < n; i += stride) {
+        double h = H[i];
+        double f = h + 2.0 * J[i] - K[i];
+        F[i] = f;
+        e += D[i] * (f + h);
+    }
+    return e;
+}
+
+__device__ __forceinline__ double block_sum(double e)
+{
+    __shared__ double sh[32];
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffff, e, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = e;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x < 32) {
+        r = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffff, r, o);
+    }
+    return r;   // valid in thread 0
+}
+
+}  // namespace tscf

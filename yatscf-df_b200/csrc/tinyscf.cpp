@@ -24,6 +24,9 @@
 #include "tinyscf_b200.h"
 #include "tscf_internal.h"
 #include "guess.h"
+#include "batch.h"
+
+#include <cusolverDn.h>
 
 using namespace tscf;
 
@@ -1632,6 +1635,373 @@ int TinySCF_get_timings(TinySCF_t t, double *ms, int n)
     if (!t || !t->dev || !ms) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
     for (int k = 0; k < n && k < TINYSCF_T_COUNT; k++) ms[k] = e->timers[k];
+    return TINYSCF_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batched SCF
+// Many molecules, each set up through the single-molecule API, iterate
+// together: every SCF phase is one launch over all molecules still iterating
+// (batch.cu), the density eigensolves are one batched cuSOLVER call per group
+// of equal basis size. Each molecule follows the reference loop
+// (TinySCF.c:378-435) with its own ene_tol, niters and convergence.
+struct TinySCF_batch_struct {
+    std::vector<TinySCF_t> mols;
+    cudaStream_t s = nullptr;
+    BatchPlan plan;
+    std::vector<void *> mem;
+    struct Group {
+        int n = 0;
+        std::vector<int> members;
+        double *A = nullptr, *W = nullptr;
+        int *info = nullptr;
+        void *dwork = nullptr;
+        std::vector<char> hwork;
+        size_t dbytes = 0;
+        bool batched = true;
+        Eig *eig = nullptr;
+    };
+    std::vector<Group> groups;
+    cusolverDnHandle_t h = nullptr;
+    cusolverDnParams_t params = nullptr;
+    double *d_Eall = nullptr;
+    int *d_active = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double scf_ms = 0.0;
+    int iterations = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+template <typename T>
+int balloc(TinySCF_batch_t b, T **p, size_t count)
+{
+    void *q = nullptr;
+    if (cudaMalloc(&q, sizeof(T) * (count ? count : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return ERR_ALLOC;
+    }
+    b->mem.push_back(q);
+    *p = (T *) q;
+    return OK;
+}
+
+int make_list(TinySCF_batch_t b, const std::vector<int> &counts, WorkList &wl)
+{
+    std::vector<int> st(counts.size() + 1, 0);
+    for (size_t k = 0; k < counts.size(); k++) st[k + 1] = st[k] + counts[k];
+    int *d = nullptr;
+    RC(balloc(b, &d, st.size()));
+    if (cudaMemcpy(d, st.data(), sizeof(int) * st.size(), cudaMemcpyHostToDevice) != cudaSuccess) return ERR_CUDA;
+    wl.start = d;
+    wl.nmol = (int) counts.size();
+    wl.total = st.back();
+    return OK;
+}
+
+int make_gemm(TinySCF_batch_t b, const std::vector<GemmDesc> &descs, bool ta, bool tb, BatchGemm &g)
+{
+    std::vector<int> counts;
+    for (const GemmDesc &d : descs) counts.push_back(((d.m + 63) / 64) * ((d.n + 63) / 64));
+    RC(make_list(b, counts, g.wl));
+    GemmDesc *dd = nullptr;
+    RC(balloc(b, &dd, descs.size()));
+    if (cudaMemcpy(dd, descs.data(), sizeof(GemmDesc) * descs.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return ERR_CUDA;
+    g.descs = dd;
+    g.ta = ta;
+    g.tb = tb;
+    return OK;
+}
+
+int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
+{
+    const int dev = ts[0]->device;
+    for (int k = 0; k < nmol; k++) {
+        if (!ts[k] || !ts[k]->dev || E_(ts[k])->stage < 5 || ts[k]->device != dev) return ERR_STATE;
+        b->mols.push_back(ts[k]);
+    }
+    TSCF_CUDA_CHECK(cudaSetDevice(dev));
+    TSCF_CUDA_CHECK(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
+    TSCF_CUDA_CHECK(cudaEventCreate(&b->ev0));
+    TSCF_CUDA_CHECK(cudaEventCreate(&b->ev1));
+    if (cusolverDnCreate(&b->h) != CUSOLVER_STATUS_SUCCESS || cusolverDnCreateParams(&b->params) != CUSOLVER_STATUS_SUCCESS)
+        return ERR_CUDA;
+    cusolverDnSetStream(b->h, b->s);
+    // eigensolver groups of equal basis size
+    std::map<int, int> gid;
+    std::vector<int> slot(nmol);
+    for (int k = 0; k < nmol; k++) {
+        const int n = ts[k]->nbasfuncs;
+        if (!gid.count(n)) {
+            gid[n] = (int) b->groups.size();
+            b->groups.push_back({});
+            b->groups.back().n = n;
+        }
+        auto &g = b->groups[gid[n]];
+        slot[k] = (int) g.members.size();
+        g.members.push_back(k);
+    }
+    for (auto &g : b->groups) {
+        const int64_t cnt = (int64_t) g.members.size(), n = g.n;
+        RC(balloc(b, &g.A, (size_t) cnt * n * n));
+        RC(balloc(b, &g.W, (size_t) cnt * n));
+        RC(balloc(b, &g.info, (size_t) cnt));
+        size_t dws = 0, hws = 0;
+        cusolverStatus_t st = cusolverDnXsyevBatched_bufferSize(b->h, b->params, CUSOLVER_EIG_MODE_VECTOR,
+                                                                CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, g.A, n,
+                                                                CUDA_R_64F, g.W, CUDA_R_64F, &dws, &hws, cnt);
+        if (st == CUSOLVER_STATUS_SUCCESS) {
+            g.dbytes = dws;
+            char *w = nullptr;
+            RC(balloc(b, &w, dws));
+            g.dwork = w;
+            g.hwork.resize(hws ? hws : 1);
+        } else {
+            g.batched = false;   // one syevd per member
+            g.eig = eig_create(g.n, b->s);
+            if (!g.eig) return ERR_CUDA;
+        }
+    }
+    // per-molecule descriptors and work lists
+    std::vector<MolDev> md(nmol);
+    std::vector<int> c_nup256, c_jblk, c_naux256, c_nup64, c_half, c_syrk, c_nn256, c_efb;
+    std::vector<GemmDesc> xtf, txfp, fd, fds, xtt, t2x, txt2, cocc, dens;
+    int naux_max = 1;
+    for (int k = 0; k < nmol; k++) {
+        TinySCF_t t = ts[k];
+        Engine *e = E_(t);
+        const int n = t->nbasfuncs, o = t->n_occ, na = t->df_nbf;
+        auto &g = b->groups[gid[n]];
+        MolDev &m = md[k];
+        memset(&m, 0, sizeof(m));
+        m.nbf = n;
+        m.naux = na;
+        m.nocc = o;
+        m.nup = e->nup;
+        m.jblk = e->jblk;
+        m.ksplit = e->ksplit;
+        m.max_diis = (t->max_diis < 1 || t->max_diis > MAX_DIIS) ? MAX_DIIS : t->max_diis;
+        m.up_i = e->up_i;
+        m.up_j = e->up_j;
+        m.up_u = e->up_u;
+        m.csr_j = e->csr_j;
+        m.csr_u = e->csr_u;
+        m.displs = e->csr_displs;
+        m.tiles = e->tiles;
+        m.B = e->B;
+        m.H = e->H;
+        m.S = e->S;
+        m.X = e->X;
+        m.D = e->D;
+        m.J = e->J;
+        m.K = e->K;
+        m.F = e->F;
+        m.Fp = e->Fp;
+        m.Cocc = e->Cocc;
+        m.T = e->T;
+        m.Kpart = e->Kpart;
+        m.Jt = e->Jt;
+        m.Jpart = e->Jpart;
+        m.Jw = e->Jw;
+        m.epart = e->epart;
+        m.E = e->E;
+        m.tmp = e->tmp;
+        m.tmp2 = e->tmp2;
+        m.F0 = e->F0;
+        m.R = e->R;
+        m.diis = e->diis;
+        m.eigA = g.A + (size_t) slot[k] * n * n;
+        naux_max = std::max(naux_max, na);
+        const int nt = (n + 63) / 64;
+        const size_t nn = (size_t) n * n;
+        c_nup256.push_back((e->nup + 255) / 256);
+        c_jblk.push_back(e->jblk);
+        c_naux256.push_back((na + 255) / 256);
+        c_nup64.push_back((e->nup + 63) / 64);
+        c_half.push_back(n * ((o + 63) / 64) * ((na + 63) / 64));
+        c_syrk.push_back(nt * (nt + 1) / 2 * e->ksplit);
+        c_nn256.push_back((int) ((nn + 255) / 256));
+        c_efb.push_back(ENERGY_BLOCKS);
+        xtf.push_back({n, n, n, n, n, n, e->X, e->F, e->tmp, 1.0, 0.0});
+        txfp.push_back({n, n, n, n, n, n, e->tmp, e->X, e->Fp, 1.0, 0.0});
+        fd.push_back({n, n, n, n, n, n, e->F, e->D, e->tmp, 1.0, 0.0});
+        fds.push_back({n, n, n, n, n, n, e->tmp, e->S, e->tmp2, 1.0, 0.0});
+        xtt.push_back({n, n, n, n, n, n, e->X, e->tmp, e->tmp2, 1.0, 0.0});
+        t2x.push_back({n, n, n, n, n, n, e->tmp2, e->X, e->tmp, 1.0, 0.0});
+        txt2.push_back({n, n, n, n, n, n, e->tmp, e->X, e->tmp2, 1.0, 0.0});
+        cocc.push_back({n, o, n, n, n, o, e->X, m.eigA, e->Cocc, 1.0, 0.0});
+        dens.push_back({n, n, o, o, o, n, e->Cocc, e->Cocc, e->D, 1.0, 0.0});
+    }
+    BatchPlan &p = b->plan;
+    p.nmol = nmol;
+    p.naux_max = naux_max;
+    MolDev *dm = nullptr;
+    RC(balloc(b, &dm, nmol));
+    TSCF_CUDA_CHECK(cudaMemcpy(dm, md.data(), sizeof(MolDev) * nmol, cudaMemcpyHostToDevice));
+    p.mols = dm;
+    int *da = nullptr;
+    RC(balloc(b, &da, nmol));
+    p.active = da;
+    b->d_active = da;
+    RC(balloc(b, &b->d_Eall, nmol));
+    RC(make_list(b, c_nup256, p.nup256));
+    RC(make_list(b, c_jblk, p.jblk));
+    RC(make_list(b, c_naux256, p.naux256));
+    RC(make_list(b, c_nup64, p.nup64));
+    RC(make_list(b, c_half, p.half));
+    RC(make_list(b, c_syrk, p.syrk));
+    RC(make_list(b, c_nn256, p.nn256));
+    RC(make_list(b, c_efb, p.efb));
+    RC(make_gemm(b, xtf, true, false, p.g_xtf));
+    RC(make_gemm(b, txfp, false, false, p.g_tx_fp));
+    RC(make_gemm(b, fd, false, false, p.g_fd));
+    RC(make_gemm(b, fds, false, false, p.g_fds));
+    RC(make_gemm(b, xtt, true, false, p.g_xtt));
+    RC(make_gemm(b, t2x, false, false, p.g_t2x));
+    RC(make_gemm(b, txt2, false, false, p.g_tx_t2));
+    RC(make_gemm(b, cocc, false, true, p.g_cocc));
+    RC(make_gemm(b, dens, false, true, p.g_dens));
+    return OK;
+}
+
+int batch_eigs(TinySCF_batch_t b)
+{
+    for (auto &g : b->groups) {
+        const int64_t cnt = (int64_t) g.members.size(), n = g.n;
+        if (g.batched) {
+            cusolverStatus_t st = cusolverDnXsyevBatched(b->h, b->params, CUSOLVER_EIG_MODE_VECTOR,
+                                                         CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, g.A, n, CUDA_R_64F,
+                                                         g.W, CUDA_R_64F, g.dwork, g.dbytes, g.hwork.data(),
+                                                         g.hwork.size(), g.info, cnt);
+            if (st != CUSOLVER_STATUS_SUCCESS) return ERR_NUMERIC;
+        } else {
+            for (int64_t k = 0; k < cnt; k++)
+                RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
+        }
+    }
+    return OK;
+}
+
+int batch_scf_impl(TinySCF_batch_t b)
+{
+    const int nmol = (int) b->mols.size();
+    std::vector<int> act(nmol, 0);
+    std::vector<double> prev(nmol, 0.0), delta(nmol, 223.0), Eh(nmol, 0.0);
+    for (int k = 0; k < nmol; k++) {
+        TinySCF_t t = b->mols[k];
+        t->iter = 0;
+        act[k] = (t->niters > 0) ? 1 : 0;
+        // the loop consumes the guess (or the state a reset left) exactly like do_SCF
+        TSCF_CUDA_CHECK(cudaStreamSynchronize(E_(t)->s));
+    }
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
+    const long long l0 = g_launches;
+    cudaEventRecord(b->ev0, b->s);
+    int it = 0;
+    for (;; it++) {
+        bool any = false;
+        for (int v : act) any |= v != 0;
+        if (!any) break;
+        batch_j(b->plan, b->s);
+        batch_k(b->plan, b->s);
+        batch_fock(b->plan, b->d_Eall, b->s);
+        batch_diis(b->plan, it >= 2, b->s);
+        batch_copy_fp(b->plan, b->s);
+        RC(batch_eigs(b));
+        batch_gemm(b->plan.g_cocc, b->d_active, b->s);
+        batch_gemm(b->plan.g_dens, b->d_active, b->s);
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(Eh.data(), b->d_Eall, sizeof(double) * nmol, cudaMemcpyDeviceToHost, b->s));
+        TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
+        TSCF_CUDA_CHECK(cudaGetLastError());
+        for (int k = 0; k < nmol; k++) {
+            if (!act[k]) continue;
+            TinySCF_t t = b->mols[k];
+            t->HF_energy = Eh[k];
+            if (!std::isfinite(Eh[k])) return ERR_NUMERIC;
+            delta[k] = fabs(Eh[k] - prev[k]);
+            prev[k] = Eh[k];
+            if (t->iter == 0) delta[k] = 223;
+            t->iter++;
+            if (!(t->iter < t->niters && delta[k] >= t->ene_tol)) act[k] = 0;
+        }
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
+    }
+    cudaEventRecord(b->ev1, b->s);
+    TSCF_CUDA_CHECK(cudaEventSynchronize(b->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->scf_ms = ms;
+    b->iterations = it;
+    b->launches = g_launches - l0;
+    // eigenvalues and host mirrors of every molecule
+    for (auto &g : b->groups)
+        for (size_t k = 0; k < g.members.size(); k++) {
+            Engine *e = E_(b->mols[g.members[k]]);
+            TSCF_CUDA_CHECK(cudaMemcpyAsync(e->w, g.W + k * g.n, sizeof(double) * g.n, cudaMemcpyDeviceToDevice, b->s));
+        }
+    TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
+    for (TinySCF_t t : b->mols) {
+        Engine *e = E_(t);
+        e->F_is_orth = true;
+        e->have_eig = false;
+        RC(sync_host_impl(t));
+    }
+    return OK;
+}
+
+void batch_free_impl(TinySCF_batch_t b)
+{
+    if (b->s) cudaStreamSynchronize(b->s);
+    for (auto &g : b->groups) eig_destroy(g.eig);
+    for (void *p : b->mem) cudaFree(p);
+    if (b->params) cusolverDnDestroyParams(b->params);
+    if (b->h) cusolverDnDestroy(b->h);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->s) cudaStreamDestroy(b->s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int TinySCF_batch_create(TinySCF_batch_t *out, TinySCF_t *mols, int nmol)
+{
+    if (!out || !mols || nmol <= 0) return TINYSCF_ERR_INPUT;
+    TinySCF_batch_t b = new TinySCF_batch_struct();
+    int rc = batch_create_impl(b, mols, nmol);
+    if (rc) {
+        batch_free_impl(b);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return TINYSCF_OK;
+}
+
+int TinySCF_batch_do_SCF(TinySCF_batch_t b)
+{
+    if (!b) return TINYSCF_ERR_STATE;
+    return batch_scf_impl(b);
+}
+
+int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long long *launches)
+{
+    if (!b) return TINYSCF_ERR_STATE;
+    if (scf_ms) *scf_ms = b->scf_ms;
+    if (iterations) *iterations = b->iterations;
+    if (launches) *launches = b->launches;
+    return TINYSCF_OK;
+}
+
+int TinySCF_batch_free(TinySCF_batch_t b)
+{
+    if (!b) return TINYSCF_ERR_STATE;
+    batch_free_impl(b);
+    delete b;
     return TINYSCF_OK;
 }
 

@@ -107,6 +107,11 @@ def load_library(path=LIBPATH):
         "TinySCF_set_density_solver": ([T, ip], ip),
         "TinySCF_set_graph": ([T, ip], ip),
         "TinySCF_set_guess": ([T, ip, ctypes.c_char_p], ip),
+        "TinySCF_batch_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(T), ip], ip),
+        "TinySCF_batch_do_SCF": ([ctypes.c_void_p], ip),
+        "TinySCF_batch_stats": ([ctypes.c_void_p, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)],
+                                ip),
+        "TinySCF_batch_free": ([ctypes.c_void_p], ip),
         "TinySCF_guess_used": ([T], ip),
         "TinySCF_guess_dataset": ([T, dp, fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong], ctypes.c_longlong),
         "TinySCF_guess_train": ([fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ip, ip, ctypes.c_float,
@@ -367,3 +372,35 @@ class TinySCF:
             self.free()
         except Exception:
             pass
+
+
+class TinySCFBatch:
+    """Batched SCF over engines that have been set up (TinySCF.setup()); every
+    SCF phase is one launch over all molecules still iterating."""
+
+    def __init__(self, engines):
+        self.lib = load_library()
+        self.engines = list(engines)
+        arr = (TinySCF_t * len(self.engines))(*[e.t for e in self.engines])
+        self.b = ctypes.c_void_p()
+        rc = self.lib.TinySCF_batch_create(ctypes.byref(self.b), arr, len(self.engines))
+        if rc:
+            raise TinySCFError("batch_create: " + STATUS.get(rc, str(rc)))
+
+    def do_SCF(self):
+        rc = self.lib.TinySCF_batch_do_SCF(self.b)
+        if rc:
+            raise TinySCFError("batch_do_SCF: " + STATUS.get(rc, str(rc)))
+
+    def stats(self):
+        """(device ms of the last batched SCF, batched iterations, kernel launches)."""
+        ms = ctypes.c_double()
+        it = ctypes.c_int()
+        nl = ctypes.c_longlong()
+        self.lib.TinySCF_batch_stats(self.b, ctypes.byref(ms), ctypes.byref(it), ctypes.byref(nl))
+        return ms.value, it.value, nl.value
+
+    def free(self):
+        if self.b:
+            self.lib.TinySCF_batch_free(self.b)
+            self.b = None
