@@ -168,6 +168,17 @@ TINYSCF_API int TinySCF_guess_train(const float *feat, const float *target, cons
  * by the training kernels: host in, host out. */
 TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *params, const float *X, const float *T,
                                        int n, float *grad, float *loss);
+/* Autotuner (on unless TINYSCF_AUTOTUNE=0): the first time a shape is met
+ * outside a stream capture, the candidates for these knobs are timed on the
+ * device and the fastest kept for the process (and saved to / loaded from the
+ * file named by TINYSCF_TUNE_FILE): the block size and thread order of each
+ * 3-centre integral AM class, the tile shape of each FP64 GEMM shape
+ * (64x64, 32x32, 128x64), the split count of the FP64 exchange and the row
+ * blocks of the J first pass. All candidates compute the same values. */
+TINYSCF_API int TinySCF_set_autotune(int on);
+/* The tuner's table as text ("key -> choice (ms) [candidate: ms]..."); writes
+ * at most len bytes into buf and returns the full length. */
+TINYSCF_API int TinySCF_autotune_report(char *buf, int len);
 /* Batched SCF over many molecules of uneven size. Each molecule is a handle
  * set up through the single-molecule calls (up to TinySCF_build_DF_tensor,
  * any initial guess; FP64 exchange). TinySCF_batch_do_SCF then iterates all of

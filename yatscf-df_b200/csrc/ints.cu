@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "tscf_internal.h"
+#include "tune.h"
 
 namespace tscf {
 
@@ -348,15 +349,20 @@ __device__ void quartet_acc(const Sh &A, const Sh &B, bool ub, const Sh &C, cons
 
 // ------------------------------------------------------------------ 3-centre kernel
 // One thread per (shell pair in class, aux shell of AM lc). Writes pqA_u rows.
+// aux_major = 0: consecutive threads take consecutive aux shells of one pair;
+// 1: consecutive pairs for one aux shell. The block size and this order are
+// picked per AM class by the autotuner (launch_3c_class).
 template <int LA, int LB, int LC>
-__global__ void __launch_bounds__(128) k_three_center(DevShells sh, DevShells aux, const int2 *pairs, int pair0,
+__global__ void __launch_bounds__(256) k_three_center(DevShells sh, DevShells aux, const int2 *pairs, int pair0,
                                                       int npairs, const int *aux_ids, int naux_am,
                                                       const double *sp_scr, const double *df_scr, double scrtol2,
-                                                      const int *upair_index, int nbf, int naux, double *pqA)
+                                                      const int *upair_index, int nbf, int naux, double *pqA,
+                                                      int aux_major)
 {
     const long long tid = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (long long) npairs * naux_am) return;
-    const int ip = (int) (tid / naux_am), iq = (int) (tid % naux_am);
+    const int ip = aux_major ? (int) (tid % npairs) : (int) (tid / naux_am);
+    const int iq = aux_major ? (int) (tid / npairs) : (int) (tid % naux_am);
     const int2 mn = pairs[pair0 + ip];
     const int P = aux_ids[iq];
     const double s0 = sp_scr[mn.x * sh.nsh + mn.y];
@@ -399,10 +405,23 @@ static void launch_3c_class(const DevShells &sh, const DevShells &aux, const Thr
 {
     long long n = (long long) npairs * naux_am;
     if (n == 0) return;
-    int blocks = (int) ((n + 127) / 128);
-    k_three_center<LA, LB, LC><<<blocks, 128, 0, s>>>(sh, aux, pl.pairs, pair0, npairs, pl.aux_by_am + lc_start,
-                                                      naux_am, pl.sp_scr, pl.df_scr, pl.scrtol2, pl.upair_index,
-                                                      pl.nbf, pl.naux, pqA);
+    auto run = [&](int c) {
+        const int bs = 64 << (c % 3), order = c / 3;
+        const int blocks = (int) ((n + bs - 1) / bs);
+        k_three_center<LA, LB, LC><<<blocks, bs, 0, s>>>(sh, aux, pl.pairs, pair0, npairs, pl.aux_by_am + lc_start,
+                                                         naux_am, pl.sp_scr, pl.df_scr, pl.scrtol2, pl.upair_index,
+                                                         pl.nbf, pl.naux, pqA, order);
+        g_launches++;
+    };
+    // every candidate writes the same values, so re-running while tuning is harmless
+    char key[64];
+    snprintf(key, sizeof(key), "3c:%d%d%d:%s", LA, LB, LC, n < 65536 ? "small" : "large");
+    int c = tune_lookup(key);
+    if (c < 0 && tune_enabled()) {
+        tune_run(key, {0, 1, 2, 3, 4, 5}, run, s, 1);
+        return;
+    }
+    run(c < 0 ? 1 : c);
 }
 
 template <int LA, int LB>

@@ -8,6 +8,7 @@
 #include <cusolverDn.h>
 
 #include "tiles.cuh"
+#include "tune.h"
 #include "tscf_internal.h"
 
 namespace tscf {
@@ -15,24 +16,62 @@ namespace tscf {
 long long g_launches = 0;
 
 // ------------------------------------------------------------------ DGEMM
-// 64x64 output tile per 256-thread block (dgemm_tile).
-template <bool TA, bool TB>
+// Three tile shapes (dgemm_tile): 64x64 (default), 32x32 (more blocks for
+// small matrices) and 128x64 (more reuse for large ones). The autotuner picks
+// one per call shape the first time the shape is met outside a stream capture.
+template <bool TA, bool TB, int BM, int BN>
 __global__ void __launch_bounds__(256) k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
                                                const double *__restrict__ B, int ldb, double beta, double *C, int ldc)
 {
-    dgemm_tile<TA, TB>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, blockIdx.y * GB_M, blockIdx.x * GB_N);
+    dgemm_tile<TA, TB, BM, BN>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, blockIdx.y * BM, blockIdx.x * BN);
+}
+
+template <int BM, int BN>
+static void dgemm_shape(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
+                        const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
+{
+    dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM);
+    g_launches++;
+    if (!ta && !tb) k_dgemm<false, false, BM, BN><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (!ta && tb) k_dgemm<false, true, BM, BN><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (ta && !tb) k_dgemm<true, false, BM, BN><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else k_dgemm<true, true, BM, BN><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+static void dgemm_variant(int v, bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
+                          const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
+{
+    if (v == 1) dgemm_shape<32, 32>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    else if (v == 2) dgemm_shape<128, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    else dgemm_shape<64, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
 
 void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda, const double *B, int ldb,
            double beta, double *C, int ldc, cudaStream_t s)
 {
     if (m <= 0 || n <= 0) return;
-    dim3 grid((n + GB_N - 1) / GB_N, (m + GB_M - 1) / GB_M);
-    g_launches++;
-    if (!ta && !tb) k_dgemm<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else if (!ta && tb) k_dgemm<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else if (ta && !tb) k_dgemm<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else k_dgemm<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    char key[96];
+    snprintf(key, sizeof(key), "dgemm:%d%d:%dx%dx%d", (int) ta, (int) tb, m, n, k);
+    int v = tune_lookup(key);
+    if (v < 0) {
+        v = 0;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(s, &cs);
+        // tune only where re-running is harmless: C overwritten (beta = 0) and
+        // not read by the product
+        const char *c0 = (const char *) C, *c1 = c0 + sizeof(double) * ((size_t) (m - 1) * ldc + n);
+        auto disjoint = [&](const double *X, size_t elems) {
+            const char *x0 = (const char *) X, *x1 = x0 + sizeof(double) * elems;
+            return x1 <= c0 || c1 <= x0;
+        };
+        const size_t ea = ta ? (size_t) k * lda : (size_t) m * lda, eb = tb ? (size_t) n * ldb : (size_t) k * ldb;
+        if (tune_enabled() && cs == cudaStreamCaptureStatusNone && beta == 0.0 && disjoint(A, ea) && disjoint(B, eb) &&
+            (double) m * n * k >= 2e6) {
+            v = tune_run(key, {0, 1, 2}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
+            return;
+        }
+    }
+    dgemm_variant(v, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
 
 // ------------------------------------------------------------------ eigensolver

@@ -6,33 +6,39 @@
 
 namespace tscf {
 
-// ---- FP64 GEMM tile: 64x64 outputs per 256 threads, 4x4 per thread, K step 16.
-// op(A) is m x k, op(B) is k x n, row-major; C = alpha op(A) op(B) + beta C.
+// ---- FP64 GEMM tile: BM x BN outputs per 256 threads (a 16 x 16 thread grid,
+// BM/16 x BN/16 outputs per thread), K step 16. op(A) is m x k, op(B) is
+// k x n, row-major; C = alpha op(A) op(B) + beta C. Every tile shape sums
+// over k in the same order, so all shapes give identical results.
 constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
 
-template <bool TA, bool TB>
+template <bool TA, bool TB, int BM = 64, int BN = 64>
 __device__ __forceinline__ void dgemm_tile(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
                                            const double *__restrict__ B, int ldb, double beta, double *C, int ldc,
                                            int m0, int n0)
 {
-    __shared__ double As[GB_K][GB_M + 1];
-    __shared__ double Bs[GB_K][GB_N + 1];
+    constexpr int TM = BM / 16, TN = BN / 16;
+    __shared__ double As[GB_K][BM + 1];
+    __shared__ double Bs[GB_K][BN + 1];
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    double acc[4][4] = {};
+    double acc[TM][TN] = {};
     for (int k0 = 0; k0 < k; k0 += GB_K) {
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            int l = tid + 256 * r;
+        for (int r = 0; r < BM / 16; r++) {
+            const int l = tid + 256 * r;
             int row, kk;
-            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / GB_M; row = l % GB_M; }
-            int gi = m0 + row, gk = k0 + kk;
+            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / BM; row = l % BM; }
+            const int gi = m0 + row, gk = k0 + kk;
             double v = 0.0;
             if (gi < m && gk < k) v = TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk];
             As[kk][row] = v;
-            int col;
-            if (!TB) { kk = l / GB_N; col = l % GB_N; } else { col = l / GB_K; kk = l % GB_K; }
-            int gj = n0 + col;
-            gk = k0 + kk;
+        }
+#pragma unroll
+        for (int r = 0; r < BN / 16; r++) {
+            const int l = tid + 256 * r;
+            int col, kk;
+            if (!TB) { kk = l / BN; col = l % BN; } else { col = l / GB_K; kk = l % GB_K; }
+            const int gj = n0 + col, gk = k0 + kk;
             double w = 0.0;
             if (gj < n && gk < k) w = TB ? B[(size_t) gj * ldb + gk] : B[(size_t) gk * ldb + gj];
             Bs[kk][col] = w;
@@ -40,25 +46,25 @@ __device__ __forceinline__ void dgemm_tile(int m, int n, int k, double alpha, co
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < GB_K; kk++) {
-            double a[4], b[4];
+            double a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+            for (int i = 0; i < TM; i++) a[i] = As[kk][ty + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+            for (int j = 0; j < TN; j++) b[j] = Bs[kk][tx + 16 * j];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+            for (int i = 0; i < TM; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < TN; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        int gi = m0 + ty + 16 * i;
+    for (int i = 0; i < TM; i++) {
+        const int gi = m0 + ty + 16 * i;
         if (gi >= m) continue;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            int gj = n0 + tx + 16 * j;
+        for (int j = 0; j < TN; j++) {
+            const int gj = n0 + tx + 16 * j;
             if (gj >= n) continue;
             double *c = C + (size_t) gi * ldc + gj;
             *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * *c;

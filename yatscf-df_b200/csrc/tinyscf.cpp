@@ -25,6 +25,7 @@
 #include "tscf_internal.h"
 #include "guess.h"
 #include "batch.h"
+#include "tune.h"
 
 #include <cusolverDn.h>
 
@@ -288,9 +289,9 @@ struct Engine {
     double *B = nullptr;
     double *T = nullptr, *Kpart = nullptr;
     int2 *tiles = nullptr;
-    int ksplit = 1;
+    int ksplit = 1, ksplit_max = 1;
     double *Jt = nullptr, *Jpart = nullptr, *Jw = nullptr;
-    int jblk = 1;
+    int jblk = 1, jblk_max = 1;
     double *epart = nullptr, *E = nullptr;
     Eig *eig = nullptr;
     int kprec = TINYSCF_K_FP64;
@@ -765,7 +766,8 @@ int sparsity_impl(TinySCF_t t)
     RC(dalloc(e, &e->T, (size_t) nbf * nocc * naux));
     const int nt = (nbf + 63) / 64, ntiles = nt * (nt + 1) / 2;
     e->ksplit = std::max(1, std::min(64, (4 * 148 + ntiles - 1) / ntiles));
-    RC(dalloc(e, &e->Kpart, (size_t) e->ksplit * nbf * nbf));
+    e->ksplit_max = std::min(64, 2 * e->ksplit);   // room for the autotuner's candidates
+    RC(dalloc(e, &e->Kpart, (size_t) e->ksplit_max * nbf * nbf));
     {
         std::vector<int2> tl;
         for (int a = 0; a < nt; a++)
@@ -774,8 +776,9 @@ int sparsity_impl(TinySCF_t t)
     }
     FockPlan p = e->plan();
     e->jblk = build_J_part_blocks(p);
+    e->jblk_max = std::max(e->jblk, std::min(4 * 148, std::max(1, e->nup)));
     RC(dalloc(e, &e->Jt, naux));
-    RC(dalloc(e, &e->Jpart, (size_t) e->jblk * naux));
+    RC(dalloc(e, &e->Jpart, (size_t) e->jblk_max * naux));
     RC(dalloc(e, &e->Jw, std::max(1, e->nup)));
     RC(sync_rc(e, "sparsity"));
     t->mem_size = (double) nu * naux * 8 + (double) nbf * nocc * naux * 8 + 24.0 * e->nn * 8;
@@ -899,6 +902,40 @@ int guess_impl(TinySCF_t t)
     return OK;
 }
 
+// ------------------------------------------------------------------ autotuning of the Fock build
+// The split count of the FP64 exchange (K = T T^T) and the number of row
+// blocks of the J first pass are timed on this molecule's buffers (their
+// contents do not matter for the timing; the first Fock build rewrites J and
+// K) and the fastest kept; later molecules of the same sizes reuse the choice.
+int autotune_fock(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    if (!tune_enabled()) return OK;
+    FockPlan p = e->plan();
+    p.nocc = t->n_occ;
+    char key[96];
+    snprintf(key, sizeof(key), "ksyrk:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf);
+    int c = tune_lookup(key);
+    if (c < 0) {
+        std::vector<int> cand;
+        for (int v : {std::max(1, e->ksplit / 2), e->ksplit, e->ksplit_max})
+            if (std::find(cand.begin(), cand.end(), v) == cand.end()) cand.push_back(v);
+        c = tune_run(key, cand, [&](int k) { build_K_syrk(p, e->T, e->K, e->Kpart, k, e->tiles, e->s); }, e->s);
+    }
+    if (c >= 1 && c <= e->ksplit_max) e->ksplit = c;
+    snprintf(key, sizeof(key), "jrows:%d:%d", e->nup, t->df_nbf);
+    c = tune_lookup(key);
+    if (c < 0) {
+        std::vector<int> cand;
+        for (int v : {148, 296, 592})
+            if (v <= e->jblk_max && std::find(cand.begin(), cand.end(), v) == cand.end()) cand.push_back(v);
+        if (cand.empty()) cand.push_back(e->jblk);
+        c = tune_run(key, cand, [&](int nb) { build_J(p, e->D, e->J, e->Jt, e->Jpart, nb, e->Jw, e->s); }, e->s);
+    }
+    if (c >= 1 && c <= e->jblk_max) e->jblk = c;
+    return sync_rc(e, "autotuning");
+}
+
 // ------------------------------------------------------------------ DF tensor (build_DF_tensor.c:256-287)
 int df_impl(TinySCF_t t)
 {
@@ -966,7 +1003,7 @@ int df_impl(TinySCF_t t)
         printf("---------- DF tensor construction finished ----------\n");
     }
     e->stage = std::max(e->stage, 5);
-    return OK;
+    return autotune_fock(t);
 }
 
 // ------------------------------------------------------------------ Fock (build_Fock.c:349-396)
@@ -1967,6 +2004,21 @@ void batch_free_impl(TinySCF_batch_t b)
 }  // namespace
 
 extern "C" {
+
+int TinySCF_set_autotune(int on)
+{
+    tune_set_enabled(on != 0);
+    return TINYSCF_OK;
+}
+
+int TinySCF_autotune_report(char *buf, int len)
+{
+    std::string r = tune_report();
+    if (buf && len > 0) {
+        snprintf(buf, (size_t) len, "%s", r.c_str());
+    }
+    return (int) r.size();
+}
 
 int TinySCF_batch_create(TinySCF_batch_t *out, TinySCF_t *mols, int nmol)
 {

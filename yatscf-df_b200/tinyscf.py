@@ -112,6 +112,8 @@ def load_library(path=LIBPATH):
         "TinySCF_batch_stats": ([ctypes.c_void_p, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)],
                                 ip),
         "TinySCF_batch_free": ([ctypes.c_void_p], ip),
+        "TinySCF_set_autotune": ([ip], ip),
+        "TinySCF_autotune_report": ([ctypes.c_char_p, ip], ip),
         "TinySCF_guess_used": ([T], ip),
         "TinySCF_guess_dataset": ([T, dp, fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong], ctypes.c_longlong),
         "TinySCF_guess_train": ([fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ip, ip, ctypes.c_float,
@@ -404,3 +406,16 @@ class TinySCFBatch:
         if self.b:
             self.lib.TinySCF_batch_free(self.b)
             self.b = None
+
+
+def autotune_report():
+    """The autotuner's choices so far (text, one line per tuned shape)."""
+    lib = load_library()
+    n = lib.TinySCF_autotune_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.TinySCF_autotune_report(buf, n + 1)
+    return buf.value.decode()
+
+
+def set_autotune(on):
+    load_library().TinySCF_set_autotune(int(bool(on)))
