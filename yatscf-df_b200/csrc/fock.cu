@@ -106,6 +106,16 @@ __global__ void __launch_bounds__(256) k_syrk_part(const double *__restrict__ T,
     syrk_tile(T, nbf, Q, q_beg, q_end, tl.x * KT_M, tl.y * KT_N, Kpart + (size_t) split * nbf * nbf);
 }
 
+__global__ void __launch_bounds__(256, 1) k_syrk_part128(const double *__restrict__ T, int nbf, long long Q,
+                                                         long long qchunk, const int2 *__restrict__ tiles,
+                                                         double *__restrict__ Kpart)
+{
+    const int2 tl = tiles[blockIdx.x];
+    const int split = blockIdx.y;
+    const long long q_beg = (long long) split * qchunk, q_end = min(Q, q_beg + qchunk);
+    syrk_tile128(T, nbf, Q, q_beg, q_end, tl.x * KB_T, tl.y * KB_T, Kpart + (size_t) split * nbf * nbf);
+}
+
 // K[i][j] = K[j][i] = sum_split Kpart[split][i][j] for i <= j (TinySCF keeps
 // the upper triangle and mirrors it, build_Fock.c:369-379).
 __global__ void k_syrk_reduce(const double *Kpart, int nsplit, int nbf, double *K)
@@ -130,16 +140,17 @@ void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T,
 }
 
 void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_Kpart, int ksplit, const int2 *d_tiles,
-                  cudaStream_t s)
+                  cudaStream_t s, int tile)
 {
-    const int nt = (p.nbf + KT_M - 1) / KT_M;
+    const int nt = (p.nbf + tile - 1) / tile;
     const int ntiles = nt * (nt + 1) / 2;
     const long long Q = (long long) p.nocc * p.naux;
     long long qchunk = (Q + ksplit - 1) / ksplit;
     qchunk = (qchunk + KT_K - 1) / KT_K * KT_K;
     dim3 g2(ntiles, ksplit);
     g_launches += 2;
-    k_syrk_part<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
+    if (tile == KB_T) k_syrk_part128<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
+    else k_syrk_part<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
     size_t nn = (size_t) p.nbf * p.nbf;
     k_syrk_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(d_Kpart, ksplit, p.nbf, d_K);
 }

@@ -174,6 +174,71 @@ __device__ __forceinline__ void syrk_tile(const double *__restrict__ T, int nbf,
     }
 }
 
+// ---- K = T T^T partial tile, 128 x 128 outputs per 256 threads (8 x 8 per
+// thread, half the shared-memory reads per FMA of the 64 x 64 tile); the next
+// K-step's operands are prefetched into registers while the current one runs.
+// Same summation order over q as syrk_tile.
+constexpr int KB_T = 128;
+
+__device__ __forceinline__ void syrk_tile128(const double *__restrict__ T, int nbf, long long Q, long long q_beg,
+                                             long long q_end, int i0, int j0, double *__restrict__ out)
+{
+    __shared__ double As[KT_K][KB_T + 1];
+    __shared__ double Bs[KT_K][KB_T + 1];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    double acc[8][8];
+#pragma unroll
+    for (int x = 0; x < 8; x++)
+#pragma unroll
+        for (int y = 0; y < 8; y++) acc[x][y] = 0.0;
+    double pa[8], pb[8];
+    auto fetch = [&](long long q0) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = tid + 256 * r;
+            const int row = l / KT_K, kk = l % KT_K;
+            const long long q = q0 + kk;
+            const int gi = i0 + row, gj = j0 + row;
+            pa[r] = (gi < nbf && q < q_end) ? T[(size_t) gi * Q + q] : 0.0;
+            pb[r] = (gj < nbf && q < q_end) ? T[(size_t) gj * Q + q] : 0.0;
+        }
+    };
+    if (q_beg < q_end) fetch(q_beg);
+    for (long long q0 = q_beg; q0 < q_end; q0 += KT_K) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = tid + 256 * r;
+            As[l % KT_K][l / KT_K] = pa[r];
+            Bs[l % KT_K][l / KT_K] = pb[r];
+        }
+        __syncthreads();
+        if (q0 + KT_K < q_end) fetch(q0 + KT_K);
+#pragma unroll
+        for (int kk = 0; kk < KT_K; kk++) {
+            double a[8], b[8];
+#pragma unroll
+            for (int x = 0; x < 8; x++) a[x] = As[kk][ty + 16 * x];
+#pragma unroll
+            for (int y = 0; y < 8; y++) b[y] = Bs[kk][tx + 16 * y];
+#pragma unroll
+            for (int x = 0; x < 8; x++)
+#pragma unroll
+                for (int y = 0; y < 8; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 8; x++) {
+        const int gi = i0 + ty + 16 * x;
+        if (gi >= nbf) continue;
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+            const int gj = j0 + tx + 16 * y;
+            if (gj < nbf) out[(size_t) gi * nbf + gj] = acc[x][y];
+        }
+    }
+}
+
 // ---- J first pass: partial t(P) of upper rows [r0, r1), weights (2 - d_ij) D_ij.
 // Thread x owns columns x, x + 512, ... (naux <= 8192).
 constexpr int JT_THREADS = 512, JT_COLS = 16;

@@ -289,7 +289,8 @@ struct Engine {
     double *B = nullptr;
     double *T = nullptr, *Kpart = nullptr;
     int2 *tiles = nullptr;
-    int ksplit = 1, ksplit_max = 1;
+    int ksplit = 1, ksplit_max = 1, ksplit64 = 1, ktile = 64;
+    int2 *tiles128 = nullptr;
     double *Jt = nullptr, *Jpart = nullptr, *Jw = nullptr;
     int jblk = 1, jblk_max = 1;
     double *epart = nullptr, *E = nullptr;
@@ -765,14 +766,20 @@ int sparsity_impl(TinySCF_t t)
     RC(dalloc(e, &e->B, (size_t) nu * naux));
     RC(dalloc(e, &e->T, (size_t) nbf * nocc * naux));
     const int nt = (nbf + 63) / 64, ntiles = nt * (nt + 1) / 2;
+    const int nt2 = (nbf + 127) / 128, ntiles2 = nt2 * (nt2 + 1) / 2;
     e->ksplit = std::max(1, std::min(64, (4 * 148 + ntiles - 1) / ntiles));
-    e->ksplit_max = std::min(64, 2 * e->ksplit);   // room for the autotuner's candidates
+    e->ksplit64 = e->ksplit;
+    const int h128 = std::max(1, std::min(64, (2 * 148 + ntiles2 - 1) / ntiles2));
+    e->ksplit_max = std::min(64, 2 * std::max(e->ksplit, h128));   // room for the autotuner's candidates
     RC(dalloc(e, &e->Kpart, (size_t) e->ksplit_max * nbf * nbf));
     {
-        std::vector<int2> tl;
+        std::vector<int2> tl, tl2;
         for (int a = 0; a < nt; a++)
             for (int b = a; b < nt; b++) tl.push_back(make_int2(a, b));
+        for (int a = 0; a < nt2; a++)
+            for (int b = a; b < nt2; b++) tl2.push_back(make_int2(a, b));
         RC(upload(e, &e->tiles, tl));
+        RC(upload(e, &e->tiles128, tl2));
     }
     FockPlan p = e->plan();
     e->jblk = build_J_part_blocks(p);
@@ -914,15 +921,27 @@ int autotune_fock(TinySCF_t t)
     FockPlan p = e->plan();
     p.nocc = t->n_occ;
     char key[96];
+    // candidates: tile * 1000 + split count
     snprintf(key, sizeof(key), "ksyrk:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf);
     int c = tune_lookup(key);
     if (c < 0) {
+        const int nt2 = (t->nbasfuncs + 127) / 128, ntiles2 = nt2 * (nt2 + 1) / 2;
+        const int h128 = std::max(1, std::min(64, (2 * 148 + ntiles2 - 1) / ntiles2));
         std::vector<int> cand;
-        for (int v : {std::max(1, e->ksplit / 2), e->ksplit, e->ksplit_max})
-            if (std::find(cand.begin(), cand.end(), v) == cand.end()) cand.push_back(v);
-        c = tune_run(key, cand, [&](int k) { build_K_syrk(p, e->T, e->K, e->Kpart, k, e->tiles, e->s); }, e->s);
+        for (int v : {std::max(1, e->ksplit / 2), e->ksplit, std::min(e->ksplit_max, 2 * e->ksplit)})
+            if (std::find(cand.begin(), cand.end(), 64000 + v) == cand.end()) cand.push_back(64000 + v);
+        for (int v : {std::max(1, h128 / 2), h128, std::min(e->ksplit_max, 2 * h128)})
+            if (std::find(cand.begin(), cand.end(), 128000 + v) == cand.end()) cand.push_back(128000 + v);
+        c = tune_run(key, cand, [&](int k) {
+            const int tile = k / 1000;
+            build_K_syrk(p, e->T, e->K, e->Kpart, k % 1000, tile == 128 ? e->tiles128 : e->tiles, e->s, tile);
+        }, e->s);
     }
-    if (c >= 1 && c <= e->ksplit_max) e->ksplit = c;
+    if ((c / 1000 == 64 || c / 1000 == 128) && c % 1000 >= 1 && c % 1000 <= e->ksplit_max) {
+        e->ktile = c / 1000;
+        e->ksplit = c % 1000;
+        if (e->ktile == 64) e->ksplit64 = e->ksplit;
+    }
     snprintf(key, sizeof(key), "jrows:%d:%d", e->nup, t->df_nbf);
     c = tune_lookup(key);
     if (c < 0) {
@@ -1026,7 +1045,7 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
         build_K_halftransform(p, e->Cocc, e->T, e->s);
         tstop(e, TINYSCF_T_K_HT);
         tstart(e, TINYSCF_T_K_SYRK);
-        build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->tiles, e->s);
+        build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 128 ? e->tiles128 : e->tiles, e->s, e->ktile);
         tstop(e, TINYSCF_T_K_SYRK);
     }
     if (Kuse != e->K)
@@ -1819,7 +1838,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         m.nocc = o;
         m.nup = e->nup;
         m.jblk = e->jblk;
-        m.ksplit = e->ksplit;
+        m.ksplit = e->ksplit64;   // the batched exchange runs the 64 x 64 tiles
         m.max_diis = (t->max_diis < 1 || t->max_diis > MAX_DIIS) ? MAX_DIIS : t->max_diis;
         m.up_i = e->up_i;
         m.up_j = e->up_j;
@@ -1859,7 +1878,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         c_naux256.push_back((na + 255) / 256);
         c_nup64.push_back((e->nup + 63) / 64);
         c_half.push_back(n * ((o + 63) / 64) * ((na + 63) / 64));
-        c_syrk.push_back(nt * (nt + 1) / 2 * e->ksplit);
+        c_syrk.push_back(nt * (nt + 1) / 2 * e->ksplit64);
         c_nn256.push_back((int) ((nn + 255) / 256));
         c_efb.push_back(ENERGY_BLOCKS);
         xtf.push_back({n, n, n, n, n, n, e->X, e->F, e->tmp, 1.0, 0.0});

@@ -138,8 +138,10 @@ int  build_J_part_blocks(const FockPlan &p);
 // K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s);
 // ... then K = T T^T over upper 64x64 tiles (d_tiles: (bi,bj), bi <= bj), split-K, mirrored.
+// tile = 64 (k_syrk_part) or 128 (k_syrk_part128); d_tiles lists the upper
+// tile pairs for that tile size
 void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_Kpart, int ksplit,
-                  const int2 *d_tiles, cudaStream_t s);
+                  const int2 *d_tiles, cudaStream_t s, int tile = 64);
 size_t build_K_part_elems(const FockPlan &p, int ksplit);
 // F = H + 2J - K and e_part[b] = partial sums of D .* (F + H) (TinySCF.c:367-376).
 void build_F_energy(const double *d_H, const double *d_J, const double *d_K, const double *d_D,
