@@ -40,6 +40,8 @@ CONFIGS = {
     "c10h22": "C10H22 all-trans alkane, C-C 1.54 A, C-H 1.09 A",
     "c20h42": "C20H42 all-trans alkane, C-C 1.54 A, C-H 1.09 A",
     "c40h82": "C40H82 all-trans alkane, C-C 1.54 A, C-H 1.09 A",
+    "waters256": "256 water clusters of 2-32 molecules (seeds 0-255: random rigid rotations and translations, "
+                 "O-O >= 2.6 A, 30 A^3 per molecule), batched SCF",
 }
 METRIC = "SCF time-to-converge at 1e-8 Eh"
 
@@ -117,7 +119,8 @@ def cpu_reference(config, ene_tol, nsolves, threads):
     if not os.path.exists(REF_BENCH):
         return None
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
-    out = subprocess.run([REF_BENCH, BAS, DFBAS, os.path.join(DATA, config + ".xyz"), "100", repr(ene_tol),
+    path = config if config.endswith(".xyz") else os.path.join(DATA, config + ".xyz")
+    out = subprocess.run([REF_BENCH, BAS, DFBAS, path, "100", repr(ene_tol),
                           str(nsolves)], capture_output=True, text=True, env=env)
     if out.returncode != 0:
         raise RuntimeError("ref_bench failed: " + out.stderr[-500:])
@@ -145,10 +148,39 @@ def ref_scale(config):
     return sample, f(config) / f(sample)
 
 
+def run_reference_waters(args, threads):
+    """The reference solves every 64th cluster (4 of 256) one by one; their SCF
+    times are summed and scaled by 64."""
+    import tempfile
+    td = tempfile.mkdtemp()
+    paths = water_cluster_files(td, [0, 64, 128, 192])
+    tot, iters = 0.0, []
+    for p in paths:
+        res = cpu_reference(p, args.ene_tol, 1, threads)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built"}))
+            return
+        tot += res[1][0][2]
+        iters.append(res[1][0][0])
+    t = tot * 64
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": t, "unit": "s", "n_gpus": args.gpus, "steps": 1,
+        "warmup": 0, "ms_per_step": 1e3 * t, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "waters256: " + CONFIGS["waters256"], "sample_iterations": iters},
+        "cpu_baseline": {"value": t, "unit": "s", "cores": threads, "kind": "reference",
+                         "sample": "SCF solves of clusters 0, 64, 128, 192 (reference C sources, OpenMP + OpenBLAS; "
+                                   "set-up excluded), summed and scaled by 64"},
+        "e2e": {"value": t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if args.config == "waters256":
+        run_reference_waters(args, threads)
+        return
     sample, scale = ref_scale(args.config)
     res = cpu_reference(sample, args.ene_tol, args.warmup + args.steps, threads)
     if res is None:
@@ -347,6 +379,122 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def water_cluster_files(tmpdir, seeds):
+    sys.path.insert(0, PKG)
+    import geometry
+    paths = []
+    for sd in seeds:
+        p = os.path.join(tmpdir, "w%d.xyz" % sd)
+        geometry.write_xyz(p, geometry.water_cluster(sd))
+        paths.append(p)
+    return paths
+
+
+def run_batch(args, rank, world, local_rank):
+    """256 water clusters: batched SCF (one launch per phase over all clusters
+    of a wave) from the learned guess, against the same clusters solved one by
+    one with SAD (sampled: every 8th cluster, scaled by 8). Waves are filled
+    until less than 24 GB of device memory is free. Strong scaling over ranks."""
+    import tempfile
+    sys.path.insert(0, PKG)
+    import tinyscf
+    tinyscf.load_library()
+    tinyscf.set_autotune(False)            # many distinct sizes: keep the set-up short
+    seeds = list(range(256))[rank::world]
+    td = tempfile.mkdtemp()
+    paths = water_cluster_files(td, seeds)
+    sizes = []
+    for p in paths:
+        with open(p) as f:
+            sizes.append(int(f.readline()))
+    order = sorted(range(len(paths)), key=lambda k: -sizes[k])
+
+    def engine(p, guess):
+        e = tinyscf.TinySCF(BAS, DFBAS, p, 100, device=local_rank)
+        e.setup(guess=guess)
+        e.s.ene_tol = args.ene_tol
+        return e
+
+    # warm-up: one small batch (kernels, cuSOLVER handles)
+    w = [engine(paths[order[-1]], tinyscf.GUESS_LEARNED), engine(paths[order[-2]], tinyscf.GUESS_LEARNED)]
+    bw = tinyscf.TinySCFBatch(w)
+    bw.do_SCF()
+    bw.free()
+    for e in w:
+        e.free()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    scf_ms, guess_ms, waves, launches, iters, setup_s = 0.0, 0.0, 0, 0, [], 0.0
+    k = 0
+    while k < len(order):
+        wave = []
+        t0 = time.perf_counter()
+        while k < len(order):
+            e = engine(paths[order[k]], tinyscf.GUESS_LEARNED)
+            wave.append(e)
+            guess_ms += e.timings()["GUESS"]
+            k += 1
+            if tinyscf.device_memory(local_rank)[0] < 24 * 2 ** 30:
+                break
+        setup_s += time.perf_counter() - t0
+        b = tinyscf.TinySCFBatch(wave)
+        b.do_SCF()
+        ms, it, nl = b.stats()
+        scf_ms += ms
+        launches += nl
+        waves += 1
+        iters += [e.s.iter for e in wave]
+        b.free()
+        for e in wave:
+            e.free()
+    clk = clocks.stop()
+    # one by one, sampled
+    sample = order[::8]
+    seq_sad, seq_ml, it_sad = 0.0, 0.0, []
+    for kk in sample:
+        for guess in (None, tinyscf.GUESS_LEARNED):
+            e = engine(paths[kk], guess)
+            g = e.timings()["GUESS"]
+            e.do_SCF()
+            t = g + e.timings()["SCF"]
+            if guess is None:
+                seq_sad += t
+                it_sad.append(e.s.iter)
+            else:
+                seq_ml += t
+            e.free()
+    scale = len(order) / len(sample)
+    total = (scf_ms + guess_ms) * 1e-3
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl")
+        t = torch.tensor([total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": total, "unit": "s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "waters256: " + CONFIGS["waters256"] + ", cc-pVDZ / cc-pVDZ-RI (Cartesian)",
+                       "clusters": len(order), "basis_functions": [min(sizes) // 3 * 25, max(sizes) // 3 * 25],
+                       "timed": "learned guess + batched SCF of every cluster (device time), set-up excluded",
+                       "waves": waves, "batched_launches": launches,
+                       "iterations": {"learned_batched_mean": statistics.mean(iters), "max": max(iters),
+                                      "sad_sample_mean": statistics.mean(it_sad)},
+                       "sequential_sad_plain_s": seq_sad * scale * 1e-3,
+                       "sequential_learned_s": seq_ml * scale * 1e-3,
+                       "sequential_sample": "every 8th cluster by size (%d), scaled by %.1f" % (len(sample), scale),
+                       "speedup_vs_sequential_sad": seq_sad * scale * 1e-3 / total,
+                       "setup_s": setup_s, "guess_s": guess_ms * 1e-3, "autotune": "off"},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -364,6 +512,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.config == "waters256":
+        run_batch(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

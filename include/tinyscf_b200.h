@@ -176,6 +176,9 @@ TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *
  * (64x64, 32x32, 128x64), the split count of the FP64 exchange and the row
  * blocks of the J first pass. All candidates compute the same values. */
 TINYSCF_API int TinySCF_set_autotune(int on);
+/* Free and total device memory in bytes (cudaMemGetInfo) of a CUDA device,
+ * for callers that size batches of molecules to what fits. */
+TINYSCF_API int TinySCF_device_memory(int device, long long *free_bytes, long long *total_bytes);
 /* The tuner's table as text ("key -> choice (ms) [candidate: ms]..."); writes
  * at most len bytes into buf and returns the full length. */
 TINYSCF_API int TinySCF_autotune_report(char *buf, int len);

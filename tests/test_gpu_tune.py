@@ -31,5 +31,5 @@ def test_tuned_engine_matches_untuned():
     assert np.abs(K0 - K1).max() < 1e-11
     assert np.abs(B0 - B1).max() == 0.0          # integral launch shapes do not change a single value
     rep = tinyscf.autotune_report()
-    for key in ("3c:", "dgemm:", "ksyrk:", "jrows:"):
+    for key in ("3c:", "dgemm:", "ksyrk:", "khalf:", "jrows:"):
         assert key in rep, rep

@@ -95,6 +95,15 @@ __global__ void __launch_bounds__(256) k_halftransform(const double *__restrict_
     half_tile(B, C, csr_j, csr_u, displs, nocc, naux, T, blockIdx.z, blockIdx.y * KT_M, blockIdx.x * KT_N);
 }
 
+__global__ void __launch_bounds__(256, 1) k_halftransform_wide(const double *__restrict__ B, const double *__restrict__ C,
+                                                               const int *__restrict__ csr_j,
+                                                               const int *__restrict__ csr_u,
+                                                               const int *__restrict__ displs, int nocc, int naux,
+                                                               double *__restrict__ T)
+{
+    half_tile_wide(B, C, csr_j, csr_u, displs, nocc, naux, T, blockIdx.z, blockIdx.y * KH_S, blockIdx.x * KH_P);
+}
+
 // K partial tiles: upper tile pairs (bi <= bj) of 64x64, split over the
 // flattened Q = nocc*naux index. Kpart[split][i][j].
 __global__ void __launch_bounds__(256) k_syrk_part(const double *__restrict__ T, int nbf, long long Q, long long qchunk,
@@ -132,11 +141,16 @@ __global__ void k_syrk_reduce(const double *Kpart, int nsplit, int nbf, double *
 
 size_t build_K_part_elems(const FockPlan &p, int ksplit) { return (size_t) ksplit * p.nbf * p.nbf; }
 
-void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s)
+void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide)
 {
-    dim3 g1((p.naux + KT_N - 1) / KT_N, (p.nocc + KT_M - 1) / KT_M, p.nbf);
     g_launches++;
-    k_halftransform<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
+    if (wide) {
+        dim3 g1((p.naux + KH_P - 1) / KH_P, (p.nocc + KH_S - 1) / KH_S, p.nbf);
+        k_halftransform_wide<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
+    } else {
+        dim3 g1((p.naux + KT_N - 1) / KT_N, (p.nocc + KT_M - 1) / KT_M, p.nbf);
+        k_halftransform<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
+    }
 }
 
 void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_Kpart, int ksplit, const int2 *d_tiles,

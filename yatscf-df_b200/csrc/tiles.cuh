@@ -129,6 +129,78 @@ __device__ __forceinline__ void half_tile(const double *__restrict__ B, const do
     }
 }
 
+// ---- K half-transform tile, 64 (s) x 256 (P) outputs per 256 threads (4 x 16
+// per thread, fewer shared-memory reads per FMA than the 64 x 64 tile), next
+// CSR chunk prefetched into registers. Same summation order as half_tile.
+constexpr int KH_S = 64, KH_P = 256;
+
+__device__ __forceinline__ void half_tile_wide(const double *__restrict__ B, const double *__restrict__ C,
+                                               const int *__restrict__ csr_j, const int *__restrict__ csr_u,
+                                               const int *__restrict__ displs, int nocc, int naux,
+                                               double *__restrict__ T, int i, int s0, int p0)
+{
+    __shared__ double As[KT_K][KH_S + 1];
+    __shared__ double Bs[KT_K][KH_P + 1];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int r_beg = displs[i], r_end = displs[i + 1];
+    double acc[4][16];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 16; y++) acc[x][y] = 0.0;
+    double pa[4], pb[16];
+    auto fetch = [&](int r0) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int l = tid + 256 * q, kk = l / KH_S, c = l % KH_S, r = r0 + kk, sg = s0 + c;
+            pa[q] = (r < r_end && sg < nocc) ? C[(size_t) csr_j[r] * nocc + sg] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int l = tid + 256 * q, kk = l / KH_P, c = l % KH_P, r = r0 + kk, pg = p0 + c;
+            pb[q] = (r < r_end && pg < naux) ? B[(size_t) csr_u[r] * naux + pg] : 0.0;
+        }
+    };
+    if (r_beg < r_end) fetch(r_beg);
+    for (int r0 = r_beg; r0 < r_end; r0 += KT_K) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int l = tid + 256 * q;
+            As[l / KH_S][l % KH_S] = pa[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int l = tid + 256 * q;
+            Bs[l / KH_P][l % KH_P] = pb[q];
+        }
+        __syncthreads();
+        if (r0 + KT_K < r_end) fetch(r0 + KT_K);
+#pragma unroll
+        for (int kk = 0; kk < KT_K; kk++) {
+            double a[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[kk][ty + 16 * x];
+#pragma unroll
+            for (int y = 0; y < 16; y++) {
+                const double b = Bs[kk][tx + 16 * y];
+#pragma unroll
+                for (int x = 0; x < 4; x++) acc[x][y] = fma(a[x], b, acc[x][y]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        const int sg = s0 + ty + 16 * x;
+        if (sg >= nocc) continue;
+#pragma unroll
+        for (int y = 0; y < 16; y++) {
+            const int pg = p0 + tx + 16 * y;
+            if (pg < naux) T[((size_t) i * nocc + sg) * naux + pg] = acc[x][y];
+        }
+    }
+}
+
 // ---- K = T T^T partial tile over q in [q_beg, q_end) of the flattened (s,P) index
 __device__ __forceinline__ void syrk_tile(const double *__restrict__ T, int nbf, long long Q, long long q_beg,
                                           long long q_end, int i0, int j0, double *__restrict__ out)

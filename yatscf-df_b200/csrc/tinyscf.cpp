@@ -289,7 +289,7 @@ struct Engine {
     double *B = nullptr;
     double *T = nullptr, *Kpart = nullptr;
     int2 *tiles = nullptr;
-    int ksplit = 1, ksplit_max = 1, ksplit64 = 1, ktile = 64;
+    int ksplit = 1, ksplit_max = 1, ksplit64 = 1, ktile = 64, khwide = 0;
     int2 *tiles128 = nullptr;
     double *Jt = nullptr, *Jpart = nullptr, *Jw = nullptr;
     int jblk = 1, jblk_max = 1;
@@ -942,6 +942,10 @@ int autotune_fock(TinySCF_t t)
         e->ksplit = c % 1000;
         if (e->ktile == 64) e->ksplit64 = e->ksplit;
     }
+    snprintf(key, sizeof(key), "khalf:%d:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf, e->nnz);
+    c = tune_lookup(key);
+    if (c < 0) c = tune_run(key, {0, 1}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
+    if (c == 0 || c == 1) e->khwide = c;
     snprintf(key, sizeof(key), "jrows:%d:%d", e->nup, t->df_nbf);
     c = tune_lookup(key);
     if (c < 0) {
@@ -1042,7 +1046,7 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
         Kuse = e->Kmix;
     } else {
         tstart(e, TINYSCF_T_K_HT);
-        build_K_halftransform(p, e->Cocc, e->T, e->s);
+        build_K_halftransform(p, e->Cocc, e->T, e->s, e->khwide);
         tstop(e, TINYSCF_T_K_HT);
         tstart(e, TINYSCF_T_K_SYRK);
         build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 128 ? e->tiles128 : e->tiles, e->s, e->ktile);
@@ -1932,8 +1936,14 @@ int batch_eigs(TinySCF_batch_t b)
                                                          CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, g.A, n, CUDA_R_64F,
                                                          g.W, CUDA_R_64F, g.dwork, g.dbytes, g.hwork.data(),
                                                          g.hwork.size(), g.info, cnt);
-            if (st != CUSOLVER_STATUS_SUCCESS) return ERR_NUMERIC;
-        } else {
+            if (st != CUSOLVER_STATUS_SUCCESS) {
+                // this size is not taken by the batched solver: one syevd per member from now on
+                g.batched = false;
+                g.eig = eig_create(g.n, b->s);
+                if (!g.eig) return ERR_CUDA;
+            }
+        }
+        if (!g.batched) {
             for (int64_t k = 0; k < cnt; k++)
                 RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
         }
@@ -2023,6 +2033,23 @@ void batch_free_impl(TinySCF_batch_t b)
 }  // namespace
 
 extern "C" {
+
+int TinySCF_device_memory(int device, long long *free_bytes, long long *total_bytes)
+{
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) {
+        cudaGetLastError();
+        return TINYSCF_ERR_CUDA;
+    }
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    size_t f = 0, tot = 0;
+    cudaError_t err = cudaMemGetInfo(&f, &tot);
+    cudaSetDevice(cur);
+    if (err != cudaSuccess) return TINYSCF_ERR_CUDA;
+    if (free_bytes) *free_bytes = (long long) f;
+    if (total_bytes) *total_bytes = (long long) tot;
+    return TINYSCF_OK;
+}
 
 int TinySCF_set_autotune(int on)
 {

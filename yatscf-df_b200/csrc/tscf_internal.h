@@ -136,7 +136,8 @@ void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, dou
              double *d_w, cudaStream_t s);
 int  build_J_part_blocks(const FockPlan &p);
 // K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
-void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s);
+// wide = 1: 64 x 256 tiles (k_halftransform_wide), else 64 x 64
+void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide = 0);
 // ... then K = T T^T over upper 64x64 tiles (d_tiles: (bi,bj), bi <= bj), split-K, mirrored.
 // tile = 64 (k_syrk_part) or 128 (k_syrk_part128); d_tiles lists the upper
 // tile pairs for that tile size

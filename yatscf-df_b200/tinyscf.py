@@ -113,6 +113,7 @@ def load_library(path=LIBPATH):
                                 ip),
         "TinySCF_batch_free": ([ctypes.c_void_p], ip),
         "TinySCF_set_autotune": ([ip], ip),
+        "TinySCF_device_memory": ([ip, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)], ip),
         "TinySCF_autotune_report": ([ctypes.c_char_p, ip], ip),
         "TinySCF_guess_used": ([T], ip),
         "TinySCF_guess_dataset": ([T, dp, fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong], ctypes.c_longlong),
@@ -419,3 +420,13 @@ def autotune_report():
 
 def set_autotune(on):
     load_library().TinySCF_set_autotune(int(bool(on)))
+
+
+def device_memory(device=0):
+    """(free bytes, total bytes) of a CUDA device."""
+    lib = load_library()
+    f, t = ctypes.c_longlong(), ctypes.c_longlong()
+    rc = lib.TinySCF_device_memory(int(device), ctypes.byref(f), ctypes.byref(t))
+    if rc:
+        raise TinySCFError("device_memory: " + STATUS.get(rc, str(rc)))
+    return f.value, t.value
