@@ -424,7 +424,7 @@ def run_batch(args, rank, world, local_rank):
         e.free()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    scf_ms, guess_ms, waves, launches, iters, setup_s = 0.0, 0.0, 0, 0, [], 0.0
+    scf_ms, guess_ms, waves, launches, iters, setup_s, phases = 0.0, 0.0, 0, 0, [], 0.0, {}
     k = 0
     while k < len(order):
         wave = []
@@ -440,6 +440,8 @@ def run_batch(args, rank, world, local_rank):
         b = tinyscf.TinySCFBatch(wave)
         b.do_SCF()
         ms, it, nl = b.stats()
+        for ph, v in b.phase_ms().items():
+            phases[ph] = phases.get(ph, 0.0) + v
         scf_ms += ms
         launches += nl
         waves += 1
@@ -489,7 +491,8 @@ def run_batch(args, rank, world, local_rank):
                        "sequential_learned_s": seq_ml * scale * 1e-3,
                        "sequential_sample": "every 8th cluster by size (%d), scaled by %.1f" % (len(sample), scale),
                        "speedup_vs_sequential_sad": seq_sad * scale * 1e-3 / total,
-                       "setup_s": setup_s, "guess_s": guess_ms * 1e-3, "autotune": "off"},
+                       "setup_s": setup_s, "guess_s": guess_ms * 1e-3, "autotune": "off",
+                       "batched_phase_s": {k: round(v * 1e-3, 3) for k, v in phases.items()}},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
         }
         print(json.dumps(line))

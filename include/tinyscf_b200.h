@@ -197,6 +197,9 @@ TINYSCF_API int TinySCF_batch_do_SCF(TinySCF_batch_t b);
 /* Device time of the last TinySCF_batch_do_SCF (ms), its number of batched
  * iterations (the slowest molecule's count) and the kernels it launched. */
 TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long long *launches);
+/* Device time (ms) of the last TinySCF_batch_do_SCF by phase: [0] J,
+ * [1] K, [2] Fock + energy, [3] DIIS, [4] density; min(n, 5) values. */
+TINYSCF_API int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n);
 TINYSCF_API int TinySCF_batch_free(TinySCF_batch_t b);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */

@@ -6,9 +6,9 @@
 namespace tscf {
 
 struct MolDev {
-    int nbf, naux, nocc, nup, jblk, ksplit, max_diis, pad;
+    int nbf, naux, nocc, nup, jblk, ksplit, max_diis, ktile;   // ktile: 64 or 128 (exchange rank-k tile)
     const int *up_i, *up_j, *up_u, *csr_j, *csr_u, *displs;
-    const int2 *tiles;
+    const int2 *tiles;   // upper tile pairs for ktile
     const double *B, *H, *S, *X;
     double *D, *J, *K, *F, *Fp, *Cocc, *T, *Kpart, *Jt, *Jpart, *Jw, *epart, *E, *tmp, *tmp2, *F0, *R, *eigA;
     DiisState *diis;
@@ -38,7 +38,9 @@ struct BatchPlan {
     const MolDev *mols = nullptr;   // device
     const int *active = nullptr;    // device, 1 while the molecule iterates
     int nmol = 0, naux_max = 0;
-    WorkList nup256, jblk, naux256, nup64, half, syrk, nn256, efb;
+    // half / half_wide and syrk / syrk128 hold the items of the molecules that
+    // use that tile (the other molecules contribute none)
+    WorkList nup256, jblk, naux256, nup64, half, half_wide, syrk, syrk128, nn256, efb;
     BatchGemm g_xtf, g_tx_fp, g_fd, g_fds, g_xtt, g_t2x, g_tx_t2, g_cocc, g_dens;
 };
 

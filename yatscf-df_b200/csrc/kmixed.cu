@@ -137,12 +137,13 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bflo
     lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
-struct HalfArgs {            // half-transform of one CSR row per blockIdx.y
+struct HalfArgs {            // half-transform work items: (CSR row, 128-row block of P)
     const int *row_chunk0;   // [nbf+1] first 64-chunk of each padded CSR row
     float *Tm;               // T master [nbf][Qp] FP32
     __nv_bfloat16 *dTh, *dTl, *Sh, *Sl;   // [nbf][Qp]
     int nocc, naux;
     long long Qp;
+    int n_items, ptiles;     // nbf * ptiles items, ptiles = ceil(naux / 128)
 };
 struct GArgs {               // split-K partial of dT S^T
     double *part;            // [ksplit][nbf][nbf]
@@ -183,8 +184,31 @@ __device__ __forceinline__ void tmem_alloc_warp(uint32_t *slot, uint32_t cols)
 }
 
 // ------------------------------------------------------------------ half-transform
-// CTA (x, y): rows P = 128x..128x+127 of the aux index, CSR row i = y.
-// D[P][s] = sum_r BpT[P][r] CgT[s][r] over the padded CSR row i.
+// Persistent: CTA b takes work items b, b + gridDim.x, ...; item t covers aux
+// rows P = 128 (t % ptiles) .. +127 of CSR row i = t / ptiles:
+//   D[P][s] = sum_r BpT[P][r] CgT[s][r] over the padded CSR row i.
+// The TMA warp runs ahead across items through the shared-memory stages; the
+// MMA warp accumulates item t in TMEM buffer t & 1 while the epilogue warps
+// update T and write the BF16 operands of the G GEMM from the other buffer,
+// so the epilogue's global traffic overlaps the next item's loads and MMAs.
+// All four split products go into one FP32 accumulator: a CSR row has at most
+// a few hundred terms.
+template <bool FIRST>
+__device__ __forceinline__ void mma_chunk4(uint32_t a_hi, uint32_t a_lo, uint32_t b_hi, uint32_t b_lo, uint32_t acc,
+                                           uint32_t idesc)
+{
+#pragma unroll
+    for (int kk = 0; kk < BK / UK; kk++) {
+        const uint32_t off = kk * UK * 2;
+        const uint64_t dah = desc_sw128(a_hi + off), dal = desc_sw128(a_lo + off);
+        const uint64_t dbh = desc_sw128(b_hi + off), dbl = desc_sw128(b_lo + off);
+        umma_bf16(acc, dah, dbh, idesc, (FIRST && kk == 0) ? 0u : 1u);
+        umma_bf16(acc, dah, dbl, idesc, 1u);
+        umma_bf16(acc, dal, dbh, idesc, 1u);
+        umma_bf16(acc, dal, dbl, idesc, 1u);
+    }
+}
+
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(THREADS, 1)
 k_half(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
@@ -194,23 +218,26 @@ k_half(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
     constexpr int B_BYTES = BN * BK * 2;
     constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     constexpr uint32_t ACC_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
-    constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;   // main + corrections
+    constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;   // two accumulator buffers
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
     uint64_t *full = (uint64_t *) (smem + STAGES * STAGE_BYTES);
     uint64_t *empty = full + STAGES;
-    uint64_t *accum = empty + STAGES;
-    uint32_t *tmem_slot = (uint32_t *) (accum + 1);
+    uint64_t *tfull = empty + STAGES;   // [2]
+    uint64_t *tempty = tfull + 2;       // [2]
+    uint32_t *tmem_slot = (uint32_t *) (tempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * UM, i = blockIdx.y;
-    const int kc0 = ha.row_chunk0[i], nk = ha.row_chunk0[i + 1] - kc0;
+    const int n_items = ha.n_items, ptiles = ha.ptiles;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(accum, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], EPI_WARPS);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc_warp(tmem_slot, TMEM_COLS);
@@ -221,84 +248,110 @@ k_half(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
 
     if (warp == 0 && lane == 0) {
         bool ok = true;
-        for (int kb = 0; kb < nk && ok; kb++) {
-            const int s = kb % STAGES;
-            if (kb >= STAGES) ok = mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, 1);
-            if (!ok) break;
-            unsigned char *st = smem + s * STAGE_BYTES;
-            mbar_expect_tx(&full[s], STAGE_BYTES);
-            const int kx = (kc0 + kb) * BK;
-            tma_load_2d(st, &mAh, &full[s], kx, m0);
-            tma_load_2d(st + A_BYTES, &mAl, &full[s], kx, m0);
-            tma_load_2d(st + 2 * A_BYTES, &mBh, &full[s], kx, 0);
-            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, &full[s], kx, 0);
+        long long g = 0;   // chunk counter across this CTA's items
+        for (int t = blockIdx.x; t < n_items && ok; t += gridDim.x) {
+            const int i = t / ptiles, m0 = (t % ptiles) * UM;
+            const int kc0 = ha.row_chunk0[i], nk = ha.row_chunk0[i + 1] - kc0;
+            for (int kb = 0; kb < nk && ok; kb++, g++) {
+                const int s = (int) (g % STAGES);
+                if (g >= STAGES) ok = mbar_wait(&empty[s], (uint32_t) (((g / STAGES) - 1) & 1), 1);
+                if (!ok) break;
+                unsigned char *st = smem + s * STAGE_BYTES;
+                mbar_expect_tx(&full[s], STAGE_BYTES);
+                const int kx = (kc0 + kb) * BK;
+                tma_load_2d(st, &mAh, &full[s], kx, m0);
+                tma_load_2d(st + A_BYTES, &mAl, &full[s], kx, m0);
+                tma_load_2d(st + 2 * A_BYTES, &mBh, &full[s], kx, 0);
+                tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, &full[s], kx, 0);
+            }
         }
-        for (int kb = (nk > STAGES ? nk - STAGES : 0); kb < nk; kb++)
-            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, 2);
+        // copies in flight finish before the CTA exits
+        for (long long q = (g > STAGES ? g - STAGES : 0); q < g; q++)
+            mbar_wait(&full[q % STAGES], (uint32_t) ((q / STAGES) & 1), 2);
     } else if (warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16(BN);
         bool ok = true;
-        for (int kb = 0; kb < nk && ok; kb++) {
-            const int s = kb % STAGES;
-            ok = mbar_wait(&full[s], (kb / STAGES) & 1, 3);
+        long long g = 0;
+        int li = 0;
+        for (int t = blockIdx.x; t < n_items && ok; t += gridDim.x, li++) {
+            const int i = t / ptiles;
+            const int nk = ha.row_chunk0[i + 1] - ha.row_chunk0[i];
+            const int b = li & 1;
+            if (li >= 2) ok = mbar_wait(&tempty[b], (uint32_t) (((li >> 1) - 1) & 1), 5);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
-            // the half-transform is bandwidth-bound: the fourth (lo*lo) product is free
-            mma_chunk<true>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + B_BYTES, tmem,
-                            tmem + ACC_COLS, idesc, kb == 0);
-            umma_commit(&empty[s]);
+            const uint32_t acc = tmem + b * ACC_COLS;
+            for (int kb = 0; kb < nk && ok; kb++, g++) {
+                const int s = (int) (g % STAGES);
+                ok = mbar_wait(&full[s], (uint32_t) ((g / STAGES) & 1), 3);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
+                if (kb == 0) mma_chunk4<true>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + B_BYTES,
+                                              acc, idesc);
+                else mma_chunk4<false>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + B_BYTES, acc,
+                                       idesc);
+                umma_commit(&empty[s]);
+            }
+            umma_commit(&tfull[b]);
         }
-        umma_commit(accum);
     } else if (warp >= 2) {
-        const bool ok = (nk > 0) ? mbar_wait(accum, 0, 4) : true;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int quad = warp & 3, half = (warp - 2) >> 2;
         const int row = quad * 32 + lane;
         const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16);
-        const int P = m0 + row;
-        const size_t base = (size_t) i * ha.Qp + P;
         uint32_t rm[32];
         float dtv[32];
-        for (int c0 = half * 32; c0 < BN; c0 += 64) {
-            if (nk > 0 && ok) {
-                tmem_ld32(tq + c0, rm);
+        bool ok = true;
+        int li = 0;
+        for (int t = blockIdx.x; t < n_items && ok; t += gridDim.x, li++) {
+            const int i = t / ptiles, m0 = (t % ptiles) * UM;
+            const int nk = ha.row_chunk0[i + 1] - ha.row_chunk0[i];
+            const int b = li & 1;
+            ok = mbar_wait(&tfull[b], (uint32_t) ((li >> 1) & 1), 4);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int P = m0 + row;
+            const size_t base = (size_t) i * ha.Qp + P;
+            for (int c0 = half * 32; c0 < BN; c0 += 64) {
+                if (nk > 0) {
+                    tmem_ld32(tq + b * ACC_COLS + c0, rm);
 #pragma unroll
-                for (int q = 0; q < 32; q++) dtv[q] = __uint_as_float(rm[q]);
-                tmem_ld32(tq + ACC_COLS + c0, rm);
+                    for (int q = 0; q < 32; q++) dtv[q] = __uint_as_float(rm[q]);
+                } else {
 #pragma unroll
-                for (int q = 0; q < 32; q++) dtv[q] += __uint_as_float(rm[q]);
-            } else {
+                    for (int q = 0; q < 32; q++) dtv[q] = 0.f;
+                }
+                if (P >= ha.naux) continue;
 #pragma unroll
-                for (int q = 0; q < 32; q++) dtv[q] = 0.f;
-            }
-            if (P >= ha.naux) continue;
+                for (int h16 = 0; h16 < 32; h16 += 16) {
+                    float told[16];
 #pragma unroll
-            for (int h16 = 0; h16 < 32; h16 += 16) {
-            float told[16];
+                    for (int q = h16; q < h16 + 16; q++) {   // loads first: 16 in flight per thread
+                        const int s = c0 + q;
+                        told[q - h16] = (s < ha.nocc) ? ha.Tm[base + (size_t) s * ha.naux] : 0.f;
+                    }
 #pragma unroll
-            for (int q = h16; q < h16 + 16; q++) {   // loads first: 16 in flight per thread
-                const int s = c0 + q;
-                told[q - h16] = (s < ha.nocc) ? ha.Tm[base + (size_t) s * ha.naux] : 0.f;
-            }
-#pragma unroll
-            for (int q = h16; q < h16 + 16; q++) {
-                const int s = c0 + q;
-                if (s < ha.nocc) {
-                    const size_t idx = base + (size_t) s * ha.naux;
-                    const float dt = dtv[q];
-                    const float tnew = told[q - h16] + dt;
-                    ha.Tm[idx] = tnew;
-                    __nv_bfloat16 h, l;
-                    split_bf16(dt, h, l);
-                    ha.dTh[idx] = h;
-                    ha.dTl[idx] = l;
-                    split_bf16(told[q - h16] + tnew, h, l);
-                    ha.Sh[idx] = h;
-                    ha.Sl[idx] = l;
+                    for (int q = h16; q < h16 + 16; q++) {
+                        const int s = c0 + q;
+                        if (s < ha.nocc) {
+                            const size_t idx = base + (size_t) s * ha.naux;
+                            const float dt = dtv[q];
+                            const float tnew = told[q - h16] + dt;
+                            ha.Tm[idx] = tnew;
+                            __nv_bfloat16 h, l;
+                            split_bf16(dt, h, l);
+                            ha.dTh[idx] = h;
+                            ha.dTl[idx] = l;
+                            split_bf16(told[q - h16] + tnew, h, l);
+                            ha.Sh[idx] = h;
+                            ha.Sl[idx] = l;
+                        }
+                    }
                 }
             }
-            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[b])) : "memory");
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -454,7 +507,7 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
 template <int BN, int STAGES>
 constexpr int half_smem_bytes()
 {
-    return STAGES * (2 * UM * BK * 2 + 2 * BN * BK * 2) + 1024 + 8 * (2 * STAGES + 1) + 16;
+    return STAGES * (2 * UM * BK * 2 + 2 * BN * BK * 2) + 1024 + 8 * (2 * STAGES + 4) + 16;
 }
 template <int STAGES>
 constexpr int gemm_smem_bytes()
@@ -736,17 +789,23 @@ void kmix_reset(KMix *k, cudaStream_t s)
 }
 
 template <int BN>
-static int launch_half(const KMix *k, const HalfArgs &ha, cudaStream_t s)
+static int launch_half(const KMix *k, HalfArgs ha, cudaStream_t s)
 {
-    constexpr int STAGES = 2;
+    constexpr int STAGES = BN <= 112 ? 3 : 2;   // within 227 KB of shared memory
     constexpr int SMEM = half_smem_bytes<BN, STAGES>();
+    static_assert(SMEM <= 227 * 1024, "half-transform stages exceed shared memory");
     static bool attr_set = false;
     if (!attr_set) {
         if (cudaFuncSetAttribute(k_half<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
             return ERR_CUDA;
         attr_set = true;
     }
-    dim3 grid((k->naux + UM - 1) / UM, k->nbf);
+    ha.ptiles = (k->naux + UM - 1) / UM;
+    ha.n_items = k->nbf * ha.ptiles;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::max(1, std::min(ha.n_items, nsm));
     k_half<BN, STAGES><<<grid, THREADS, SMEM, s>>>(k->mBh, k->mBl, k->mCh, k->mCl, ha);
     g_launches++;
     return OK;
@@ -789,7 +848,7 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     dim3 gg((unsigned) ((k->rp + 255) / 256), k->bn_half);
     k_gather_dc<<<gg, 256, 0, s>>>(k->dC, k->pad_entry, k->csr_j, o, k->rp, k->Ch, k->Cl);
     g_launches += 3;
-    HalfArgs ha{k->row_chunk0, k->Tm, k->dTh, k->dTl, k->Sh, k->Sl, o, k->naux, k->Qp};
+    HalfArgs ha{k->row_chunk0, k->Tm, k->dTh, k->dTl, k->Sh, k->Sl, o, k->naux, k->Qp, 0, 0};
     int rc;
     switch (k->bn_half) {
     case 16: rc = launch_half<16>(k, ha, s); break;

@@ -771,6 +771,12 @@ int sparsity_impl(TinySCF_t t)
     e->ksplit64 = e->ksplit;
     const int h128 = std::max(1, std::min(64, (2 * 148 + ntiles2 - 1) / ntiles2));
     e->ksplit_max = std::min(64, 2 * std::max(e->ksplit, h128));   // room for the autotuner's candidates
+    // untuned defaults by size: the larger register tiles pay off once there are enough of them
+    if (nbf >= 384) {
+        e->ktile = 128;
+        e->ksplit = h128;
+    }
+    e->khwide = naux >= 1024 ? 1 : 0;
     RC(dalloc(e, &e->Kpart, (size_t) e->ksplit_max * nbf * nbf));
     {
         std::vector<int2> tl, tl2;
@@ -928,7 +934,7 @@ int autotune_fock(TinySCF_t t)
         const int nt2 = (t->nbasfuncs + 127) / 128, ntiles2 = nt2 * (nt2 + 1) / 2;
         const int h128 = std::max(1, std::min(64, (2 * 148 + ntiles2 - 1) / ntiles2));
         std::vector<int> cand;
-        for (int v : {std::max(1, e->ksplit / 2), e->ksplit, std::min(e->ksplit_max, 2 * e->ksplit)})
+        for (int v : {std::max(1, e->ksplit64 / 2), e->ksplit64, std::min(e->ksplit_max, 2 * e->ksplit64)})
             if (std::find(cand.begin(), cand.end(), 64000 + v) == cand.end()) cand.push_back(64000 + v);
         for (int v : {std::max(1, h128 / 2), h128, std::min(e->ksplit_max, 2 * h128)})
             if (std::find(cand.begin(), cand.end(), 128000 + v) == cand.end()) cand.push_back(128000 + v);
@@ -1731,6 +1737,9 @@ struct TinySCF_batch_struct {
     double scf_ms = 0.0;
     int iterations = 0;
     long long launches = 0;
+    // per-phase device time of the last batched SCF: J, K, Fock + energy, DIIS, density
+    cudaEvent_t pev[6] = {};
+    double phase_ms[5] = {};
 };
 
 namespace {
@@ -1787,6 +1796,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     TSCF_CUDA_CHECK(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
     TSCF_CUDA_CHECK(cudaEventCreate(&b->ev0));
     TSCF_CUDA_CHECK(cudaEventCreate(&b->ev1));
+    for (auto &ev : b->pev) TSCF_CUDA_CHECK(cudaEventCreate(&ev));
     if (cusolverDnCreate(&b->h) != CUSOLVER_STATUS_SUCCESS || cusolverDnCreateParams(&b->params) != CUSOLVER_STATUS_SUCCESS)
         return ERR_CUDA;
     cusolverDnSetStream(b->h, b->s);
@@ -1827,7 +1837,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     }
     // per-molecule descriptors and work lists
     std::vector<MolDev> md(nmol);
-    std::vector<int> c_nup256, c_jblk, c_naux256, c_nup64, c_half, c_syrk, c_nn256, c_efb;
+    std::vector<int> c_nup256, c_jblk, c_naux256, c_nup64, c_half, c_halfw, c_syrk, c_syrk128, c_nn256, c_efb;
     std::vector<GemmDesc> xtf, txfp, fd, fds, xtt, t2x, txt2, cocc, dens;
     int naux_max = 1;
     for (int k = 0; k < nmol; k++) {
@@ -1842,7 +1852,8 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         m.nocc = o;
         m.nup = e->nup;
         m.jblk = e->jblk;
-        m.ksplit = e->ksplit64;   // the batched exchange runs the 64 x 64 tiles
+        m.ksplit = e->ksplit;
+        m.ktile = e->ktile;
         m.max_diis = (t->max_diis < 1 || t->max_diis > MAX_DIIS) ? MAX_DIIS : t->max_diis;
         m.up_i = e->up_i;
         m.up_j = e->up_j;
@@ -1850,7 +1861,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         m.csr_j = e->csr_j;
         m.csr_u = e->csr_u;
         m.displs = e->csr_displs;
-        m.tiles = e->tiles;
+        m.tiles = e->ktile == 128 ? e->tiles128 : e->tiles;
         m.B = e->B;
         m.H = e->H;
         m.S = e->S;
@@ -1881,8 +1892,11 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         c_jblk.push_back(e->jblk);
         c_naux256.push_back((na + 255) / 256);
         c_nup64.push_back((e->nup + 63) / 64);
-        c_half.push_back(n * ((o + 63) / 64) * ((na + 63) / 64));
-        c_syrk.push_back(nt * (nt + 1) / 2 * e->ksplit64);
+        c_half.push_back(e->khwide ? 0 : n * ((o + 63) / 64) * ((na + 63) / 64));
+        c_halfw.push_back(e->khwide ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);
+        const int nt2 = (n + 127) / 128;
+        c_syrk.push_back(e->ktile == 64 ? nt * (nt + 1) / 2 * e->ksplit : 0);
+        c_syrk128.push_back(e->ktile == 128 ? nt2 * (nt2 + 1) / 2 * e->ksplit : 0);
         c_nn256.push_back((int) ((nn + 255) / 256));
         c_efb.push_back(ENERGY_BLOCKS);
         xtf.push_back({n, n, n, n, n, n, e->X, e->F, e->tmp, 1.0, 0.0});
@@ -1912,7 +1926,9 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     RC(make_list(b, c_naux256, p.naux256));
     RC(make_list(b, c_nup64, p.nup64));
     RC(make_list(b, c_half, p.half));
+    RC(make_list(b, c_halfw, p.half_wide));
     RC(make_list(b, c_syrk, p.syrk));
+    RC(make_list(b, c_syrk128, p.syrk128));
     RC(make_list(b, c_nn256, p.nn256));
     RC(make_list(b, c_efb, p.efb));
     RC(make_gemm(b, xtf, true, false, p.g_xtf));
@@ -1965,22 +1981,34 @@ int batch_scf_impl(TinySCF_batch_t b)
     }
     TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
     const long long l0 = g_launches;
+    for (double &v : b->phase_ms) v = 0.0;
     cudaEventRecord(b->ev0, b->s);
     int it = 0;
     for (;; it++) {
         bool any = false;
         for (int v : act) any |= v != 0;
         if (!any) break;
+        cudaEventRecord(b->pev[0], b->s);
         batch_j(b->plan, b->s);
+        cudaEventRecord(b->pev[1], b->s);
         batch_k(b->plan, b->s);
+        cudaEventRecord(b->pev[2], b->s);
         batch_fock(b->plan, b->d_Eall, b->s);
+        cudaEventRecord(b->pev[3], b->s);
         batch_diis(b->plan, it >= 2, b->s);
+        cudaEventRecord(b->pev[4], b->s);
         batch_copy_fp(b->plan, b->s);
         RC(batch_eigs(b));
         batch_gemm(b->plan.g_cocc, b->d_active, b->s);
         batch_gemm(b->plan.g_dens, b->d_active, b->s);
+        cudaEventRecord(b->pev[5], b->s);
         TSCF_CUDA_CHECK(cudaMemcpyAsync(Eh.data(), b->d_Eall, sizeof(double) * nmol, cudaMemcpyDeviceToHost, b->s));
         TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
+        for (int q = 0; q < 5; q++) {
+            float pm = 0.f;
+            cudaEventElapsedTime(&pm, b->pev[q], b->pev[q + 1]);
+            b->phase_ms[q] += pm;
+        }
         TSCF_CUDA_CHECK(cudaGetLastError());
         for (int k = 0; k < nmol; k++) {
             if (!act[k]) continue;
@@ -2025,6 +2053,8 @@ void batch_free_impl(TinySCF_batch_t b)
     for (void *p : b->mem) cudaFree(p);
     if (b->params) cusolverDnDestroyParams(b->params);
     if (b->h) cusolverDnDestroy(b->h);
+    for (auto &ev : b->pev)
+        if (ev) cudaEventDestroy(ev);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->s) cudaStreamDestroy(b->s);
@@ -2092,6 +2122,13 @@ int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long
     if (scf_ms) *scf_ms = b->scf_ms;
     if (iterations) *iterations = b->iterations;
     if (launches) *launches = b->launches;
+    return TINYSCF_OK;
+}
+
+int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n)
+{
+    if (!b || !ms) return TINYSCF_ERR_STATE;
+    for (int q = 0; q < n && q < 5; q++) ms[q] = b->phase_ms[q];
     return TINYSCF_OK;
 }
 

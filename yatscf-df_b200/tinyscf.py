@@ -112,6 +112,7 @@ def load_library(path=LIBPATH):
         "TinySCF_batch_stats": ([ctypes.c_void_p, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)],
                                 ip),
         "TinySCF_batch_free": ([ctypes.c_void_p], ip),
+        "TinySCF_batch_phase_ms": ([ctypes.c_void_p, dp, ip], ip),
         "TinySCF_set_autotune": ([ip], ip),
         "TinySCF_device_memory": ([ip, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)], ip),
         "TinySCF_autotune_report": ([ctypes.c_char_p, ip], ip),
@@ -402,6 +403,12 @@ class TinySCFBatch:
         nl = ctypes.c_longlong()
         self.lib.TinySCF_batch_stats(self.b, ctypes.byref(ms), ctypes.byref(it), ctypes.byref(nl))
         return ms.value, it.value, nl.value
+
+    def phase_ms(self):
+        """{phase: device ms} of the last batched SCF."""
+        ms = np.zeros(5)
+        self.lib.TinySCF_batch_phase_ms(self.b, _dptr(ms), 5)
+        return dict(zip(("J", "K", "FOCK", "DIIS", "DENSITY"), (float(v) for v in ms)))
 
     def free(self):
         if self.b:
