@@ -155,7 +155,7 @@ struct GArgs {               // split-K partial of dT S^T
 constexpr int EPI_WARPS = 8;                  // two warps per TMEM lane quadrant
 constexpr int THREADS = 64 + 32 * EPI_WARPS;  // TMA warp, MMA warp, epilogue warps
 constexpr int SEG_CHUNKS = 4;                 // G: drain the accumulator every 256 K
-constexpr int FLUSH_SEGS = 8;                 // G: fold the FP32 register sums into FP64 every 2048 K
+constexpr int MAX_SEGS = 64;                  // G: at most 64 segment results summed in FP32 registers per split
 
 // One k-chunk (64 K) of split-BF16 MMAs: hi*hi into acc_main, hi*lo + lo*hi
 // into acc_corr. Keeping the small correction terms apart means the large
@@ -365,9 +365,10 @@ k_half(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
 // ------------------------------------------------------------------ G = dT S^T, split-K
 // CTA (x, y, z): output tile rows 128x.., cols 128y.., K chunks of split z.
 // The K range is cut into segments of SEG_CHUNKS chunks; each segment
-// accumulates in one of two TMEM buffers (main 128 cols + corrections 128
-// cols each, 512 cols in all) while the epilogue warps drain the other one
-// into FP64 registers, so no FP32 accumulation runs longer than 256 K.
+// accumulates in one of two TMEM buffers (hi*hi in 128 columns, hi*lo + lo*hi
+// in another 128) while the epilogue warps drain the other buffer into FP32
+// registers, so no TMEM accumulation runs longer than 256 K. The register
+// sums of a split (at most MAX_SEGS segments) are written once, as FP64.
 template <int STAGES>
 __global__ void __launch_bounds__(THREADS, 1)
 k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
@@ -377,6 +378,7 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
     constexpr int A_BYTES = UM * BK * 2, B_BYTES = BN * BK * 2;
     constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     constexpr uint32_t TMEM_COLS = 512;
+    constexpr int WC = BN / 2;                 // output columns per epilogue warp
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
     uint64_t *full = (uint64_t *) (smem + STAGES * STAGE_BYTES);
@@ -432,7 +434,7 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
             if (seg >= 2) ok = mbar_wait(&tempty[b], ((seg >> 1) - 1) & 1, 13);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t acc_main = tmem + b * 256, acc_corr = acc_main + 128;
+            const uint32_t acc_main = tmem + b * 256;
             const int kend = min(nk, (seg + 1) * SEG_CHUNKS);
             for (; kb < kend && ok; kb++) {
                 const int s = kb % STAGES;
@@ -440,8 +442,8 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
-                mma_chunk<false>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + B_BYTES, acc_main,
-                                 acc_corr, idesc, kb == seg * SEG_CHUNKS);
+                const uint32_t a_lo = a_hi + A_BYTES, b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+                mma_chunk<false>(a_hi, a_lo, b_hi, b_lo, acc_main, acc_main + 128, idesc, kb == seg * SEG_CHUNKS);
                 umma_commit(&empty[s]);
             }
             umma_commit(&tfull[b]);
@@ -451,23 +453,23 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
         const int row = quad * 32 + lane;
         const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16) + half * 64;
         const int gi = m0 + row;
-        const int lim = ga.nbf - (n0 + half * 64);
-        double *o = ga.part + (size_t) blockIdx.z * ga.nbf * ga.nbf + (size_t) gi * ga.nbf + n0 + half * 64;
+        const int lim = ga.nbf - (n0 + half * WC);
+        double *o = ga.part + (size_t) blockIdx.z * ga.nbf * ga.nbf + (size_t) gi * ga.nbf + n0 + half * WC;
         const bool own = gi < ga.nbf;
-        // FP32 sums of at most FLUSH_SEGS segment results (round-to-nearest adds),
-        // folded into the split's FP64 partial, which this thread alone owns
-        float acc[64];
+        // FP32 sums of the split's segment results (round-to-nearest adds),
+        // written once into the split's FP64 partial, which this thread alone owns
+        float acc[WC];
 #pragma unroll
-        for (int c = 0; c < 64; c++) acc[c] = 0.f;
+        for (int c = 0; c < WC; c++) acc[c] = 0.f;
         uint32_t r[32];
-        bool ok = true, wrote = false;
+        bool ok = true;
         for (int seg = 0; seg < nseg && ok; seg++) {
             const int b = seg & 1;
             ok = mbar_wait(&tfull[b], (seg >> 1) & 1, 15);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-            for (int c0 = 0; c0 < 64; c0 += 32) {
+            for (int c0 = 0; c0 < WC; c0 += 32) {
                 tmem_ld32(tq + b * 256 + c0, r);
                 float t[32];
 #pragma unroll
@@ -479,21 +481,11 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[b])) : "memory");
-            if ((seg + 1) % FLUSH_SEGS == 0 || seg + 1 == nseg) {
-                if (own) {
-#pragma unroll
-                    for (int c = 0; c < 64; c++)
-                        if (c < lim) o[c] = (wrote ? o[c] : 0.0) + (double) acc[c];
-                }
-                wrote = true;
-#pragma unroll
-                for (int c = 0; c < 64; c++) acc[c] = 0.f;
-            }
         }
-        if (!wrote && own) {
+        if (own) {   // zero when the split is empty or a wait gave up
 #pragma unroll
-            for (int c = 0; c < 64; c++)
-                if (c < lim) o[c] = 0.0;
+            for (int c = 0; c < WC; c++)
+                if (c < lim) o[c] = ok ? (double) acc[c] : 0.0;
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -509,10 +501,10 @@ constexpr int half_smem_bytes()
 {
     return STAGES * (2 * UM * BK * 2 + 2 * BN * BK * 2) + 1024 + 8 * (2 * STAGES + 4) + 16;
 }
-template <int STAGES>
+template <int BN, int STAGES>
 constexpr int gemm_smem_bytes()
 {
-    return STAGES * (4 * UM * BK * 2) + 1024 + 8 * (2 * STAGES + 4) + 16;
+    return STAGES * (2 * UM * BK * 2 + 2 * BN * BK * 2) + 1024 + 8 * (2 * STAGES + 4) + 16;
 }
 
 // ---------------------------------------------------------------- TMA descriptors
@@ -715,9 +707,21 @@ int kmix_create(KMix **out, const FockPlan &p, const int *h_displs, cudaStream_t
     k->rp = pos;
     k->Qp = ((long long) p.nocc * p.naux + BK - 1) / BK * BK;
     k->total_chunks = (int) (k->Qp / BK);
+    // Split count: at least 4 CTAs per SM, at most MAX_SEGS segments per split
+    // (their FP32 register sums are written once, as FP64, at the end), and
+    // the CTA count rounded up to whole waves of 148 when that costs little.
     const int mt = (p.nbf + UM - 1) / UM;
     const int tiles = mt * mt;
-    int ks = (4 * 148 + tiles - 1) / tiles;
+    int ks = std::max((4 * 148 + tiles - 1) / tiles, (k->total_chunks + SEG_CHUNKS * MAX_SEGS - 1) / (SEG_CHUNKS * MAX_SEGS));
+    {
+        int best = ks;
+        for (int c = ks; c <= ks + ks / 4 + 1; c++)
+            if ((tiles * c) % 148 == 0) {
+                best = c;
+                break;
+            }
+        ks = best;
+    }
     ks = std::max(1, std::min(ks, k->total_chunks / 4 > 0 ? k->total_chunks / 4 : 1));
     if (const char *ev = getenv("TINYSCF_KMIX_KSPLIT"))
         if (atoi(ev) > 0) ks = std::min(atoi(ev), k->total_chunks);
@@ -811,17 +815,18 @@ static int launch_half(const KMix *k, HalfArgs ha, cudaStream_t s)
     return OK;
 }
 
-static int launch_gemm(const KMix *k, const GArgs &ga, dim3 grid, cudaStream_t s)
+static int launch_gemm(const KMix *k, const GArgs &ga, cudaStream_t s)
 {
     constexpr int STAGES = 3;
-    constexpr int SMEM = gemm_smem_bytes<STAGES>();
+    constexpr int SMEM = gemm_smem_bytes<128, STAGES>();
     static bool attr_set = false;
     if (!attr_set) {
         if (cudaFuncSetAttribute(k_gemm<STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
             return ERR_CUDA;
         attr_set = true;
     }
-    k_gemm<STAGES><<<grid, THREADS, SMEM, s>>>(k->mdTh, k->mdTl, k->mSh, k->mSl, ga);
+    const int mt = (k->nbf + UM - 1) / UM;
+    k_gemm<STAGES><<<dim3(mt, mt, k->ksplit), THREADS, SMEM, s>>>(k->mdTh, k->mdTl, k->mSh, k->mSl, ga);
     g_launches++;
     return OK;
 }
@@ -870,9 +875,8 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     default: rc = ERR_UNSUPPORTED;
     }
     if (rc) return rc;
-    const int mt = (n + UM - 1) / UM;
     GArgs ga{k->G, n, k->chunks_per_split, k->total_chunks};
-    rc = launch_gemm(k, ga, dim3(mt, mt, k->ksplit), s);
+    rc = launch_gemm(k, ga, s);
     if (rc) return rc;
     const size_t nn = (size_t) n * n;
     k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, k->ksplit, n, k->first ? 1 : 0, K);
