@@ -117,6 +117,15 @@ __global__ void __launch_bounds__(256, 1) kb_half_wide(const MolDev *mols, const
                    (rem % pt) * KH_P);
 }
 
+__global__ void __launch_bounds__(256, 1) kb_half_dmma(const MolDev *mols, const int *active, WorkList wl)
+{
+    BATCH_ITEM(wl)
+    const int st = (m.nocc + KH_S - 1) / KH_S, pt = (m.naux + KH_P - 1) / KH_P;
+    const int i = li / (st * pt), rem = li % (st * pt);
+    half_tile_dmma(m.B, m.Cocc, m.csr_j, m.csr_u, m.displs, m.nocc, m.naux, m.T, i, (rem / pt) * KH_S,
+                   (rem % pt) * KH_P);
+}
+
 __global__ void __launch_bounds__(256, 1) kb_syrk128(const MolDev *mols, const int *active, WorkList wl)
 {
     BATCH_ITEM(wl)
@@ -127,6 +136,18 @@ __global__ void __launch_bounds__(256, 1) kb_syrk128(const MolDev *mols, const i
     const long long q_beg = (long long) split * qchunk, q_end = min(Q, q_beg + qchunk);
     const int2 tl = m.tiles[tile];
     syrk_tile128(m.T, m.nbf, Q, q_beg, q_end, tl.x * KB_T, tl.y * KB_T, m.Kpart + (size_t) split * m.nbf * m.nbf);
+}
+
+__global__ void __launch_bounds__(256, 1) kb_syrk_dmma(const MolDev *mols, const int *active, WorkList wl)
+{
+    BATCH_ITEM(wl)
+    const int tile = li / m.ksplit, split = li % m.ksplit;
+    const long long Q = (long long) m.nocc * m.naux;
+    long long qchunk = (Q + m.ksplit - 1) / m.ksplit;
+    qchunk = (qchunk + KT_K - 1) / KT_K * KT_K;
+    const long long q_beg = (long long) split * qchunk, q_end = min(Q, q_beg + qchunk);
+    const int2 tl = m.tiles[tile];
+    syrk_tile_dmma(m.T, m.nbf, Q, q_beg, q_end, tl.x * KB_T, tl.y * KB_T, m.Kpart + (size_t) split * m.nbf * m.nbf);
 }
 
 __global__ void kb_syrk_reduce(const MolDev *mols, const int *active, WorkList wl)
@@ -277,10 +298,13 @@ void batch_k(const BatchPlan &b, cudaStream_t s)
 {
     if (b.half.total) kb_half<<<b.half.total, 256, 0, s>>>(b.mols, b.active, b.half);
     if (b.half_wide.total) kb_half_wide<<<b.half_wide.total, 256, 0, s>>>(b.mols, b.active, b.half_wide);
+    if (b.half_dmma.total) kb_half_dmma<<<b.half_dmma.total, 256, 0, s>>>(b.mols, b.active, b.half_dmma);
     if (b.syrk.total) kb_syrk<<<b.syrk.total, 256, 0, s>>>(b.mols, b.active, b.syrk);
     if (b.syrk128.total) kb_syrk128<<<b.syrk128.total, 256, 0, s>>>(b.mols, b.active, b.syrk128);
+    if (b.syrk_dmma.total) kb_syrk_dmma<<<b.syrk_dmma.total, 256, 0, s>>>(b.mols, b.active, b.syrk_dmma);
     kb_syrk_reduce<<<b.nn256.total, 256, 0, s>>>(b.mols, b.active, b.nn256);
-    g_launches += 1 + (b.half.total > 0) + (b.half_wide.total > 0) + (b.syrk.total > 0) + (b.syrk128.total > 0);
+    g_launches += 1 + (b.half.total > 0) + (b.half_wide.total > 0) + (b.half_dmma.total > 0) + (b.syrk.total > 0) +
+                  (b.syrk128.total > 0) + (b.syrk_dmma.total > 0);
 }
 
 void batch_fock(const BatchPlan &b, double *d_Eall, cudaStream_t s)

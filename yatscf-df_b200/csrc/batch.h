@@ -6,7 +6,7 @@
 namespace tscf {
 
 struct MolDev {
-    int nbf, naux, nocc, nup, jblk, ksplit, max_diis, ktile;   // ktile: 64 or 128 (exchange rank-k tile)
+    int nbf, naux, nocc, nup, jblk, ksplit, max_diis, ktile;   // ktile: 64, 128 or KSYRK_DMMA
     const int *up_i, *up_j, *up_u, *csr_j, *csr_u, *displs;
     const int2 *tiles;   // upper tile pairs for ktile
     const double *B, *H, *S, *X;
@@ -40,7 +40,7 @@ struct BatchPlan {
     int nmol = 0, naux_max = 0;
     // half / half_wide and syrk / syrk128 hold the items of the molecules that
     // use that tile (the other molecules contribute none)
-    WorkList nup256, jblk, naux256, nup64, half, half_wide, syrk, syrk128, nn256, efb;
+    WorkList nup256, jblk, naux256, nup64, half, half_wide, half_dmma, syrk, syrk128, syrk_dmma, nn256, efb;
     BatchGemm g_xtf, g_tx_fp, g_fd, g_fds, g_xtt, g_t2x, g_tx_t2, g_cocc, g_dens;
 };
 

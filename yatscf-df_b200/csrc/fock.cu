@@ -104,6 +104,15 @@ __global__ void __launch_bounds__(256, 1) k_halftransform_wide(const double *__r
     half_tile_wide(B, C, csr_j, csr_u, displs, nocc, naux, T, blockIdx.z, blockIdx.y * KH_S, blockIdx.x * KH_P);
 }
 
+__global__ void __launch_bounds__(256, 1) k_halftransform_dmma(const double *__restrict__ B, const double *__restrict__ C,
+                                                               const int *__restrict__ csr_j,
+                                                               const int *__restrict__ csr_u,
+                                                               const int *__restrict__ displs, int nocc, int naux,
+                                                               double *__restrict__ T)
+{
+    half_tile_dmma(B, C, csr_j, csr_u, displs, nocc, naux, T, blockIdx.z, blockIdx.y * KH_S, blockIdx.x * KH_P);
+}
+
 // K partial tiles: upper tile pairs (bi <= bj) of 64x64, split over the
 // flattened Q = nocc*naux index. Kpart[split][i][j].
 __global__ void __launch_bounds__(256) k_syrk_part(const double *__restrict__ T, int nbf, long long Q, long long qchunk,
@@ -123,6 +132,16 @@ __global__ void __launch_bounds__(256, 1) k_syrk_part128(const double *__restric
     const int split = blockIdx.y;
     const long long q_beg = (long long) split * qchunk, q_end = min(Q, q_beg + qchunk);
     syrk_tile128(T, nbf, Q, q_beg, q_end, tl.x * KB_T, tl.y * KB_T, Kpart + (size_t) split * nbf * nbf);
+}
+
+__global__ void __launch_bounds__(256, 1) k_syrk_dmma(const double *__restrict__ T, int nbf, long long Q,
+                                                      long long qchunk, const int2 *__restrict__ tiles,
+                                                      double *__restrict__ Kpart)
+{
+    const int2 tl = tiles[blockIdx.x];
+    const int split = blockIdx.y;
+    const long long q_beg = (long long) split * qchunk, q_end = min(Q, q_beg + qchunk);
+    syrk_tile_dmma(T, nbf, Q, q_beg, q_end, tl.x * KB_T, tl.y * KB_T, Kpart + (size_t) split * nbf * nbf);
 }
 
 // K[i][j] = K[j][i] = sum_split Kpart[split][i][j] for i <= j (TinySCF keeps
@@ -146,7 +165,10 @@ void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T,
     g_launches++;
     if (wide) {
         dim3 g1((p.naux + KH_P - 1) / KH_P, (p.nocc + KH_S - 1) / KH_S, p.nbf);
-        k_halftransform_wide<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
+        if (wide == 2)
+            k_halftransform_dmma<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
+        else
+            k_halftransform_wide<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
     } else {
         dim3 g1((p.naux + KT_N - 1) / KT_N, (p.nocc + KT_M - 1) / KT_M, p.nbf);
         k_halftransform<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);
@@ -156,14 +178,16 @@ void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T,
 void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_Kpart, int ksplit, const int2 *d_tiles,
                   cudaStream_t s, int tile)
 {
-    const int nt = (p.nbf + tile - 1) / tile;
+    const int tdim = tile == KSYRK_DMMA ? KB_T : tile;
+    const int nt = (p.nbf + tdim - 1) / tdim;
     const int ntiles = nt * (nt + 1) / 2;
     const long long Q = (long long) p.nocc * p.naux;
     long long qchunk = (Q + ksplit - 1) / ksplit;
     qchunk = (qchunk + KT_K - 1) / KT_K * KT_K;
     dim3 g2(ntiles, ksplit);
     g_launches += 2;
-    if (tile == KB_T) k_syrk_part128<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
+    if (tile == KSYRK_DMMA) k_syrk_dmma<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
+    else if (tile == KB_T) k_syrk_part128<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
     else k_syrk_part<<<g2, 256, 0, s>>>(d_T, p.nbf, Q, qchunk, d_tiles, d_Kpart);
     size_t nn = (size_t) p.nbf * p.nbf;
     k_syrk_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(d_Kpart, ksplit, p.nbf, d_K);

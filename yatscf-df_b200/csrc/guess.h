@@ -58,11 +58,14 @@ void guess_atom_rotation(const std::vector<int> &shell_am, const double *Q, doub
 // Target block in the local frame: D_loc = M_a^T D_ab M_b (D row-major nbf x nbf).
 void guess_local_block(const GuessAtoms &g, const GuessPair &p, const double *D, int nbf, float *out);
 
+struct GuessWork;   // device workspace of guessnet_predict, grown on demand and kept
+
 struct GuessNet {
     int din = G_DIN, hid = G_HID;
     int dout[G_NTYPES];
     float *d_params[G_NTYPES] = {};
     float *d_scale[G_NTYPES] = {}, *d_offset[G_NTYPES] = {};   // y = raw * scale + offset
+    GuessWork *work = nullptr;
 };
 
 int guessnet_load(GuessNet **net, const char *path);
@@ -70,7 +73,7 @@ void guessnet_free(GuessNet *net);
 
 // Predict the blocks of the given pairs and write the (symmetric) density
 // into d_D (zeroed first). Runs on stream s; returns 0 or an error status.
-int guessnet_predict(const GuessNet *net, const std::vector<GuessPair> &pairs, const GuessAtoms &g, double *d_D,
+int guessnet_predict(GuessNet *net, const std::vector<GuessPair> &pairs, const GuessAtoms &g, double *d_D,
                      int nbf, cudaStream_t s);
 
 // Train all five types on host data and write the weights file.

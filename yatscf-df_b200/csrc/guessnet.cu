@@ -367,26 +367,73 @@ int guessnet_load(GuessNet **out, const char *path)
     return OK;
 }
 
-void guessnet_free(GuessNet *net)
+
+struct GuessWork {
+    int cap_pairs = 0, cap_rows = 0;
+    float *dX = nullptr, *dY = nullptr;
+    PairDev *dpd = nullptr;
+    double *dP = nullptr;
+    const float **dptr = nullptr;   // [3][G_NTYPES]: Y, scale, offset of each type
+    MlpWork w{};
+    std::vector<void *> mem;
+};
+
+static void work_release(GuessWork *gw)
 {
-    if (!net) return;
-    for (int t = 0; t < G_NTYPES; t++)
-        if (net->d_params[t]) cudaFree(net->d_params[t]);
-    delete net;
+    if (!gw) return;
+    work_free(gw->w);
+    for (void *p : gw->mem) cudaFree(p);
+    gw->mem.clear();
+    gw->cap_pairs = gw->cap_rows = 0;
 }
 
-int guessnet_predict(const GuessNet *net, const std::vector<GuessPair> &pairs, const GuessAtoms &g, double *d_D,
-                     int nbf, cudaStream_t s)
+// Buffers for np pairs with at most maxrows of one type (the forward pass
+// runs type by type through one MlpWork).
+static int work_reserve(GuessNet *net, int np, int maxrows)
+{
+    if (!net->work) net->work = new GuessWork();
+    GuessWork *gw = net->work;
+    if (np <= gw->cap_pairs && maxrows <= gw->cap_rows) return OK;
+    work_release(gw);
+    np = std::max(np, 1);
+    maxrows = std::max(maxrows, 1);
+    auto dal = [&](void **p, size_t bytes) {
+        if (cudaMalloc(p, bytes ? bytes : 16) != cudaSuccess) return false;
+        gw->mem.push_back(*p);
+        return true;
+    };
+    if (!dal((void **) &gw->dX, sizeof(float) * (size_t) np * G_DIN) ||
+        !dal((void **) &gw->dY, sizeof(float) * (size_t) np * G_MAXF * G_MAXF) ||
+        !dal((void **) &gw->dpd, sizeof(PairDev) * np) ||
+        !dal((void **) &gw->dP, sizeof(double) * (size_t) np * 2 * G_MAXF * G_MAXF) ||
+        !dal((void **) &gw->dptr, sizeof(float *) * 3 * G_NTYPES))
+        return ERR_ALLOC;
+    int rc = work_alloc(gw->w, net->din, net->hid, G_MAXF * G_MAXF, maxrows);
+    if (rc) return rc;
+    gw->cap_pairs = np;
+    gw->cap_rows = maxrows;
+    return OK;
+}
+
+int guessnet_predict(GuessNet *net, const std::vector<GuessPair> &pairs, const GuessAtoms &g, double *d_D, int nbf,
+                     cudaStream_t s)
 {
     const int np = (int) pairs.size();
-    std::vector<std::vector<float>> X(G_NTYPES);
+    // rows of each type contiguous: type t starts at row off[t]
+    int cnt[G_NTYPES] = {}, off[G_NTYPES + 1] = {};
+    for (const GuessPair &p : pairs) cnt[p.type]++;
+    for (int t = 0; t < G_NTYPES; t++) off[t + 1] = off[t] + cnt[t];
+    size_t yoff[G_NTYPES + 1] = {};
+    for (int t = 0; t < G_NTYPES; t++) yoff[t + 1] = yoff[t] + (size_t) cnt[t] * net->dout[t];
+    std::vector<float> X((size_t) np * G_DIN);
     std::vector<PairDev> pd(np);
     std::vector<double> P((size_t) np * 2 * G_MAXF * G_MAXF, 0.0);
-    int cnt[G_NTYPES] = {};
+    int fill[G_NTYPES] = {};
     for (int k = 0; k < np; k++) {
         const GuessPair &p = pairs[k];
-        pd[k] = PairDev{p.type, cnt[p.type]++, p.off_a, p.off_b, p.nf_a, p.nf_b};
-        X[p.type].insert(X[p.type].end(), p.feat, p.feat + G_DIN);
+        const int row = fill[p.type]++;
+        pd[k] = PairDev{p.type, row, p.off_a, p.off_b, p.nf_a, p.nf_b};
+        std::memcpy(&X[(size_t) (off[p.type] + row) * G_DIN], p.feat, sizeof(float) * G_DIN);
         double Qt[9];
         for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++) Qt[i * 3 + j] = p.Qf[j * 3 + i];
@@ -395,56 +442,46 @@ int guessnet_predict(const GuessNet *net, const std::vector<GuessPair> &pairs, c
     }
     int maxrows = 1;
     for (int t = 0; t < G_NTYPES; t++) maxrows = std::max(maxrows, cnt[t]);
-    std::vector<void *> mem;
-    auto dal = [&](void **p, size_t bytes) {
-        if (cudaMalloc(p, bytes ? bytes : 16) != cudaSuccess) return false;
-        mem.push_back(*p);
-        return true;
-    };
-    int rc = OK;
-    float *dX = nullptr;
-    float *dY[G_NTYPES] = {};
-    PairDev *dpd = nullptr;
-    double *dP = nullptr;
-    const float **dYp = nullptr, **dSc = nullptr, **dOf = nullptr;
-    MlpWork w{};
-    if (!dal((void **) &dX, sizeof(float) * (size_t) maxrows * G_DIN) ||
-        !dal((void **) &dpd, sizeof(PairDev) * np) || !dal((void **) &dP, sizeof(double) * P.size()) ||
-        !dal((void **) &dYp, sizeof(float *) * G_NTYPES) || !dal((void **) &dSc, sizeof(float *) * G_NTYPES) ||
-        !dal((void **) &dOf, sizeof(float *) * G_NTYPES))
-        rc = ERR_ALLOC;
-    for (int t = 0; rc == OK && t < G_NTYPES; t++)
-        if (!dal((void **) &dY[t], sizeof(float) * (size_t) std::max(cnt[t], 1) * net->dout[t])) rc = ERR_ALLOC;
-    if (rc == OK) rc = work_alloc(w, net->din, net->hid, 225, maxrows);
-    if (rc == OK) {
-        cudaMemsetAsync(d_D, 0, sizeof(double) * (size_t) nbf * nbf, s);
-        for (int t = 0; t < G_NTYPES; t++) {
-            if (!cnt[t]) continue;
-            cudaMemcpyAsync(dX, X[t].data(), sizeof(float) * X[t].size(), cudaMemcpyHostToDevice, s);
-            w.dout = net->dout[t];
-            MlpParams prm = split_params(net->d_params[t], net->din, net->hid, net->dout[t]);
-            mlp_forward(prm, dX, cnt[t], w, s);
-            cudaMemcpyAsync(dY[t], w.Y, sizeof(float) * (size_t) cnt[t] * net->dout[t], cudaMemcpyDeviceToDevice, s);
-            cudaStreamSynchronize(s);   // dX is reused by the next type
-        }
-        const float *hy[G_NTYPES], *hs[G_NTYPES], *ho[G_NTYPES];
-        for (int t = 0; t < G_NTYPES; t++) {
-            hy[t] = dY[t];
-            hs[t] = net->d_scale[t];
-            ho[t] = net->d_offset[t];
-        }
-        cudaMemcpyAsync(dYp, hy, sizeof(hy), cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(dSc, hs, sizeof(hs), cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(dOf, ho, sizeof(ho), cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(dpd, pd.data(), sizeof(PairDev) * np, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice, s);
-        if (np > 0) k_assemble<<<np, 128, 0, s>>>(dpd, dYp, dSc, dOf, dP, d_D, nbf);
-        g_launches++;
-        if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = ERR_CUDA;
+    int rc = work_reserve(net, np, maxrows);
+    if (rc) return rc;
+    GuessWork *gw = net->work;
+    cudaMemsetAsync(d_D, 0, sizeof(double) * (size_t) nbf * nbf, s);
+    cudaMemcpyAsync(gw->dX, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gw->dpd, pd.data(), sizeof(PairDev) * np, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(gw->dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice, s);
+    const float *hp[3 * G_NTYPES];
+    for (int t = 0; t < G_NTYPES; t++) {
+        hp[t] = gw->dY + yoff[t];
+        hp[G_NTYPES + t] = net->d_scale[t];
+        hp[2 * G_NTYPES + t] = net->d_offset[t];
     }
-    work_free(w);
-    for (void *p : mem) cudaFree(p);
-    return rc;
+    cudaMemcpyAsync(gw->dptr, hp, sizeof(hp), cudaMemcpyHostToDevice, s);
+    for (int t = 0; t < G_NTYPES; t++) {
+        if (!cnt[t]) continue;
+        gw->w.dout = net->dout[t];
+        MlpParams prm = split_params(net->d_params[t], net->din, net->hid, net->dout[t]);
+        mlp_forward(prm, gw->dX + (size_t) off[t] * G_DIN, cnt[t], gw->w, s);
+        cudaMemcpyAsync(gw->dY + yoff[t], gw->w.Y, sizeof(float) * (size_t) cnt[t] * net->dout[t],
+                        cudaMemcpyDeviceToDevice, s);
+    }
+    if (np > 0) k_assemble<<<np, 128, 0, s>>>(gw->dpd, gw->dptr, gw->dptr + G_NTYPES, gw->dptr + 2 * G_NTYPES, gw->dP,
+                                               d_D, nbf);
+    g_launches++;
+    // the host arrays above are staged by the copies: wait before they go out of scope
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ERR_CUDA;
+    return OK;
+}
+
+void guessnet_free(GuessNet *net)
+{
+    if (!net) return;
+    if (net->work) {
+        work_release(net->work);
+        delete net->work;
+    }
+    for (int t = 0; t < G_NTYPES; t++)
+        if (net->d_params[t]) cudaFree(net->d_params[t]);
+    delete net;
 }
 
 // ------------------------------------------------------------------ training

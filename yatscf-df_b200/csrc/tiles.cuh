@@ -311,6 +311,155 @@ __device__ __forceinline__ void syrk_tile128(const double *__restrict__ T, int n
     }
 }
 
+// ---- K = T T^T partial tile on the FP64 tensor cores (DMMA, mma.sync
+// m8n8k4): 128 x 128 outputs per 256 threads, 8 warps of 64 x 32 (8 x 4 DMMA
+// tiles each). Per 4-wide K step a thread reads 12 doubles from shared memory
+// for 32 DMMAs (8192 FMAs per warp), so the FP64 pipe, not shared memory, sets
+// the pace. Operands staged as in syrk_tile128 (register prefetch of the next
+// 16-wide K step).
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void syrk_tile_dmma(const double *__restrict__ T, int nbf, long long Q, long long q_beg,
+                                               long long q_end, int i0, int j0, double *__restrict__ out)
+{
+    __shared__ double As[KT_K][KB_T + 2];
+    __shared__ double Bs[KT_K][KB_T + 2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;   // warp tile origin inside the CTA tile
+    const int fr = lane >> 2, fc = lane & 3;                 // fragment row / column of this lane
+    double acc[8][4][2];
+#pragma unroll
+    for (int x = 0; x < 8; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    double pa[8], pb[8];
+    auto fetch = [&](long long q0) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = tid + 256 * r;
+            const int row = l / KT_K, kk = l % KT_K;
+            const long long q = q0 + kk;
+            const int gi = i0 + row, gj = j0 + row;
+            pa[r] = (gi < nbf && q < q_end) ? T[(size_t) gi * Q + q] : 0.0;
+            pb[r] = (gj < nbf && q < q_end) ? T[(size_t) gj * Q + q] : 0.0;
+        }
+    };
+    if (q_beg < q_end) fetch(q_beg);
+    for (long long q0 = q_beg; q0 < q_end; q0 += KT_K) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = tid + 256 * r;
+            As[l % KT_K][l / KT_K] = pa[r];
+            Bs[l % KT_K][l / KT_K] = pb[r];
+        }
+        __syncthreads();
+        if (q0 + KT_K < q_end) fetch(q0 + KT_K);
+#pragma unroll
+        for (int k4 = 0; k4 < KT_K; k4 += 4) {
+            double a[8], b[4];
+#pragma unroll
+            for (int x = 0; x < 8; x++) a[x] = As[k4 + fc][wm + 8 * x + fr];   // A(row fr, k fc)
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[k4 + fc][wn + 8 * y + fr];   // B(k fc, col fr)
+#pragma unroll
+            for (int x = 0; x < 8; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 8; x++) {
+        const int gi = i0 + wm + 8 * x + fr;
+        if (gi >= nbf) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const int gj = j0 + wn + 8 * y + 2 * fc;   // C(row fr, cols 2 fc, 2 fc + 1)
+            if (gj < nbf) out[(size_t) gi * nbf + gj] = acc[x][y][0];
+            if (gj + 1 < nbf) out[(size_t) gi * nbf + gj + 1] = acc[x][y][1];
+        }
+    }
+}
+
+// ---- K half-transform tile on the FP64 tensor cores: 64 (s) x 256 (P)
+// outputs per 256 threads, 8 warps of 32 x 64 (4 x 8 DMMA tiles each), CSR
+// chunks of 16 prefetched into registers as in half_tile_wide.
+__device__ __forceinline__ void half_tile_dmma(const double *__restrict__ B, const double *__restrict__ C,
+                                               const int *__restrict__ csr_j, const int *__restrict__ csr_u,
+                                               const int *__restrict__ displs, int nocc, int naux,
+                                               double *__restrict__ T, int i, int s0, int p0)
+{
+    __shared__ double As[KT_K][KH_S + 2];
+    __shared__ double Bs[KT_K][KH_P + 2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ws = (warp >> 2) * 32, wp = (warp & 3) * 64;
+    const int fr = lane >> 2, fc = lane & 3;
+    const int r_beg = displs[i], r_end = displs[i + 1];
+    double acc[4][8][2];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 8; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    double pa[4], pb[16];
+    auto fetch = [&](int r0) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int l = tid + 256 * q, kk = l / KH_S, c = l % KH_S, r = r0 + kk, sg = s0 + c;
+            pa[q] = (r < r_end && sg < nocc) ? C[(size_t) csr_j[r] * nocc + sg] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int l = tid + 256 * q, kk = l / KH_P, c = l % KH_P, r = r0 + kk, pg = p0 + c;
+            pb[q] = (r < r_end && pg < naux) ? B[(size_t) csr_u[r] * naux + pg] : 0.0;
+        }
+    };
+    if (r_beg < r_end) fetch(r_beg);
+    for (int r0 = r_beg; r0 < r_end; r0 += KT_K) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int l = tid + 256 * q;
+            As[l / KH_S][l % KH_S] = pa[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int l = tid + 256 * q;
+            Bs[l / KH_P][l % KH_P] = pb[q];
+        }
+        __syncthreads();
+        if (r0 + KT_K < r_end) fetch(r0 + KT_K);
+#pragma unroll
+        for (int k4 = 0; k4 < KT_K; k4 += 4) {
+            double a[4], b[8];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[k4 + fc][ws + 8 * x + fr];
+#pragma unroll
+            for (int y = 0; y < 8; y++) b[y] = Bs[k4 + fc][wp + 8 * y + fr];
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 8; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        const int sg = s0 + ws + 8 * x + fr;
+        if (sg >= nocc) continue;
+        double *row = T + ((size_t) i * nocc + sg) * naux;
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+            const int pg = p0 + wp + 8 * y + 2 * fc;
+            if (pg < naux) row[pg] = acc[x][y][0];
+            if (pg + 1 < naux) row[pg + 1] = acc[x][y][1];
+        }
+    }
+}
+
 // ---- J first pass: partial t(P) of upper rows [r0, r1), weights (2 - d_ij) D_ij.
 // Thread x owns columns x, x + 512, ... (naux <= 8192).
 constexpr int JT_THREADS = 512, JT_COLS = 16;

@@ -773,10 +773,10 @@ int sparsity_impl(TinySCF_t t)
     e->ksplit_max = std::min(64, 2 * std::max(e->ksplit, h128));   // room for the autotuner's candidates
     // untuned defaults by size: the larger register tiles pay off once there are enough of them
     if (nbf >= 384) {
-        e->ktile = 128;
+        e->ktile = KSYRK_DMMA;
         e->ksplit = h128;
     }
-    e->khwide = naux >= 1024 ? 1 : 0;
+    e->khwide = 0;
     RC(dalloc(e, &e->Kpart, (size_t) e->ksplit_max * nbf * nbf));
     {
         std::vector<int2> tl, tl2;
@@ -936,22 +936,25 @@ int autotune_fock(TinySCF_t t)
         std::vector<int> cand;
         for (int v : {std::max(1, e->ksplit64 / 2), e->ksplit64, std::min(e->ksplit_max, 2 * e->ksplit64)})
             if (std::find(cand.begin(), cand.end(), 64000 + v) == cand.end()) cand.push_back(64000 + v);
-        for (int v : {std::max(1, h128 / 2), h128, std::min(e->ksplit_max, 2 * h128)})
+        for (int v : {std::max(1, h128 / 2), h128, std::min(e->ksplit_max, 2 * h128)}) {
             if (std::find(cand.begin(), cand.end(), 128000 + v) == cand.end()) cand.push_back(128000 + v);
+            if (std::find(cand.begin(), cand.end(), KSYRK_DMMA * 1000 + v) == cand.end())
+                cand.push_back(KSYRK_DMMA * 1000 + v);
+        }
         c = tune_run(key, cand, [&](int k) {
             const int tile = k / 1000;
-            build_K_syrk(p, e->T, e->K, e->Kpart, k % 1000, tile == 128 ? e->tiles128 : e->tiles, e->s, tile);
+            build_K_syrk(p, e->T, e->K, e->Kpart, k % 1000, tile == 64 ? e->tiles : e->tiles128, e->s, tile);
         }, e->s);
     }
-    if ((c / 1000 == 64 || c / 1000 == 128) && c % 1000 >= 1 && c % 1000 <= e->ksplit_max) {
+    if ((c / 1000 == 64 || c / 1000 == 128 || c / 1000 == KSYRK_DMMA) && c % 1000 >= 1 && c % 1000 <= e->ksplit_max) {
         e->ktile = c / 1000;
         e->ksplit = c % 1000;
         if (e->ktile == 64) e->ksplit64 = e->ksplit;
     }
     snprintf(key, sizeof(key), "khalf:%d:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf, e->nnz);
     c = tune_lookup(key);
-    if (c < 0) c = tune_run(key, {0, 1}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
-    if (c == 0 || c == 1) e->khwide = c;
+    if (c < 0) c = tune_run(key, {0, 1, 2}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
+    if (c >= 0 && c <= 2) e->khwide = c;
     snprintf(key, sizeof(key), "jrows:%d:%d", e->nup, t->df_nbf);
     c = tune_lookup(key);
     if (c < 0) {
@@ -1055,7 +1058,7 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
         build_K_halftransform(p, e->Cocc, e->T, e->s, e->khwide);
         tstop(e, TINYSCF_T_K_HT);
         tstart(e, TINYSCF_T_K_SYRK);
-        build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 128 ? e->tiles128 : e->tiles, e->s, e->ktile);
+        build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 64 ? e->tiles : e->tiles128, e->s, e->ktile);
         tstop(e, TINYSCF_T_K_SYRK);
     }
     if (Kuse != e->K)
@@ -1837,7 +1840,8 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     }
     // per-molecule descriptors and work lists
     std::vector<MolDev> md(nmol);
-    std::vector<int> c_nup256, c_jblk, c_naux256, c_nup64, c_half, c_halfw, c_syrk, c_syrk128, c_nn256, c_efb;
+    std::vector<int> c_nup256, c_jblk, c_naux256, c_nup64, c_half, c_halfw, c_halfd, c_syrk, c_syrk128, c_syrkd, c_nn256,
+        c_efb;
     std::vector<GemmDesc> xtf, txfp, fd, fds, xtt, t2x, txt2, cocc, dens;
     int naux_max = 1;
     for (int k = 0; k < nmol; k++) {
@@ -1861,7 +1865,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         m.csr_j = e->csr_j;
         m.csr_u = e->csr_u;
         m.displs = e->csr_displs;
-        m.tiles = e->ktile == 128 ? e->tiles128 : e->tiles;
+        m.tiles = e->ktile == 64 ? e->tiles : e->tiles128;
         m.B = e->B;
         m.H = e->H;
         m.S = e->S;
@@ -1893,10 +1897,12 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         c_naux256.push_back((na + 255) / 256);
         c_nup64.push_back((e->nup + 63) / 64);
         c_half.push_back(e->khwide ? 0 : n * ((o + 63) / 64) * ((na + 63) / 64));
-        c_halfw.push_back(e->khwide ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);
+        c_halfw.push_back(e->khwide == 1 ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);
+        c_halfd.push_back(e->khwide == 2 ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);
         const int nt2 = (n + 127) / 128;
         c_syrk.push_back(e->ktile == 64 ? nt * (nt + 1) / 2 * e->ksplit : 0);
         c_syrk128.push_back(e->ktile == 128 ? nt2 * (nt2 + 1) / 2 * e->ksplit : 0);
+        c_syrkd.push_back(e->ktile == KSYRK_DMMA ? nt2 * (nt2 + 1) / 2 * e->ksplit : 0);
         c_nn256.push_back((int) ((nn + 255) / 256));
         c_efb.push_back(ENERGY_BLOCKS);
         xtf.push_back({n, n, n, n, n, n, e->X, e->F, e->tmp, 1.0, 0.0});
@@ -1927,8 +1933,10 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     RC(make_list(b, c_nup64, p.nup64));
     RC(make_list(b, c_half, p.half));
     RC(make_list(b, c_halfw, p.half_wide));
+    RC(make_list(b, c_halfd, p.half_dmma));
     RC(make_list(b, c_syrk, p.syrk));
     RC(make_list(b, c_syrk128, p.syrk128));
+    RC(make_list(b, c_syrkd, p.syrk_dmma));
     RC(make_list(b, c_nn256, p.nn256));
     RC(make_list(b, c_efb, p.efb));
     RC(make_gemm(b, xtf, true, false, p.g_xtf));

@@ -136,11 +136,14 @@ void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, dou
              double *d_w, cudaStream_t s);
 int  build_J_part_blocks(const FockPlan &p);
 // K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
-// wide = 1: 64 x 256 tiles (k_halftransform_wide), else 64 x 64
+// wide = 1: 64 x 256 FFMA tiles (k_halftransform_wide), 2: 64 x 256 DMMA tiles
+// (k_halftransform_dmma), 0: 64 x 64 FFMA tiles
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide = 0);
 // ... then K = T T^T over upper 64x64 tiles (d_tiles: (bi,bj), bi <= bj), split-K, mirrored.
-// tile = 64 (k_syrk_part) or 128 (k_syrk_part128); d_tiles lists the upper
-// tile pairs for that tile size
+// tile = 64 (k_syrk_part, FFMA), 128 (k_syrk_part128, FFMA) or KSYRK_DMMA
+// (k_syrk_dmma: 128 x 128 tiles on the FP64 tensor cores); d_tiles lists the
+// upper tile pairs for that tile size (128 for KSYRK_DMMA)
+constexpr int KSYRK_DMMA = 129;
 void build_K_syrk(const FockPlan &p, const double *d_T, double *d_K, double *d_Kpart, int ksplit,
                   const int2 *d_tiles, cudaStream_t s, int tile = 64);
 size_t build_K_part_elems(const FockPlan &p, int ksplit);
