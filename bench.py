@@ -243,7 +243,7 @@ def run_ours(args, rank, world, local_rank):
         fast_form = mode == tinyscf.K_MIXED
         e.set_k_precision(mode)
         e.set_density_solver(tinyscf.DENSITY_REFINE if fast_form else tinyscf.DENSITY_EIG)
-        e.set_graph(fast_form)
+        e.set_graph(fast_form and not args.no_graph)
         e.set_guess(tinyscf.GUESS_LEARNED if fast_form else tinyscf.GUESS_SAD)
         for _ in range(warmup):
             e.reset_scf()
@@ -292,7 +292,7 @@ def run_ours(args, rank, world, local_rank):
         if args.precision == "mixed":
             e2.set_k_precision(tinyscf.K_MIXED)
             e2.set_density_solver(tinyscf.DENSITY_REFINE)
-            e2.set_graph(True)
+            e2.set_graph(not args.no_graph)
         e2.do_SCF()
         _ = e2.energy
         c = e2.counters()
@@ -509,6 +509,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="run the mixed form's iterations as individual launches (a profiler then sees every kernel)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

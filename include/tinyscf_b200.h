@@ -127,7 +127,8 @@ TINYSCF_API int TinySCF_set_k_precision(TinySCF_t t, int mode);
 #define TINYSCF_DENSITY_REFINE 1
 TINYSCF_API int TinySCF_set_density_solver(TinySCF_t t, int mode);
 /* CUDA-graph SCF iterations. With on = 1, TinySCF_do_SCF captures one
- * iteration once DIIS is active (iteration 2 on) into a CUDA graph: J, K,
+ * iteration from iteration 3 on (DIIS active and run once eagerly, so the
+ * autotuner has seen every shape) into a CUDA graph: J, K,
  * Fock and energy, DIIS and, with TINYSCF_DENSITY_REFINE, the density with its
  * refinement loop as a device-controlled conditional (WHILE) node; each later
  * iteration is one graph launch. The full eigensolve of TINYSCF_DENSITY_EIG
@@ -173,8 +174,10 @@ TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *
  * device and the fastest kept for the process (and saved to / loaded from the
  * file named by TINYSCF_TUNE_FILE): the block size and thread order of each
  * 3-centre integral AM class, the tile shape of each FP64 GEMM shape
- * (64x64, 32x32, 128x64), the split count of the FP64 exchange and the row
- * blocks of the J first pass. All candidates compute the same values. */
+ * (FFMA 64x64, 32x32, 128x64, or 128x128 on the FP64 tensor cores), the tile
+ * and split count of the FP64 exchange and the row blocks of the J first pass.
+ * All candidates compute the same values (the FP64 tensor-core tiles up to
+ * rounding in the last bits). */
 TINYSCF_API int TinySCF_set_autotune(int on);
 /* Free and total device memory in bytes (cudaMemGetInfo) of a CUDA device,
  * for callers that size batches of molecules to what fits. */

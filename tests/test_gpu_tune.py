@@ -1,4 +1,5 @@
-"""Autotuner: every candidate computes the same values, so a tuned engine
+"""Autotuner: every candidate computes the same values (the FFMA tile shapes
+bit for bit, the FP64 tensor-core tiles to rounding), so a tuned engine
 reproduces an untuned one; the tuned knobs show up in the tuner's table."""
 import numpy as np
 import pytest
@@ -29,7 +30,7 @@ def test_tuned_engine_matches_untuned():
     assert it0 == it1
     assert abs(E0 - E1) < 1e-10
     assert np.abs(K0 - K1).max() < 1e-11
-    assert np.abs(B0 - B1).max() == 0.0          # integral launch shapes do not change a single value
+    assert np.abs(B0 - B1).max() < 1e-13 * max(1.0, np.abs(B0).max())
     rep = tinyscf.autotune_report()
     for key in ("3c:", "dgemm:", "ksyrk:", "khalf:", "jrows:"):
         assert key in rep, rep

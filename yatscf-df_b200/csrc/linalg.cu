@@ -16,9 +16,10 @@ namespace tscf {
 long long g_launches = 0;
 
 // ------------------------------------------------------------------ DGEMM
-// Three tile shapes (dgemm_tile): 64x64 (default), 32x32 (more blocks for
-// small matrices) and 128x64 (more reuse for large ones). The autotuner picks
-// one per call shape the first time the shape is met outside a stream capture.
+// Four tile shapes: FFMA 64x64 (default), 32x32 (more blocks for small
+// matrices) and 128x64 (more reuse for large ones) (dgemm_tile), and 128x128
+// on the FP64 tensor cores (dgemm_tile_dmma). The autotuner picks one per call
+// shape the first time the shape is met outside a stream capture.
 template <bool TA, bool TB, int BM, int BN>
 __global__ void __launch_bounds__(256) k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
                                                const double *__restrict__ B, int ldb, double beta, double *C, int ldc)
@@ -38,10 +39,30 @@ static void dgemm_shape(bool ta, bool tb, int m, int n, int k, double alpha, con
     else k_dgemm<true, true, BM, BN><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256, 1) k_dgemm_dmma(int m, int n, int k, double alpha, const double *__restrict__ A,
+                                                       int lda, const double *__restrict__ B, int ldb, double beta,
+                                                       double *C, int ldc)
+{
+    dgemm_tile_dmma<TA, TB>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, blockIdx.y * 128, blockIdx.x * 128);
+}
+
+static void dgemm_dmma(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda, const double *B,
+                       int ldb, double beta, double *C, int ldc, cudaStream_t s)
+{
+    dim3 grid((n + 127) / 128, (m + 127) / 128);
+    g_launches++;
+    if (!ta && !tb) k_dgemm_dmma<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (!ta && tb) k_dgemm_dmma<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (ta && !tb) k_dgemm_dmma<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else k_dgemm_dmma<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
 static void dgemm_variant(int v, bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
                           const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
 {
-    if (v == 1) dgemm_shape<32, 32>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    if (v == 3) dgemm_dmma(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    else if (v == 1) dgemm_shape<32, 32>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else if (v == 2) dgemm_shape<128, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else dgemm_shape<64, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
@@ -67,7 +88,7 @@ void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
         const size_t ea = ta ? (size_t) k * lda : (size_t) m * lda, eb = tb ? (size_t) n * ldb : (size_t) k * ldb;
         if (tune_enabled() && cs == cudaStreamCaptureStatusNone && beta == 0.0 && disjoint(A, ea) && disjoint(B, eb) &&
             (double) m * n * k >= 2e6) {
-            v = tune_run(key, {0, 1, 2}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
+            v = tune_run(key, {0, 1, 2, 3}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
             return;
         }
     }

@@ -72,6 +72,79 @@ __device__ __forceinline__ void dgemm_tile(int m, int n, int k, double alpha, co
     }
 }
 
+// FP64 tensor-core MMA: D(8x8) += A(8x4, row-major) B(4x8, column-major); lane
+// l holds A(l/4, l%4), B(l%4, l/4) and D(l/4, 2(l%4)..2(l%4)+1).
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// ---- FP64 GEMM tile on the FP64 tensor cores: 128 x 128 outputs per 256
+// threads, 8 warps of 64 x 32 (8 x 4 DMMA tiles). Same operand conventions as
+// dgemm_tile.
+template <bool TA, bool TB>
+__device__ __forceinline__ void dgemm_tile_dmma(int m, int n, int k, double alpha, const double *__restrict__ A,
+                                                int lda, const double *__restrict__ B, int ldb, double beta, double *C,
+                                                int ldc, int m0, int n0)
+{
+    constexpr int BT = 128;
+    __shared__ double As[GB_K][BT + 2];
+    __shared__ double Bs[GB_K][BT + 2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
+    const int fr = lane >> 2, fc = lane & 3;
+    double acc[8][4][2];
+#pragma unroll
+    for (int x = 0; x < 8; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    for (int k0 = 0; k0 < k; k0 += GB_K) {
+#pragma unroll
+        for (int r = 0; r < BT / 16; r++) {
+            const int l = tid + 256 * r;
+            int row, kk;
+            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / BT; row = l % BT; }
+            const int gi = m0 + row, gk = k0 + kk;
+            As[kk][row] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
+            int col;
+            if (!TB) { kk = l / BT; col = l % BT; } else { col = l / GB_K; kk = l % GB_K; }
+            const int gj = n0 + col, gk2 = k0 + kk;
+            Bs[kk][col] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < GB_K; k4 += 4) {
+            double a[8], b[4];
+#pragma unroll
+            for (int x = 0; x < 8; x++) a[x] = As[k4 + fc][wm + 8 * x + fr];
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[k4 + fc][wn + 8 * y + fr];
+#pragma unroll
+            for (int x = 0; x < 8; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 8; x++) {
+        const int gi = m0 + wm + 8 * x + fr;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int gj = n0 + wn + 8 * y + 2 * fc + h;
+                if (gj >= n) continue;
+                double *c = C + (size_t) gi * ldc + gj;
+                *c = (beta == 0.0) ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * *c;
+            }
+        }
+    }
+}
+
 // ---- K half-transform tile: T[i][s0:s0+64][p0:p0+64] = sum_{r in CSR row i} C[j_r][s] B[u_r][p]
 constexpr int KT_M = 64, KT_N = 64, KT_K = 16;
 
@@ -317,13 +390,6 @@ __device__ __forceinline__ void syrk_tile128(const double *__restrict__ T, int n
 // for 32 DMMAs (8192 FMAs per warp), so the FP64 pipe, not shared memory, sets
 // the pace. Operands staged as in syrk_tile128 (register prefetch of the next
 // 16-wide K step).
-__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
-
 __device__ __forceinline__ void syrk_tile_dmma(const double *__restrict__ T, int nbf, long long Q, long long q_beg,
                                                long long q_end, int i0, int j0, double *__restrict__ out)
 {

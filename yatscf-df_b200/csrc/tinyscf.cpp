@@ -1193,7 +1193,7 @@ void graph_release(Engine *e)
     e->graph_key = -1;
 }
 
-// Capture one SCF iteration past the DIIS start (t->iter >= 2): J, K (FP64 or
+// Capture one SCF iteration once DIIS has run eagerly once (t->iter >= 3): J, K (FP64 or
 // mixed), Fock + energy, DIIS, and with the refinement solver the density with
 // its step loop as a device-controlled WHILE node. The full-eigensolve density
 // stays outside the graph (the eigensolver library is not captured).
@@ -1250,7 +1250,7 @@ int graph_capture(TinySCF_t t)
     return OK;
 }
 
-// One SCF iteration (t->iter >= 2) through the captured graph; E receives the
+// One SCF iteration (t->iter >= 3) through the captured graph; E receives the
 // energy. Falls back to a full eigensolve when the refinement loop stopped
 // without converging.
 int graph_iteration(TinySCF_t t, double *E)
@@ -1308,7 +1308,7 @@ int scf_impl(TinySCF_t t)
     while ((t->iter < t->niters) && (energy_delta >= t->ene_tol)) {
         if (t->verbose) printf("--------------- Iteration %d ---------------\n", t->iter);
         double E = 0.0;
-        if (e->use_graph && t->iter >= 2) {
+        if (e->use_graph && t->iter >= 3) {   // iteration 2 runs eagerly: its shapes get tuned before the capture
             RC(graph_iteration(t, &E));
         } else {
             tstart(e, TINYSCF_T_ITER);
