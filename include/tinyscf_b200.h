@@ -42,6 +42,8 @@ enum {
     TINYSCF_T_SCF,           /* the whole TinySCF_do_SCF             */
     TINYSCF_T_K_MIXED,       /* mixed-precision incremental K        */
     TINYSCF_T_FINAL,         /* final FP64 Fock build (mixed mode)   */
+    TINYSCF_T_K_HALF,        /* mixed K: tensor-core half-transform  */
+    TINYSCF_T_K_GEMM,        /* mixed K: tensor-core G = dT S^T      */
     TINYSCF_T_COUNT
 };
 

@@ -832,7 +832,8 @@ static int launch_gemm(const KMix *k, const GArgs &ga, cudaStream_t s)
 }
 
 // One incremental K build from the new occupied factor Cocc (nbf x nocc).
-int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s)
+int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s,
+               const std::function<void(int)> &mark)
 {
     const int n = k->nbf, o = k->nocc;
     // align C_n to C_{n-1}: R = polar(C_n^T S C_{n-1}) by Newton-Schulz; R = I if it does not converge
@@ -855,6 +856,7 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     g_launches += 3;
     HalfArgs ha{k->row_chunk0, k->Tm, k->dTh, k->dTl, k->Sh, k->Sl, o, k->naux, k->Qp, 0, 0};
     int rc;
+    if (mark) mark(0);
     switch (k->bn_half) {
     case 16: rc = launch_half<16>(k, ha, s); break;
     case 32: rc = launch_half<32>(k, ha, s); break;
@@ -875,9 +877,11 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     default: rc = ERR_UNSUPPORTED;
     }
     if (rc) return rc;
+    if (mark) mark(1);
     GArgs ga{k->G, n, k->chunks_per_split, k->total_chunks};
     rc = launch_gemm(k, ga, s);
     if (rc) return rc;
+    if (mark) mark(2);
     const size_t nn = (size_t) n * n;
     k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, k->ksplit, n, k->first ? 1 : 0, K);
     g_launches++;

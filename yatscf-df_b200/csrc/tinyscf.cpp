@@ -1050,7 +1050,15 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
     const double *Kuse = e->K;
     if (e->kprec == TINYSCF_K_MIXED && !force_fp64) {
         tstart(e, TINYSCF_T_K_MIXED);
-        RC(kmix_build(e->kmix, e->Cocc, e->S, e->Kmix, e->s));
+        RC(kmix_build(e->kmix, e->Cocc, e->S, e->Kmix, e->s, [&](int w) {
+            if (w == 0) tstart(e, TINYSCF_T_K_HALF);
+            else if (w == 1) {
+                tstop(e, TINYSCF_T_K_HALF);
+                tstart(e, TINYSCF_T_K_GEMM);
+            } else {
+                tstop(e, TINYSCF_T_K_GEMM);
+            }
+        }));
         tstop(e, TINYSCF_T_K_MIXED);
         Kuse = e->Kmix;
     } else {

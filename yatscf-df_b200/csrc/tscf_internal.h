@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <functional>
+
 namespace tscf {
 
 // Number of engine kernels launched by this process (host-side count, read by
@@ -158,7 +160,10 @@ int  kmix_create(KMix **out, const FockPlan &p, const int *h_displs, cudaStream_
 void kmix_destroy(KMix *k);
 void kmix_reset(KMix *k, cudaStream_t s);
 // K (FP64, accumulated across calls) from the occupied factor Cocc; S is the overlap.
-int  kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s);
+// mark (optional) is called with 0 before the half-transform kernel, 1 between
+// it and the G GEMM, 2 after the G GEMM (device timers around the two).
+int  kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s,
+                const std::function<void(int)> &mark = nullptr);
 int  kmix_error_flag();
 
 // ---------------------------------------------------------------- DIIS / density (scf.cu)

@@ -17,7 +17,7 @@ LIBPATH = os.path.join(HERE, "libtinyscf_b200.so")
 
 MAX_DIIS = 10
 TIMERS = ["HCORE", "SCHWARZ", "GUESS", "3C", "2C", "INVSQRT", "DFGEMM", "J", "K_HT", "K_SYRK",
-          "FOCK", "DIIS", "DENSITY", "ITER", "SCF", "K_MIXED", "FINAL"]
+          "FOCK", "DIIS", "DENSITY", "ITER", "SCF", "K_MIXED", "FINAL", "K_HALF", "K_GEMM"]
 K_FP64, K_MIXED = 0, 1
 DENSITY_EIG, DENSITY_REFINE = 0, 1
 GUESS_SAD, GUESS_LEARNED, GUESS_SAD_PROJECTED = 0, 1, 2
