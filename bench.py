@@ -397,10 +397,12 @@ def water_cluster_files(tmpdir, seeds):
 
 
 def run_batch(args, rank, world, local_rank):
-    """256 water clusters: batched SCF (one launch per phase over all clusters
-    of a wave) from the learned guess, against the same clusters solved one by
-    one with SAD (sampled: every 8th cluster, scaled by 8). Waves are filled
-    until less than 24 GB of device memory is free. Strong scaling over ranks."""
+    """256 water clusters: batched SCF (one launch per FP64 phase over all
+    clusters of a wave, tensor-core incremental K per cluster) from the learned
+    guess, against the same clusters solved one by one with SAD and plain FP64
+    and with the learned guess and tensor-core K (sampled: every 8th cluster,
+    scaled by 8). Waves are filled until less than 40 GB of device memory is
+    free. Strong scaling over ranks."""
     import tempfile
     sys.path.insert(0, PKG)
     import tinyscf
@@ -415,14 +417,16 @@ def run_batch(args, rank, world, local_rank):
             sizes.append(int(f.readline()))
     order = sorted(range(len(paths)), key=lambda k: -sizes[k])
 
-    def engine(p, guess):
+    def engine(p, guess, mixed=False):
         e = tinyscf.TinySCF(BAS, DFBAS, p, 100, device=local_rank)
         e.setup(guess=guess)
+        if mixed:
+            e.set_k_precision(tinyscf.K_MIXED)
         e.s.ene_tol = args.ene_tol
         return e
 
     # warm-up: one small batch (kernels, cuSOLVER handles)
-    w = [engine(paths[order[-1]], tinyscf.GUESS_LEARNED), engine(paths[order[-2]], tinyscf.GUESS_LEARNED)]
+    w = [engine(paths[order[-1]], tinyscf.GUESS_LEARNED, True), engine(paths[order[-2]], tinyscf.GUESS_LEARNED, True)]
     bw = tinyscf.TinySCFBatch(w)
     bw.do_SCF()
     bw.free()
@@ -436,11 +440,11 @@ def run_batch(args, rank, world, local_rank):
         wave = []
         t0 = time.perf_counter()
         while k < len(order):
-            e = engine(paths[order[k]], tinyscf.GUESS_LEARNED)
+            e = engine(paths[order[k]], tinyscf.GUESS_LEARNED, True)
             wave.append(e)
             guess_ms += e.timings()["GUESS"]
             k += 1
-            if tinyscf.device_memory(local_rank)[0] < 24 * 2 ** 30:
+            if tinyscf.device_memory(local_rank)[0] < 40 * 2 ** 30:
                 break
         setup_s += time.perf_counter() - t0
         b = tinyscf.TinySCFBatch(wave)
@@ -461,7 +465,7 @@ def run_batch(args, rank, world, local_rank):
     seq_sad, seq_ml, it_sad = 0.0, 0.0, []
     for kk in sample:
         for guess in (None, tinyscf.GUESS_LEARNED):
-            e = engine(paths[kk], guess)
+            e = engine(paths[kk], guess, guess is not None)
             g = e.timings()["GUESS"]
             e.do_SCF()
             t = g + e.timings()["SCF"]
@@ -486,10 +490,13 @@ def run_batch(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": total, "unit": "s", "n_gpus": world, "steps": 1, "warmup": 1,
             "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
+            "dtype": "bf16x2-split/f32/f64", "data": "synthetic",
             "config": {"workload": "waters256: " + CONFIGS["waters256"] + ", cc-pVDZ / cc-pVDZ-RI (Cartesian)",
                        "clusters": len(order), "basis_functions": [min(sizes) // 3 * 25, max(sizes) // 3 * 25],
                        "timed": "learned guess + batched SCF of every cluster (device time), set-up excluded",
+                       "form": "batched: learned guess, tensor-core incremental K per molecule, batched FP64 J / DIIS "
+                               "/ density and final FP64 Fock build; sequential_sad_plain: SAD, FP64, one by one; "
+                               "sequential_learned: learned guess + tensor-core K, one by one",
                        "waves": waves, "batched_launches": launches,
                        "iterations": {"learned_batched_mean": statistics.mean(iters), "max": max(iters),
                                       "sad_sample_mean": statistics.mean(it_sad)},

@@ -189,7 +189,10 @@ TINYSCF_API int TinySCF_device_memory(int device, long long *free_bytes, long lo
 TINYSCF_API int TinySCF_autotune_report(char *buf, int len);
 /* Batched SCF over many molecules of uneven size. Each molecule is a handle
  * set up through the single-molecule calls (up to TinySCF_build_DF_tensor,
- * any initial guess; FP64 exchange). TinySCF_batch_do_SCF then iterates all of
+ * any initial guess; FP64 exchange, or TINYSCF_K_MIXED: then its exchange is
+ * the tensor-core incremental build, one molecule at a time, and one batched
+ * FP64 Fock build on the converged densities gives its energy, as
+ * TinySCF_do_SCF does). TinySCF_batch_do_SCF then iterates all of
  * them together: every SCF phase (J, K, Fock + energy, DIIS, density) is one
  * launch over all molecules still iterating, the eigensolves one batched
  * cuSOLVER call per group of equal basis size. Each molecule follows its own
@@ -203,7 +206,8 @@ TINYSCF_API int TinySCF_batch_do_SCF(TinySCF_batch_t b);
  * iterations (the slowest molecule's count) and the kernels it launched. */
 TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long long *launches);
 /* Device time (ms) of the last TinySCF_batch_do_SCF by phase: [0] J,
- * [1] K, [2] Fock + energy, [3] DIIS, [4] density; min(n, 5) values. */
+ * [1] K, [2] Fock + energy, [3] DIIS, [4] density, [5] final FP64 Fock build
+ * of the molecules set to TINYSCF_K_MIXED; min(n, 6) values. */
 TINYSCF_API int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n);
 TINYSCF_API int TinySCF_batch_free(TinySCF_batch_t b);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its

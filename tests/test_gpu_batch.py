@@ -58,3 +58,30 @@ def test_batch_matches_single_molecule_scf(tmp_path, guess):
     b.free()
     for e in engines:
         e.free()
+
+
+def test_batch_mixed_k_matches_single_molecule(tmp_path):
+    """Molecules set to the tensor-core incremental K iterate in the batch with
+    the same final FP64 Fock build as their own SCF: same energies."""
+    paths = _molecules(tmp_path)[:5]
+    single = []
+    for p in paths:
+        e = _engine(p, tinyscf.GUESS_LEARNED)
+        e.set_k_precision(tinyscf.K_MIXED)
+        e.do_SCF()
+        single.append((e.energy, e.s.iter))
+        e.free()
+    engines = []
+    for p in paths:
+        e = _engine(p, tinyscf.GUESS_LEARNED)
+        e.set_k_precision(tinyscf.K_MIXED)
+        engines.append(e)
+    b = tinyscf.TinySCFBatch(engines)
+    b.do_SCF()
+    assert b.phase_ms()["FINAL"] > 0
+    for e, (E, it) in zip(engines, single):
+        assert abs(e.energy - E) < 1e-9, (e.energy, E)
+        assert e.s.iter == it
+    b.free()
+    for e in engines:
+        e.free()

@@ -294,15 +294,15 @@ void batch_j(const BatchPlan &b, cudaStream_t s)
     g_launches += 4;
 }
 
-void batch_k(const BatchPlan &b, cudaStream_t s)
+void batch_k(const BatchPlan &b, const int *kact, cudaStream_t s)
 {
-    if (b.half.total) kb_half<<<b.half.total, 256, 0, s>>>(b.mols, b.active, b.half);
-    if (b.half_wide.total) kb_half_wide<<<b.half_wide.total, 256, 0, s>>>(b.mols, b.active, b.half_wide);
-    if (b.half_dmma.total) kb_half_dmma<<<b.half_dmma.total, 256, 0, s>>>(b.mols, b.active, b.half_dmma);
-    if (b.syrk.total) kb_syrk<<<b.syrk.total, 256, 0, s>>>(b.mols, b.active, b.syrk);
-    if (b.syrk128.total) kb_syrk128<<<b.syrk128.total, 256, 0, s>>>(b.mols, b.active, b.syrk128);
-    if (b.syrk_dmma.total) kb_syrk_dmma<<<b.syrk_dmma.total, 256, 0, s>>>(b.mols, b.active, b.syrk_dmma);
-    kb_syrk_reduce<<<b.nn256.total, 256, 0, s>>>(b.mols, b.active, b.nn256);
+    if (b.half.total) kb_half<<<b.half.total, 256, 0, s>>>(b.mols, kact, b.half);
+    if (b.half_wide.total) kb_half_wide<<<b.half_wide.total, 256, 0, s>>>(b.mols, kact, b.half_wide);
+    if (b.half_dmma.total) kb_half_dmma<<<b.half_dmma.total, 256, 0, s>>>(b.mols, kact, b.half_dmma);
+    if (b.syrk.total) kb_syrk<<<b.syrk.total, 256, 0, s>>>(b.mols, kact, b.syrk);
+    if (b.syrk128.total) kb_syrk128<<<b.syrk128.total, 256, 0, s>>>(b.mols, kact, b.syrk128);
+    if (b.syrk_dmma.total) kb_syrk_dmma<<<b.syrk_dmma.total, 256, 0, s>>>(b.mols, kact, b.syrk_dmma);
+    kb_syrk_reduce<<<b.nn256.total, 256, 0, s>>>(b.mols, kact, b.nn256);
     g_launches += 1 + (b.half.total > 0) + (b.half_wide.total > 0) + (b.half_dmma.total > 0) + (b.syrk.total > 0) +
                   (b.syrk128.total > 0) + (b.syrk_dmma.total > 0);
 }

@@ -45,7 +45,8 @@ struct BatchPlan {
 };
 
 void batch_j(const BatchPlan &b, cudaStream_t s);
-void batch_k(const BatchPlan &b, cudaStream_t s);
+// kact: per-molecule flags of the molecules whose exchange is built here (FP64)
+void batch_k(const BatchPlan &b, const int *kact, cudaStream_t s);
 void batch_fock(const BatchPlan &b, double *d_Eall, cudaStream_t s);
 void batch_diis(const BatchPlan &b, bool full, cudaStream_t s);
 void batch_gemm(const BatchGemm &g, const int *d_active, cudaStream_t s);

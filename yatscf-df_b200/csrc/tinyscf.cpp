@@ -776,7 +776,7 @@ int sparsity_impl(TinySCF_t t)
         e->ktile = KSYRK_DMMA;
         e->ksplit = h128;
     }
-    e->khwide = 0;
+    e->khwide = nbf >= 384 ? 2 : 0;
     RC(dalloc(e, &e->Kpart, (size_t) e->ksplit_max * nbf * nbf));
     {
         std::vector<int2> tl, tl2;
@@ -1744,13 +1744,16 @@ struct TinySCF_batch_struct {
     cusolverDnParams_t params = nullptr;
     double *d_Eall = nullptr;
     int *d_active = nullptr;
+    int *d_kact = nullptr;             // molecules whose K the batched FP64 kernels build this iteration
+    std::vector<char> mixed;           // molecules with the tensor-core incremental K
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double scf_ms = 0.0;
     int iterations = 0;
     long long launches = 0;
-    // per-phase device time of the last batched SCF: J, K, Fock + energy, DIIS, density
+    // per-phase device time of the last batched SCF: J, K, Fock + energy, DIIS, density,
+    // final FP64 Fock build of the mixed-precision molecules
     cudaEvent_t pev[6] = {};
-    double phase_ms[5] = {};
+    double phase_ms[6] = {};
 };
 
 namespace {
@@ -1935,6 +1938,9 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     p.active = da;
     b->d_active = da;
     RC(balloc(b, &b->d_Eall, nmol));
+    RC(balloc(b, &b->d_kact, nmol));
+    b->mixed.assign(nmol, 0);
+    for (int k = 0; k < nmol; k++) b->mixed[k] = E_(ts[k])->kprec == TINYSCF_K_MIXED && E_(ts[k])->kmix != nullptr;
     RC(make_list(b, c_nup256, p.nup256));
     RC(make_list(b, c_jblk, p.jblk));
     RC(make_list(b, c_naux256, p.naux256));
@@ -1995,9 +2001,17 @@ int batch_scf_impl(TinySCF_batch_t b)
         // the loop consumes the guess (or the state a reset left) exactly like do_SCF
         TSCF_CUDA_CHECK(cudaStreamSynchronize(E_(t)->s));
     }
-    TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
+    std::vector<int> kact(nmol, 0);
+    auto upload_flags = [&]() {
+        for (int k = 0; k < nmol; k++) kact[k] = act[k] && !b->mixed[k];
+        cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s);
+        return cudaMemcpyAsync(b->d_kact, kact.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s);
+    };
+    TSCF_CUDA_CHECK(upload_flags());
     const long long l0 = g_launches;
     for (double &v : b->phase_ms) v = 0.0;
+    for (int k = 0; k < nmol; k++)   // a molecule's incremental K restarts with each batched solve
+        if (b->mixed[k]) kmix_reset(E_(b->mols[k])->kmix, b->s);
     cudaEventRecord(b->ev0, b->s);
     int it = 0;
     for (;; it++) {
@@ -2007,7 +2021,13 @@ int batch_scf_impl(TinySCF_batch_t b)
         cudaEventRecord(b->pev[0], b->s);
         batch_j(b->plan, b->s);
         cudaEventRecord(b->pev[1], b->s);
-        batch_k(b->plan, b->s);
+        batch_k(b->plan, b->d_kact, b->s);
+        for (int k = 0; k < nmol; k++) {   // tensor-core incremental exchange, one molecule at a time
+            if (!act[k] || !b->mixed[k]) continue;
+            Engine *e = E_(b->mols[k]);
+            RC(kmix_build(e->kmix, e->Cocc, e->S, e->Kmix, b->s));
+            TSCF_CUDA_CHECK(cudaMemcpyAsync(e->K, e->Kmix, sizeof(double) * e->nn, cudaMemcpyDeviceToDevice, b->s));
+        }
         cudaEventRecord(b->pev[2], b->s);
         batch_fock(b->plan, b->d_Eall, b->s);
         cudaEventRecord(b->pev[3], b->s);
@@ -2037,7 +2057,35 @@ int batch_scf_impl(TinySCF_batch_t b)
             t->iter++;
             if (!(t->iter < t->niters && delta[k] >= t->ene_tol)) act[k] = 0;
         }
+        TSCF_CUDA_CHECK(upload_flags());
+    }
+    // one FP64 Fock build on the converged density of every mixed-precision molecule;
+    // its energy is the result (as TinySCF_do_SCF does for one molecule)
+    bool any_mixed = false;
+    for (int k = 0; k < nmol; k++) {
+        act[k] = b->mixed[k];
+        any_mixed |= b->mixed[k] != 0;
+    }
+    if (any_mixed) {
         TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_kact, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
+        cudaEventRecord(b->pev[0], b->s);
+        batch_j(b->plan, b->s);
+        batch_k(b->plan, b->d_kact, b->s);
+        batch_fock(b->plan, b->d_Eall, b->s);
+        cudaEventRecord(b->pev[1], b->s);
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(Eh.data(), b->d_Eall, sizeof(double) * nmol, cudaMemcpyDeviceToHost, b->s));
+        TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
+        float pm = 0.f;
+        cudaEventElapsedTime(&pm, b->pev[0], b->pev[1]);
+        b->phase_ms[5] += pm;
+        for (int k = 0; k < nmol; k++)
+            if (b->mixed[k]) b->mols[k]->HF_energy = Eh[k];
+        const int fl = kmix_error_flag();
+        if (fl) {
+            fprintf(stderr, "[tinyscf] tensor-core K: a bounded wait timed out (code %d)\n", fl);
+            return ERR_CUDA;
+        }
     }
     cudaEventRecord(b->ev1, b->s);
     TSCF_CUDA_CHECK(cudaEventSynchronize(b->ev1));
@@ -2053,11 +2101,11 @@ int batch_scf_impl(TinySCF_batch_t b)
             TSCF_CUDA_CHECK(cudaMemcpyAsync(e->w, g.W + k * g.n, sizeof(double) * g.n, cudaMemcpyDeviceToDevice, b->s));
         }
     TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
-    for (TinySCF_t t : b->mols) {
-        Engine *e = E_(t);
-        e->F_is_orth = true;
+    for (int k = 0; k < nmol; k++) {
+        Engine *e = E_(b->mols[k]);
+        e->F_is_orth = !b->mixed[k];   // after the final build F holds H + 2J - K
         e->have_eig = false;
-        RC(sync_host_impl(t));
+        RC(sync_host_impl(b->mols[k]));
     }
     return OK;
 }
@@ -2144,7 +2192,7 @@ int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long
 int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n)
 {
     if (!b || !ms) return TINYSCF_ERR_STATE;
-    for (int q = 0; q < n && q < 5; q++) ms[q] = b->phase_ms[q];
+    for (int q = 0; q < n && q < 6; q++) ms[q] = b->phase_ms[q];
     return TINYSCF_OK;
 }
 

@@ -406,9 +406,9 @@ class TinySCFBatch:
 
     def phase_ms(self):
         """{phase: device ms} of the last batched SCF."""
-        ms = np.zeros(5)
-        self.lib.TinySCF_batch_phase_ms(self.b, _dptr(ms), 5)
-        return dict(zip(("J", "K", "FOCK", "DIIS", "DENSITY"), (float(v) for v in ms)))
+        ms = np.zeros(6)
+        self.lib.TinySCF_batch_phase_ms(self.b, _dptr(ms), 6)
+        return dict(zip(("J", "K", "FOCK", "DIIS", "DENSITY", "FINAL"), (float(v) for v in ms)))
 
     def free(self):
         if self.b:
