@@ -284,6 +284,7 @@ def run_ours(args, rank, world, local_rank):
     # end to end through the C ABI from files: parse, integrals, DF tensor, SCF,
     # host mirrors of the results (S, H, X, F, D, J, K, Cocc) copied back.
     e2e_times, h2d, d2h = [], 0, 0
+    setup_tuned, n3c = None, 0
     for _ in range(args.e2e_steps):
         t0 = time.perf_counter()
         e2 = tinyscf.TinySCF(BAS, DFBAS, xyz, 100, device=local_rank)
@@ -296,6 +297,8 @@ def run_ours(args, rank, world, local_rank):
         e2.do_SCF()
         _ = e2.energy
         c = e2.counters()
+        setup_tuned = e2.timings()
+        n3c = c[5]
         e2.free()
         e2e_times.append(time.perf_counter() - t0)
         h2d, d2h = c[1], c[2]
@@ -321,6 +324,25 @@ def run_ours(args, rank, world, local_rank):
         achieved = fg / (g_ms * 1e-3) / 1e12
         note = ("algorithmic flops of one G = dT S^T build over k_gemm's average device time (CUDA events around "
                 "each launch); tensor_pipe_frac counts the 3 BF16 products executed per algorithmic flop")
+    # achieved rates of the set-up and FP64 kernels per unit of work: 3-centre output bytes and quartets,
+    # DF GEMM 2 nu naux^2 flops, J 2 nu naux 8 bytes (two streams of the DF tensor), FP64 K flops; set-up
+    # phases from the e2e engine (the autotuner's table already filled, so no tuning runs inside)
+    su = setup_tuned if setup_tuned is not None else st
+    nu = (nnz + nbf) // 2                      # unique pairs: rows of the DF tensor
+    rates = {
+        "3c_integrals": {"ms": su["3C"], "bytes_written": nu * naux * 8,
+                         "GB_per_s": nu * naux * 8 / (su["3C"] * 1e-3) / 1e9,
+                         "quartets_per_s": (n3c / (su["3C"] * 1e-3)) if n3c else None},
+        "df_gemm": {"ms": su["DFGEMM"], "TFLOP_per_s": 2.0 * nu * naux * naux / (su["DFGEMM"] * 1e-3) / 1e12},
+        "j_build": {"ms": stats["J"][0] / max(1, stats["J"][1]),
+                    "GB_per_s": 2.0 * nu * naux * 8 / (stats["J"][0] / max(1, stats["J"][1]) * 1e-3) / 1e9,
+                    "frac_of_hbm": 2.0 * nu * naux * 8 / (stats["J"][0] / max(1, stats["J"][1]) * 1e-3) / 1e9 / hbm},
+        "k_fp64_halftransform": {"ms": stats["K_HT"][0] / max(1, stats["K_HT"][1]),
+                                 "TFLOP_per_s": fht / (stats["K_HT"][0] / max(1, stats["K_HT"][1]) * 1e-3) / 1e12},
+        "k_fp64_rank_k": {"ms": stats["K_SYRK"][0] / max(1, stats["K_SYRK"][1]),
+                          "TFLOP_per_s": fsy / (stats["K_SYRK"][0] / max(1, stats["K_SYRK"][1]) * 1e-3) / 1e12},
+        "setup_from": "e2e engine (autotuner table filled)" if setup_tuned is not None else "first engine (incl. tuning)",
+    }
     traffic = None
     tp = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -379,6 +401,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "clocks": clk,
             "k_tflops": (fht + fsy) / (k_ms * 1e-3) / 1e12,
+            "kernel_rates": rates,
         }
         print(json.dumps(line))
     if dist is not None:

@@ -88,7 +88,8 @@ TINYSCF_API int TinySCF_reset_timing_stats(TinySCF_t t);
 /* Counters: [0] engine kernels launched by this process, [1] bytes copied
  * host->device, [2] bytes copied device->host by this engine instance,
  * [3] full eigensolves and [4] occupied-subspace refinement steps taken by
- * the density builds of this instance. */
+ * the density builds of this instance, [5] (shell pair, aux shell) tuples the
+ * last 3-centre integral build launched (before screening). */
 TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
 /* Coulomb matrix J from a density D without allocating anything: for callers
  * that cannot call cudaMalloc (a host framework that owns all device memory

@@ -301,6 +301,7 @@ struct Engine {
     bool have_eig = false;        // V, w hold a full eigensolve of an earlier F'
     SubspaceWork sw{};
     long long n_eig = 0, n_refine = 0;
+    long long n3c_quartets = 0;   // (shell pair, aux shell) tuples of the last DF build
     // CUDA-graph iteration (Fock, DIIS and, with the refinement solver, the density)
     bool use_graph = false;
     bool capturing = false;
@@ -996,6 +997,7 @@ int df_impl(TinySCF_t t)
     DevShells v = shells_view(e->dsh, t->nshells), av = shells_view(e->dash, t->df_nshells);
     tstart(e, TINYSCF_T_3C);
     launch_three_center(v, av, pl, pqA, e->s);
+    e->n3c_quartets = (long long) pl.npairs * t->df_nshells;
     tstop(e, TINYSCF_T_3C);
     RC(cuda_rc("3-centre integrals"));
     RC(dalloc(e, &Jpq, (size_t) naux * naux));
@@ -1702,8 +1704,8 @@ int TinySCF_get_counters(TinySCF_t t, long long *out, int n)
 {
     if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
-    long long v[5] = {g_launches, e->h2d, e->d2h, e->n_eig, e->n_refine};
-    for (int k = 0; k < n && k < 5; k++) out[k] = v[k];
+    long long v[6] = {g_launches, e->h2d, e->d2h, e->n_eig, e->n_refine, e->n3c_quartets};
+    for (int k = 0; k < n && k < 6; k++) out[k] = v[k];
     return TINYSCF_OK;
 }
 

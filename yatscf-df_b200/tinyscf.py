@@ -332,9 +332,9 @@ class TinySCF:
 
     def counters(self):
         """(engine kernel launches in this process, bytes host->device, bytes device->host,
-        full eigensolves, subspace refinement steps)."""
-        out = (ctypes.c_longlong * 5)()
-        self.lib.TinySCF_get_counters(self.t, out, 5)
+        full eigensolves, subspace refinement steps, 3-centre (shell pair, aux shell) tuples)."""
+        out = (ctypes.c_longlong * 6)()
+        self.lib.TinySCF_get_counters(self.t, out, 6)
         return tuple(int(v) for v in out)
 
     def timings(self):
