@@ -445,6 +445,7 @@ def run_batch(args, rank, world, local_rank):
         e.setup(guess=guess)
         if mixed:
             e.set_k_precision(tinyscf.K_MIXED)
+            e.set_density_solver(tinyscf.DENSITY_REFINE)
         e.s.ene_tol = args.ene_tol
         return e
 
@@ -517,9 +518,10 @@ def run_batch(args, rank, world, local_rank):
             "config": {"workload": "waters256: " + CONFIGS["waters256"] + ", cc-pVDZ / cc-pVDZ-RI (Cartesian)",
                        "clusters": len(order), "basis_functions": [min(sizes) // 3 * 25, max(sizes) // 3 * 25],
                        "timed": "learned guess + batched SCF of every cluster (device time), set-up excluded",
-                       "form": "batched: learned guess, tensor-core incremental K per molecule, batched FP64 J / DIIS "
-                               "/ density and final FP64 Fock build; sequential_sad_plain: SAD, FP64, one by one; "
-                               "sequential_learned: learned guess + tensor-core K, one by one",
+                       "form": "batched: learned guess, tensor-core incremental K and subspace-refined density per "
+                               "molecule, batched FP64 J / DIIS / eigensolves and final FP64 Fock build; "
+                               "sequential_sad_plain: SAD, FP64, full eigensolves, one by one; sequential_learned: "
+                               "learned guess + tensor-core K + refinement, one by one",
                        "waves": waves, "batched_launches": launches,
                        "iterations": {"learned_batched_mean": statistics.mean(iters), "max": max(iters),
                                       "sad_sample_mean": statistics.mean(it_sad)},

@@ -85,3 +85,32 @@ def test_batch_mixed_k_matches_single_molecule(tmp_path):
     b.free()
     for e in engines:
         e.free()
+
+
+def test_batch_refine_density_matches_single_molecule(tmp_path):
+    """Molecules set to the subspace-refinement density solver refine in the
+    batch as in their own SCF: same energies."""
+    paths = _molecules(tmp_path)[:5]
+    single = []
+    for p in paths:
+        e = _engine(p, tinyscf.GUESS_LEARNED)
+        e.set_density_solver(tinyscf.DENSITY_REFINE)
+        e.do_SCF()
+        single.append((e.energy, e.s.iter))
+        e.free()
+    engines = []
+    for p in paths:
+        e = _engine(p, tinyscf.GUESS_LEARNED)
+        e.set_density_solver(tinyscf.DENSITY_REFINE)
+        engines.append(e)
+    b = tinyscf.TinySCFBatch(engines)
+    c0 = [e.counters() for e in engines]
+    b.do_SCF()
+    refined = sum(e.counters()[4] - c[4] for e, c in zip(engines, c0))
+    for e, (E, it) in zip(engines, single):
+        assert abs(e.energy - E) < 1e-9, (e.energy, E)
+        assert abs(e.s.iter - it) <= 1
+    assert refined > 0
+    b.free()
+    for e in engines:
+        e.free()

@@ -348,9 +348,9 @@ void batch_diis(const BatchPlan &b, bool full, cudaStream_t s)
     g_launches += 6;
 }
 
-void batch_copy_fp(const BatchPlan &b, cudaStream_t s)
+void batch_copy_fp(const BatchPlan &b, const int *mask, cudaStream_t s)
 {
-    kb_copy_fp<<<b.nn256.total, 256, 0, s>>>(b.mols, b.active, b.nn256);
+    kb_copy_fp<<<b.nn256.total, 256, 0, s>>>(b.mols, mask, b.nn256);
     g_launches++;
 }
 

@@ -50,7 +50,8 @@ void batch_k(const BatchPlan &b, const int *kact, cudaStream_t s);
 void batch_fock(const BatchPlan &b, double *d_Eall, cudaStream_t s);
 void batch_diis(const BatchPlan &b, bool full, cudaStream_t s);
 void batch_gemm(const BatchGemm &g, const int *d_active, cudaStream_t s);
-void batch_copy_fp(const BatchPlan &b, cudaStream_t s);
+// F' of the molecules flagged in mask into their eigensolver slots
+void batch_copy_fp(const BatchPlan &b, const int *mask, cudaStream_t s);
 void diis_solve_batched(const MolDev *d_mols, const int *d_active, int nmol, cudaStream_t s);
 
 }  // namespace tscf

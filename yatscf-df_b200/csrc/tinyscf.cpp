@@ -1747,6 +1747,7 @@ struct TinySCF_batch_struct {
     double *d_Eall = nullptr;
     int *d_active = nullptr;
     int *d_kact = nullptr;             // molecules whose K the batched FP64 kernels build this iteration
+    int *d_need = nullptr;             // molecules whose density takes an eigensolve this iteration
     std::vector<char> mixed;           // molecules with the tensor-core incremental K
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double scf_ms = 0.0;
@@ -1941,6 +1942,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     b->d_active = da;
     RC(balloc(b, &b->d_Eall, nmol));
     RC(balloc(b, &b->d_kact, nmol));
+    RC(balloc(b, &b->d_need, nmol));
     b->mixed.assign(nmol, 0);
     for (int k = 0; k < nmol; k++) b->mixed[k] = E_(ts[k])->kprec == TINYSCF_K_MIXED && E_(ts[k])->kmix != nullptr;
     RC(make_list(b, c_nup256, p.nup256));
@@ -1967,10 +1969,21 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     return OK;
 }
 
-int batch_eigs(TinySCF_batch_t b)
+// Eigensolves of the flagged molecules: one batched call per group when every
+// member needs one, else one syevd per flagged member.
+int batch_eigs(TinySCF_batch_t b, const std::vector<int> &need)
 {
     for (auto &g : b->groups) {
         const int64_t cnt = (int64_t) g.members.size(), n = g.n;
+        int64_t nneed = 0;
+        for (int m : g.members) nneed += need[m] ? 1 : 0;
+        if (nneed == 0) continue;
+        if (nneed < cnt) {
+            if (!g.eig && !(g.eig = eig_create(g.n, b->s))) return ERR_CUDA;
+            for (int64_t k = 0; k < cnt; k++)
+                if (need[g.members[k]]) RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
+            continue;
+        }
         if (g.batched) {
             cusolverStatus_t st = cusolverDnXsyevBatched(b->h, b->params, CUSOLVER_EIG_MODE_VECTOR,
                                                          CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, g.A, n, CUDA_R_64F,
@@ -1984,6 +1997,7 @@ int batch_eigs(TinySCF_batch_t b)
             }
         }
         if (!g.batched) {
+            if (!g.eig && !(g.eig = eig_create(g.n, b->s))) return ERR_CUDA;
             for (int64_t k = 0; k < cnt; k++)
                 RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
         }
@@ -2003,7 +2017,8 @@ int batch_scf_impl(TinySCF_batch_t b)
         // the loop consumes the guess (or the state a reset left) exactly like do_SCF
         TSCF_CUDA_CHECK(cudaStreamSynchronize(E_(t)->s));
     }
-    std::vector<int> kact(nmol, 0);
+    std::vector<int> kact(nmol, 0), need(nmol, 0);
+    for (int k = 0; k < nmol; k++) E_(b->mols[k])->have_eig = false;   // each batched solve starts from eigensolves
     auto upload_flags = [&]() {
         for (int k = 0; k < nmol; k++) kact[k] = act[k] && !b->mixed[k];
         cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s);
@@ -2035,10 +2050,45 @@ int batch_scf_impl(TinySCF_batch_t b)
         cudaEventRecord(b->pev[3], b->s);
         batch_diis(b->plan, it >= 2, b->s);
         cudaEventRecord(b->pev[4], b->s);
-        batch_copy_fp(b->plan, b->s);
-        RC(batch_eigs(b));
-        batch_gemm(b->plan.g_cocc, b->d_active, b->s);
-        batch_gemm(b->plan.g_dens, b->d_active, b->s);
+        // density: molecules set to TINYSCF_DENSITY_REFINE first refine their
+        // occupied subspace (host-checked steps, one molecule at a time); the
+        // rest, and those whose refinement did not converge, take eigensolves
+        for (int k = 0; k < nmol; k++) {
+            need[k] = act[k];
+            if (!act[k]) continue;
+            Engine *e = E_(b->mols[k]);
+            const int n = b->mols[k]->nbasfuncs, o = b->mols[k]->n_occ;
+            if (e->dmode != TINYSCF_DENSITY_REFINE || !e->have_eig || o <= 0 || o >= n) continue;
+            int steps = 0;
+            double res = 0.0;
+            RC(subspace_refine(e->Fp, e->V, e->w, e->U, n, o, e->sw, kRefineTol, kRefineSteps, &steps, &res, b->s));
+            e->n_refine += steps;
+            if (res < kRefineTol) {
+                density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, b->s);
+                need[k] = 0;
+            }
+        }
+        TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_need, need.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
+        batch_copy_fp(b->plan, b->d_need, b->s);
+        RC(batch_eigs(b, need));
+        batch_gemm(b->plan.g_cocc, b->d_need, b->s);
+        batch_gemm(b->plan.g_dens, b->d_need, b->s);
+        for (auto &g : b->groups)   // new eigenbases of the refinement molecules
+            for (size_t q = 0; q < g.members.size(); q++) {
+                const int k = g.members[q];
+                Engine *e = E_(b->mols[k]);
+                if (!need[k]) continue;
+                e->n_eig++;
+                if (e->dmode != TINYSCF_DENSITY_REFINE || !e->U) continue;
+                const int n = g.n, o = b->mols[k]->n_occ;
+                TSCF_CUDA_CHECK(cudaMemcpyAsync(e->V, g.A + q * (size_t) n * n, sizeof(double) * (size_t) n * n,
+                                                cudaMemcpyDeviceToDevice, b->s));
+                TSCF_CUDA_CHECK(cudaMemcpyAsync(e->w, g.W + q * (size_t) n, sizeof(double) * n,
+                                                cudaMemcpyDeviceToDevice, b->s));
+                TSCF_CUDA_CHECK(cudaMemcpyAsync(e->U, e->V, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice,
+                                                b->s));
+                e->have_eig = true;
+            }
         cudaEventRecord(b->pev[5], b->s);
         TSCF_CUDA_CHECK(cudaMemcpyAsync(Eh.data(), b->d_Eall, sizeof(double) * nmol, cudaMemcpyDeviceToHost, b->s));
         TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
@@ -2096,10 +2146,11 @@ int batch_scf_impl(TinySCF_batch_t b)
     b->scf_ms = ms;
     b->iterations = it;
     b->launches = g_launches - l0;
-    // eigenvalues and host mirrors of every molecule
+    // eigenvalues (of the last full eigensolve) and host mirrors of every molecule
     for (auto &g : b->groups)
         for (size_t k = 0; k < g.members.size(); k++) {
             Engine *e = E_(b->mols[g.members[k]]);
+            if (e->dmode == TINYSCF_DENSITY_REFINE && e->U) continue;   // w already holds it
             TSCF_CUDA_CHECK(cudaMemcpyAsync(e->w, g.W + k * g.n, sizeof(double) * g.n, cudaMemcpyDeviceToDevice, b->s));
         }
     TSCF_CUDA_CHECK(cudaStreamSynchronize(b->s));
