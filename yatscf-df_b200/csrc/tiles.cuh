@@ -90,8 +90,8 @@ __device__ __forceinline__ void dgemm_tile_dmma(int m, int n, int k, double alph
                                                 int ldc, int m0, int n0)
 {
     constexpr int BT = 128;
-    __shared__ double As[GB_K][BT + 2];
-    __shared__ double Bs[GB_K][BT + 2];
+    __shared__ double As[BT][GB_K + 4];   // row-major in M / N: conflict-free fragment reads
+    __shared__ double Bs[BT][GB_K + 4];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
     const int fr = lane >> 2, fc = lane & 3;
@@ -107,20 +107,20 @@ __device__ __forceinline__ void dgemm_tile_dmma(int m, int n, int k, double alph
             int row, kk;
             if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / BT; row = l % BT; }
             const int gi = m0 + row, gk = k0 + kk;
-            As[kk][row] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
+            As[row][kk] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
             int col;
             if (!TB) { kk = l / BT; col = l % BT; } else { col = l / GB_K; kk = l % GB_K; }
             const int gj = n0 + col, gk2 = k0 + kk;
-            Bs[kk][col] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
+            Bs[col][kk] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
         }
         __syncthreads();
 #pragma unroll
         for (int k4 = 0; k4 < GB_K; k4 += 4) {
             double a[8], b[4];
 #pragma unroll
-            for (int x = 0; x < 8; x++) a[x] = As[k4 + fc][wm + 8 * x + fr];
+            for (int x = 0; x < 8; x++) a[x] = As[wm + 8 * x + fr][k4 + fc];
 #pragma unroll
-            for (int y = 0; y < 4; y++) b[y] = Bs[k4 + fc][wn + 8 * y + fr];
+            for (int y = 0; y < 4; y++) b[y] = Bs[wn + 8 * y + fr][k4 + fc];
 #pragma unroll
             for (int x = 0; x < 8; x++)
 #pragma unroll
@@ -393,8 +393,10 @@ __device__ __forceinline__ void syrk_tile128(const double *__restrict__ T, int n
 __device__ __forceinline__ void syrk_tile_dmma(const double *__restrict__ T, int nbf, long long Q, long long q_beg,
                                                long long q_end, int i0, int j0, double *__restrict__ out)
 {
-    __shared__ double As[KT_K][KB_T + 2];
-    __shared__ double Bs[KT_K][KB_T + 2];
+    // operands stored row-major in M/N with rows of KT_K + 4 doubles: the
+    // fragment reads (8 rows x 4 K per warp) then hit 32 distinct banks per wavefront
+    __shared__ double As[KB_T][KT_K + 4];
+    __shared__ double Bs[KB_T][KT_K + 4];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;   // warp tile origin inside the CTA tile
     const int fr = lane >> 2, fc = lane & 3;                 // fragment row / column of this lane
@@ -420,8 +422,8 @@ __device__ __forceinline__ void syrk_tile_dmma(const double *__restrict__ T, int
 #pragma unroll
         for (int r = 0; r < 8; r++) {
             const int l = tid + 256 * r;
-            As[l % KT_K][l / KT_K] = pa[r];
-            Bs[l % KT_K][l / KT_K] = pb[r];
+            As[l / KT_K][l % KT_K] = pa[r];
+            Bs[l / KT_K][l % KT_K] = pb[r];
         }
         __syncthreads();
         if (q0 + KT_K < q_end) fetch(q0 + KT_K);
@@ -429,9 +431,9 @@ __device__ __forceinline__ void syrk_tile_dmma(const double *__restrict__ T, int
         for (int k4 = 0; k4 < KT_K; k4 += 4) {
             double a[8], b[4];
 #pragma unroll
-            for (int x = 0; x < 8; x++) a[x] = As[k4 + fc][wm + 8 * x + fr];   // A(row fr, k fc)
+            for (int x = 0; x < 8; x++) a[x] = As[wm + 8 * x + fr][k4 + fc];   // A(row fr, k fc)
 #pragma unroll
-            for (int y = 0; y < 4; y++) b[y] = Bs[k4 + fc][wn + 8 * y + fr];   // B(k fc, col fr)
+            for (int y = 0; y < 4; y++) b[y] = Bs[wn + 8 * y + fr][k4 + fc];   // B(k fc, col fr)
 #pragma unroll
             for (int x = 0; x < 8; x++)
 #pragma unroll
@@ -460,8 +462,11 @@ __device__ __forceinline__ void half_tile_dmma(const double *__restrict__ B, con
                                                const int *__restrict__ displs, int nocc, int naux,
                                                double *__restrict__ T, int i, int s0, int p0)
 {
-    __shared__ double As[KT_K][KH_S + 2];
-    __shared__ double Bs[KT_K][KH_P + 2];
+    // K-major rows padded by 4 doubles (a row offset of 8 banks): the fragment
+    // reads (4 K rows x 4 consecutive columns per 16-lane phase) and the
+    // prefetch stores (consecutive columns) are both free of bank conflicts
+    __shared__ double As[KT_K][KH_S + 4];
+    __shared__ double Bs[KT_K][KH_P + 4];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ws = (warp >> 2) * 32, wp = (warp & 3) * 64;
     const int fr = lane >> 2, fc = lane & 3;
