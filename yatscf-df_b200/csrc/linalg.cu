@@ -16,10 +16,11 @@ namespace tscf {
 long long g_launches = 0;
 
 // ------------------------------------------------------------------ DGEMM
-// Four tile shapes: FFMA 64x64 (default), 32x32 (more blocks for small
+// Five tile shapes: FFMA 64x64 (default), 32x32 (more blocks for small
 // matrices) and 128x64 (more reuse for large ones) (dgemm_tile), and 128x128
-// on the FP64 tensor cores (dgemm_tile_dmma). The autotuner picks one per call
-// shape the first time the shape is met outside a stream capture.
+// and 64x64 on the FP64 tensor cores (dgemm_tile_dmma, dgemm_tile_dmma64). The
+// autotuner picks one per call shape the first time the shape is met outside
+// a stream capture.
 template <bool TA, bool TB, int BM, int BN>
 __global__ void __launch_bounds__(256) k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, int lda,
                                                const double *__restrict__ B, int ldb, double beta, double *C, int ldc)
@@ -58,10 +59,30 @@ static void dgemm_dmma(bool ta, bool tb, int m, int n, int k, double alpha, cons
     else k_dgemm_dmma<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_dgemm_dmma64(int m, int n, int k, double alpha, const double *__restrict__ A,
+                                                      int lda, const double *__restrict__ B, int ldb, double beta,
+                                                      double *C, int ldc)
+{
+    dgemm_tile_dmma64<TA, TB>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, blockIdx.y * 64, blockIdx.x * 64);
+}
+
+static void dgemm_dmma64(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
+                         const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
+{
+    dim3 grid((n + 63) / 64, (m + 63) / 64);
+    g_launches++;
+    if (!ta && !tb) k_dgemm_dmma64<false, false><<<grid, 128, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (!ta && tb) k_dgemm_dmma64<false, true><<<grid, 128, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (ta && !tb) k_dgemm_dmma64<true, false><<<grid, 128, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else k_dgemm_dmma64<true, true><<<grid, 128, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
 static void dgemm_variant(int v, bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
                           const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
 {
-    if (v == 3) dgemm_dmma(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    if (v == 4) dgemm_dmma64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    else if (v == 3) dgemm_dmma(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else if (v == 1) dgemm_shape<32, 32>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else if (v == 2) dgemm_shape<128, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else dgemm_shape<64, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
@@ -88,7 +109,7 @@ void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
         const size_t ea = ta ? (size_t) k * lda : (size_t) m * lda, eb = tb ? (size_t) n * ldb : (size_t) k * ldb;
         if (tune_enabled() && cs == cudaStreamCaptureStatusNone && beta == 0.0 && disjoint(A, ea) && disjoint(B, eb) &&
             (double) m * n * k >= 2e6) {
-            v = tune_run(key, {0, 1, 2, 3}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
+            v = tune_run(key, {0, 1, 2, 3, 4}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
             return;
         }
     }

@@ -145,6 +145,70 @@ __device__ __forceinline__ void dgemm_tile_dmma(int m, int n, int k, double alph
     }
 }
 
+// ---- FP64 GEMM tile on the FP64 tensor cores, 64 x 64 outputs per 128
+// threads (4 warps of 32 x 32 = 4 x 4 DMMA tiles): four times the CTAs of the
+// 128 x 128 tile for the nbf-sized matrices of DIIS and the density.
+template <bool TA, bool TB>
+__device__ __forceinline__ void dgemm_tile_dmma64(int m, int n, int k, double alpha, const double *__restrict__ A,
+                                                  int lda, const double *__restrict__ B, int ldb, double beta,
+                                                  double *C, int ldc, int m0, int n0)
+{
+    constexpr int BT = 64;
+    __shared__ double As[BT][GB_K + 4];
+    __shared__ double Bs[BT][GB_K + 4];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int fr = lane >> 2, fc = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    for (int k0 = 0; k0 < k; k0 += GB_K) {
+#pragma unroll
+        for (int r = 0; r < BT * GB_K / 128; r++) {
+            const int l = tid + 128 * r;
+            int row, kk;
+            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / BT; row = l % BT; }
+            const int gi = m0 + row, gk = k0 + kk;
+            As[row][kk] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
+            int col;
+            if (!TB) { kk = l / BT; col = l % BT; } else { col = l / GB_K; kk = l % GB_K; }
+            const int gj = n0 + col, gk2 = k0 + kk;
+            Bs[col][kk] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < GB_K; k4 += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[wm + 8 * x + fr][k4 + fc];
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[wn + 8 * y + fr][k4 + fc];
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        const int gi = m0 + wm + 8 * x + fr;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int gj = n0 + wn + 8 * y + 2 * fc + h;
+                if (gj >= n) continue;
+                double *c = C + (size_t) gi * ldc + gj;
+                *c = (beta == 0.0) ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * *c;
+            }
+        }
+    }
+}
+
 // ---- K half-transform tile: T[i][s0:s0+64][p0:p0+64] = sum_{r in CSR row i} C[j_r][s] B[u_r][p]
 constexpr int KT_M = 64, KT_N = 64, KT_K = 16;
 
