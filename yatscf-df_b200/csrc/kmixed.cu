@@ -1,25 +1,25 @@
 // Mixed-precision exchange (K) on the 5th-generation tensor cores (tcgen05).
 //
-// Both K contractions run as one warp-specialised UMMA GEMM kernel with
-// K-major BF16 operands staged by TMA (128-byte swizzle) and an FP32
-// accumulator in tensor memory. Every FP64/FP32 operand x is split into
-// x_hi = bf16(x), x_lo = bf16(x - x_hi); each product uses three MMAs
-// (hi*hi + hi*lo + lo*hi), which keeps ~16 significant bits per operand.
+// Two warp-specialised UMMA kernels with K-major BF16 operands staged by TMA
+// (128-byte swizzle) and FP32 accumulators in tensor memory. Every FP64/FP32
+// operand x is split into x_hi = bf16(x), x_lo = bf16(x - x_hi); a product
+// uses three MMAs (hi*hi + hi*lo + lo*hi; the half-transform adds lo*lo),
+// which keeps ~16 significant bits per operand.
 //
 // The K build is incremental (build_Fock.c:244-347 restated on differences):
 //   C'_n  = C_n R,  R = polar(C_n^T S C_{n-1})       (align the occupied orbitals)
 //   dC    = C'_n - C_{n-1}
-//   dT    = half-transform(dC)                         (mode 0, per CSR row i)
+//   dT    = half-transform(dC)                         (k_half: persistent, per CSR row i)
 //   T_n   = T_{n-1} + dT,  S_T = T_n + T_{n-1}
-//   K_n   = K_{n-1} + sym(dT S_T^T)                    (mode 1, split-K)
+//   K_n   = K_{n-1} + sym(dT S_T^T)                    (k_gemm: split-K)
 // so that T_n T_n^T - T_{n-1} T_{n-1}^T is formed from dT: the low-precision
 // error of each increment scales with |dC| ~ |dD| and vanishes as the SCF
 // converges. K_n is accumulated in FP64.
 //
-// Warp roles (192 threads): warp 0 issues TMA loads, warp 1 allocates tensor
-// memory and issues the MMAs, warps 2-5 drain the accumulator (each warp reads
-// the TMEM lane quadrant warp_id % 4). All mbarrier waits are bounded; a
-// timeout sets an error flag instead of hanging.
+// Warp roles (320 threads): warp 0 issues TMA loads, warp 1 allocates tensor
+// memory and issues the MMAs, warps 2-9 drain the accumulators (two warps per
+// TMEM lane quadrant warp_id % 4, each taking half of the columns). All
+// mbarrier waits are bounded; a timeout sets an error flag instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cstdio>
