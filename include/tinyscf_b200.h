@@ -161,6 +161,11 @@ TINYSCF_API int TinySCF_guess_used(TinySCF_t t);
  * pairs and returns the count (negative status on error). */
 TINYSCF_API long long TinySCF_guess_dataset(TinySCF_t t, const double *D, float *feat, float *target, int *type,
                                             long long cap);
+/* The basis rotation the learned guess uses for one atom (no GPU needed):
+ * with molecule coordinates x_m = Q^T x_l (Q: 3 x 3 row-major, rows the local
+ * axes), writes M (nf x nf row-major, nf = sum of Cartesian components of the
+ * shells, s/p/d only) such that the atom's functions obey phi_m = M phi_l. */
+TINYSCF_API int TinySCF_guess_rotation(const int *shell_am, int nshells, const double *Q, double *M);
 /* Train the five block-type MLPs (128-192-192-out, SiLU) with Adam on the GPU
  * from host arrays as TinySCF_guess_dataset writes them and save the weights
  * file at path; final_loss (5 floats) receives each type's last-epoch MSE in

@@ -1632,6 +1632,19 @@ long long TinySCF_guess_dataset(TinySCF_t t, const double *D, float *feat, float
     return (long long) pairs.size();
 }
 
+int TinySCF_guess_rotation(const int *shell_am, int nshells, const double *Q, double *M)
+{
+    if (!shell_am || !Q || !M || nshells <= 0) return TINYSCF_ERR_INPUT;
+    std::vector<int> am(shell_am, shell_am + nshells);
+    int nf = 0;
+    for (int l : am) {
+        if (l < 0 || l > 2) return TINYSCF_ERR_UNSUPPORTED;
+        nf += (l + 1) * (l + 2) / 2;
+    }
+    guess_atom_rotation(am, Q, M, nf);
+    return TINYSCF_OK;
+}
+
 int TinySCF_guess_train(const float *feat, const float *target, const int *type, long long n, int epochs, int batch,
                         float lr, unsigned seed, const char *path, float *final_loss)
 {

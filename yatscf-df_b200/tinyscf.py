@@ -121,6 +121,7 @@ def load_library(path=LIBPATH):
         "TinySCF_guess_train": ([fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ip, ip, ctypes.c_float,
                                  ctypes.c_uint, ctypes.c_char_p, fp], ip),
         "TinySCF_guess_mlp_grad": ([ip, ip, ip, fp, fp, fp, ip, fp, fp], ip),
+        "TinySCF_guess_rotation": ([ctypes.POINTER(ctypes.c_int), ip, dp, dp], ip),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -437,3 +438,16 @@ def device_memory(device=0):
     if rc:
         raise TinySCFError("device_memory: " + STATUS.get(rc, str(rc)))
     return f.value, t.value
+
+
+def guess_rotation(shell_am, Q):
+    """M with phi_molecule = M phi_local for one atom's Cartesian shells (x_m = Q^T x_l)."""
+    lib = load_library()
+    am = np.ascontiguousarray(shell_am, dtype=np.int32)
+    Q = np.ascontiguousarray(Q, dtype=np.float64)
+    nf = int(sum((l + 1) * (l + 2) // 2 for l in am))
+    M = np.zeros((nf, nf))
+    rc = lib.TinySCF_guess_rotation(am.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(am), _dptr(Q), _dptr(M))
+    if rc:
+        raise TinySCFError("guess_rotation: " + STATUS.get(rc, str(rc)))
+    return M
