@@ -109,8 +109,9 @@ TINYSCF_API int TinySCF_build_J_noalloc(const double *B, int naux, const int *up
 /* Precision of the exchange build. TINYSCF_K_FP64 (default): FP64 on the CUDA
  * cores, the reference's arithmetic. TINYSCF_K_MIXED: incremental builds from
  * the change of the occupied orbitals on the tcgen05 tensor cores (split-BF16
- * operands, FP32 accumulation, FP64 K), then one FP64 Fock build at
- * convergence whose energy is the result. In mixed mode each Fock build
+ * operands, FP32 accumulation, FP64 K), J of the iterations from an FP32 copy
+ * of the DF tensor (FP64 arithmetic), then one FP64 Fock build at convergence
+ * whose energy is the result. In mixed mode each Fock build
  * updates K from the previous build's orbitals; TinySCF_reset_scf restarts. */
 #define TINYSCF_K_FP64  0
 #define TINYSCF_K_MIXED 1

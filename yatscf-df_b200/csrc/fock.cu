@@ -27,12 +27,13 @@ __global__ void k_j_weights(const int *up_i, const int *up_j, const double *D, d
 
 // Each block streams a contiguous range of upper rows and keeps its partial
 // t(P) for every column in registers (jt_rows).
-__global__ void __launch_bounds__(JT_THREADS) k_j_tpart(const double *__restrict__ B, const int *__restrict__ up_u,
+template <typename BT>
+__global__ void __launch_bounds__(JT_THREADS) k_j_tpart(const BT *__restrict__ B, const int *__restrict__ up_u,
                                                         const double *__restrict__ w, int nup, int naux, int rows_per_blk,
                                                         double *__restrict__ part)
 {
     const int r0 = blockIdx.x * rows_per_blk, r1 = min(nup, r0 + rows_per_blk);
-    jt_rows(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
+    jt_rows<BT>(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
 }
 
 __global__ void k_j_treduce(const double *part, int nblk, int naux, double *t)
@@ -44,7 +45,8 @@ __global__ void k_j_treduce(const double *part, int nblk, int naux, double *t)
     t[p] = s;
 }
 
-__global__ void __launch_bounds__(256) k_j_rows(const double *__restrict__ B, const int *up_i, const int *up_j,
+template <typename BT>
+__global__ void __launch_bounds__(256) k_j_rows(const BT *__restrict__ B, const int *up_i, const int *up_j,
                                                 const int *up_u, const double *__restrict__ t, int nup, int naux,
                                                 int nbf, double *J)
 {
@@ -54,9 +56,9 @@ __global__ void __launch_bounds__(256) k_j_rows(const double *__restrict__ B, co
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;
     for (int k = blockIdx.x * nw + wid; k < nup; k += gridDim.x * nw) {
-        const double *row = B + (size_t) up_u[k] * naux;
+        const BT *row = B + (size_t) up_u[k] * naux;
         double s = 0.0;
-        for (int p = lane; p < naux; p += 32) s = fma(__ldg(row + p), ts[p], s);
+        for (int p = lane; p < naux; p += 32) s = fma((double) __ldg(row + p), ts[p], s);
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffff, s, o);
         if (lane == 0) {
             int i = up_i[k], j = up_j[k];
@@ -73,16 +75,41 @@ int build_J_part_blocks(const FockPlan &p)
     return nb;
 }
 
-void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, double *d_part, int nblk, double *d_w,
-             cudaStream_t s)
+template <typename BT>
+static void build_J_t(const FockPlan &p, const BT *B, const double *d_D, double *d_J, double *d_t, double *d_part,
+                      int nblk, double *d_w, cudaStream_t s)
 {
     g_launches += 4;
     k_j_weights<<<(p.nup + 255) / 256, 256, 0, s>>>(p.up_i, p.up_j, d_D, d_w, p.nup, p.nbf);
     int rows_per_blk = (p.nup + nblk - 1) / nblk;
-    k_j_tpart<<<nblk, JT_THREADS, 0, s>>>(p.B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
+    k_j_tpart<BT><<<nblk, JT_THREADS, 0, s>>>(B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
     k_j_treduce<<<(p.naux + 255) / 256, 256, 0, s>>>(d_part, nblk, p.naux, d_t);
     int blocks = 148 * 4;
-    k_j_rows<<<blocks, 256, sizeof(double) * p.naux, s>>>(p.B, p.up_i, p.up_j, p.up_u, d_t, p.nup, p.naux, p.nbf, d_J);
+    k_j_rows<BT><<<blocks, 256, sizeof(double) * p.naux, s>>>(B, p.up_i, p.up_j, p.up_u, d_t, p.nup, p.naux, p.nbf, d_J);
+}
+
+void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, double *d_part, int nblk, double *d_w,
+             cudaStream_t s)
+{
+    build_J_t<double>(p, p.B, d_D, d_J, d_t, d_part, nblk, d_w, s);
+}
+
+void build_J_f32(const FockPlan &p, const float *B32, const double *d_D, double *d_J, double *d_t, double *d_part,
+                 int nblk, double *d_w, cudaStream_t s)
+{
+    build_J_t<float>(p, B32, d_D, d_J, d_t, d_part, nblk, d_w, s);
+}
+
+__global__ void k_to_f32(const double *in, float *out, size_t n)
+{
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+        out[i] = (float) in[i];
+}
+
+void convert_f32(const double *in, float *out, size_t n, cudaStream_t s)
+{
+    g_launches++;
+    k_to_f32<<<148 * 8, 256, 0, s>>>(in, out, n);
 }
 
 // ------------------------------------------------------------------ K, FP64

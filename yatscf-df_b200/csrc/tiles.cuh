@@ -599,7 +599,9 @@ __device__ __forceinline__ void half_tile_dmma(const double *__restrict__ B, con
 // Thread x owns columns x, x + 512, ... (naux <= 8192).
 constexpr int JT_THREADS = 512, JT_COLS = 16;
 
-__device__ __forceinline__ void jt_rows(const double *__restrict__ B, const int *__restrict__ up_u,
+// BT = double, or float for the FP32 copy of the DF tensor (products and sums stay FP64)
+template <typename BT = double>
+__device__ __forceinline__ void jt_rows(const BT *__restrict__ B, const int *__restrict__ up_u,
                                         const double *__restrict__ w, int naux, int r0, int r1,
                                         double *__restrict__ part_row)
 {
@@ -608,11 +610,11 @@ __device__ __forceinline__ void jt_rows(const double *__restrict__ B, const int 
     for (int c = 0; c < JT_COLS; c++) acc[c] = 0.0;
     for (int r = r0; r < r1; r++) {
         const double wr = w[r];
-        const double *row = B + (size_t) up_u[r] * naux;
+        const BT *row = B + (size_t) up_u[r] * naux;
 #pragma unroll
         for (int c = 0; c < JT_COLS; c++) {
             int p = threadIdx.x + c * JT_THREADS;
-            if (p < naux) acc[c] = fma(wr, __ldg(row + p), acc[c]);
+            if (p < naux) acc[c] = fma(wr, (double) __ldg(row + p), acc[c]);
         }
     }
 #pragma unroll

@@ -320,6 +320,7 @@ struct Engine {
     GuessNet *gnet = nullptr;
     KMix *kmix = nullptr;
     double *Kmix = nullptr;
+    float *B32 = nullptr;         // FP32 copy of the DF tensor for the mixed form's J
     int stage = 0;            // 1 hcore, 2 schwarz, 3 sparsity, 4 guess, 5 df
     bool F_is_orth = false;   // which buffer currently plays the reference's F_mat
     std::vector<void *> allocs;
@@ -1047,7 +1048,10 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
     FockPlan p = e->plan();
     p.nocc = t->n_occ;
     tstart(e, TINYSCF_T_J);
-    build_J(p, e->D, e->J, e->Jt, e->Jpart, e->jblk, e->Jw, e->s);
+    if (e->kprec == TINYSCF_K_MIXED && !force_fp64 && e->B32)
+        build_J_f32(p, e->B32, e->D, e->J, e->Jt, e->Jpart, e->jblk, e->Jw, e->s);
+    else
+        build_J(p, e->D, e->J, e->Jt, e->Jpart, e->jblk, e->Jw, e->s);
     tstop(e, TINYSCF_T_J);
     const double *Kuse = e->K;
     if (e->kprec == TINYSCF_K_MIXED && !force_fp64) {
@@ -1542,6 +1546,9 @@ int TinySCF_set_k_precision(TinySCF_t t, int mode)
             if (rc) return rc;
             rc = dalloc(e, &e->Kmix, e->nn);
             if (rc) return rc;
+            rc = dalloc(e, &e->B32, (size_t) e->nu * t->df_nbf);
+            if (rc) return rc;
+            convert_f32(e->B, e->B32, (size_t) e->nu * t->df_nbf, e->s);
         }
         kmix_reset(e->kmix, e->s);
         if (sync_rc(e, "mixed K set-up")) return TINYSCF_ERR_CUDA;

@@ -137,6 +137,11 @@ struct FockPlan {
 void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, double *d_part, int part_blocks,
              double *d_w, cudaStream_t s);
 int  build_J_part_blocks(const FockPlan &p);
+// J from an FP32 copy of the DF tensor (FP64 products and sums): half the HBM
+// traffic, ~1e-7 relative error; the mixed-precision form's iterations use it
+void build_J_f32(const FockPlan &p, const float *B32, const double *d_D, double *d_J, double *d_t, double *d_part,
+                 int part_blocks, double *d_w, cudaStream_t s);
+void convert_f32(const double *in, float *out, size_t n, cudaStream_t s);
 // K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
 // wide = 1: 64 x 256 FFMA tiles (k_halftransform_wide), 2: 64 x 256 DMMA tiles
 // (k_halftransform_dmma), 0: 64 x 64 FFMA tiles
