@@ -160,3 +160,41 @@ def test_full_size_properties(name):
     assert np.abs(F @ D @ S - S @ D @ F).max() < 1e-4
     assert e.s.iter < 40
     e.free()
+
+
+SMALL = {
+    "h2": "2\n0\nH 0.0 0.0 0.0\nH 0.0 0.0 0.74\n",
+    "n2": "2\n0\nN 0.0 0.0 0.0\nN 0.0 0.0 1.10\n",
+    "hcn": "3\n0\nH 0.0 0.0 -1.066\nC 0.0 0.0 0.0\nN 0.0 0.0 1.156\n",
+    "nh4+": "5\n1\nN 0.0 0.0 0.0\nH 0.59 0.59 0.59\nH -0.59 -0.59 0.59\nH -0.59 0.59 -0.59\nH 0.59 -0.59 -0.59\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_small_molecules_against_restatement(tmp_path, name):
+    """Edge cases of the input side against the numpy restatement of the
+    reference: a two-function-per-atom minimum (H2), nitrogen (no other test
+    has it), a linear molecule whose local frames have no off-axis atom (HCN),
+    and a cation (NH4+, charge-scaled SAD). Both the reference-algorithm form
+    and the accelerated form (learned guess where covered, tensor-core K,
+    refinement, CUDA graph) reach the restatement's energy."""
+    mol = tmp_path / (name + ".xyz")
+    mol.write_text(SMALL[name])
+    o = oracle.OracleSCF(BAS, DFBAS, str(mol), 60)
+    o.setup()
+    Eo = o.do_SCF()
+    e = tinyscf.TinySCF(BAS, DFBAS, str(mol), 60)
+    e.setup()
+    e.do_SCF()
+    assert abs(e.energy - Eo[-1]) < 1e-8, (e.energy, Eo[-1])
+    assert e.s.iter == len(Eo)
+    e.free()
+    f = tinyscf.TinySCF(BAS, DFBAS, str(mol), 60)
+    f.setup(guess=tinyscf.GUESS_LEARNED)
+    f.set_k_precision(tinyscf.K_MIXED)
+    f.set_density_solver(tinyscf.DENSITY_REFINE)
+    f.set_graph(True)
+    f.s.ene_tol = 1e-10
+    f.do_SCF()
+    assert abs(f.energy - Eo[-1]) < 1e-8, (f.energy, Eo[-1])
+    f.free()

@@ -85,7 +85,9 @@ static void build_J_t(const FockPlan &p, const BT *B, const double *d_D, double 
     k_j_tpart<BT><<<nblk, JT_THREADS, 0, s>>>(B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
     k_j_treduce<<<(p.naux + 255) / 256, 256, 0, s>>>(d_part, nblk, p.naux, d_t);
     int blocks = 148 * 4;
-    k_j_rows<BT><<<blocks, 256, sizeof(double) * p.naux, s>>>(B, p.up_i, p.up_j, p.up_u, d_t, p.nup, p.naux, p.nbf, d_J);
+    const size_t shm = sizeof(double) * p.naux;   // t(P) staged in shared memory
+    if (shm > 48 * 1024) cudaFuncSetAttribute(k_j_rows<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
+    k_j_rows<BT><<<blocks, 256, shm, s>>>(B, p.up_i, p.up_j, p.up_u, d_t, p.nup, p.naux, p.nbf, d_J);
 }
 
 void build_J(const FockPlan &p, const double *d_D, double *d_J, double *d_t, double *d_part, int nblk, double *d_w,

@@ -501,6 +501,10 @@ int init_impl(TinySCF_t t, const char *bas_fname, const char *df_bas_fname, cons
         fprintf(stderr, "[tinyscf] shells beyond d (orbital) / f (auxiliary) are not supported\n");
         return ERR_UNSUPPORTED;
     }
+    if (e->ash.nbf > 8192) {   // the J kernels keep one column group of 16 x 512 aux functions per thread block
+        fprintf(stderr, "[tinyscf] %d auxiliary functions: at most 8192 are supported\n", e->ash.nbf);
+        return ERR_UNSUPPORTED;
+    }
     const int nbf = e->sh.nbf, naux = e->ash.nbf;
     t->natoms = e->mol.natoms;
     t->nshells = e->sh.nsh;
