@@ -207,6 +207,23 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def reduce_max(v, dist):
+    """Max of a per-rank float over all ranks (identity without a process
+    group): device time of a multi-GPU run is the slowest rank's."""
+    if dist is None:
+        return v
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard(items, rank, world):
+    """Round-robin share of a rank (the replicas / waters256 work split)."""
+    return list(items)[rank::world]
+
+
 def run_ours(args, rank, world, local_rank):
     sys.path.insert(0, PKG)
     import tinyscf                                  # the engine's library first (CUDA libraries)
@@ -224,12 +241,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     def allmax(v):
-        if dist is None:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, dist)
 
     xyz = os.path.join(DATA, args.config + ".xyz")
     t0 = time.perf_counter()
@@ -431,7 +443,7 @@ def run_batch(args, rank, world, local_rank):
     import tinyscf
     tinyscf.load_library()
     tinyscf.set_autotune(False)            # many distinct sizes: keep the set-up short
-    seeds = list(range(256))[rank::world]
+    seeds = shard(range(256), rank, world)
     td = tempfile.mkdtemp()
     paths = water_cluster_files(td, seeds)
     sizes = []
@@ -505,10 +517,8 @@ def run_batch(args, rank, world, local_rank):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl")
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        total = reduce_max(total, dist)
         dist.destroy_process_group()
     if rank == 0:
         line = {
