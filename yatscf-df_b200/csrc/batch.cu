@@ -36,13 +36,15 @@ __device__ __forceinline__ int find_mol(const int *start, int nmol, int g)
     if (!active[mol]) return;
 
 // ---- J
-__global__ void __launch_bounds__(JT_THREADS) kb_j_tpart(const MolDev *mols, const int *active, WorkList wl)
+__global__ void __launch_bounds__(JT_THREADS) kb_j_tpart(const MolDev *mols, const int *active, WorkList wl,
+                                                         int use32)
 {
     BATCH_ITEM(wl)
     const int nblk = wl.start[mol + 1] - wl.start[mol];
     const int rows = (m.nup + nblk - 1) / nblk;
     const int r0 = li * rows, r1 = min(m.nup, r0 + rows);
-    jt_rows(m.B, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
+    if (use32 && m.B32) jt_rows<float>(m.B32, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
+    else jt_rows<double>(m.B, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
 }
 
 __global__ void kb_j_weights(const MolDev *mols, const int *active, WorkList wl)
@@ -65,7 +67,15 @@ __global__ void kb_j_treduce(const MolDev *mols, const int *active, WorkList wl)
 }
 
 // 8 warps, 8 upper pairs per warp per item
-__global__ void __launch_bounds__(256) kb_j_rows(const MolDev *mols, const int *active, WorkList wl)
+template <typename BT>
+__device__ __forceinline__ double row_dot(const BT *__restrict__ row, const double *ts, int naux, int lane)
+{
+    double s = 0.0;
+    for (int p = lane; p < naux; p += 32) s = fma((double) __ldg(row + p), ts[p], s);
+    return s;
+}
+
+__global__ void __launch_bounds__(256) kb_j_rows(const MolDev *mols, const int *active, WorkList wl, int use32)
 {
     BATCH_ITEM(wl)
     extern __shared__ double ts[];
@@ -75,9 +85,8 @@ __global__ void __launch_bounds__(256) kb_j_rows(const MolDev *mols, const int *
     for (int q = 0; q < 8; q++) {
         const int k = li * 64 + wid * 8 + q;
         if (k >= m.nup) break;
-        const double *row = m.B + (size_t) m.up_u[k] * m.naux;
-        double s = 0.0;
-        for (int p = lane; p < m.naux; p += 32) s = fma(__ldg(row + p), ts[p], s);
+        double s = (use32 && m.B32) ? row_dot<float>(m.B32 + (size_t) m.up_u[k] * m.naux, ts, m.naux, lane)
+                                    : row_dot<double>(m.B + (size_t) m.up_u[k] * m.naux, ts, m.naux, lane);
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffff, s, o);
         if (lane == 0) {
             const int i = m.up_i[k], j = m.up_j[k];
@@ -283,14 +292,14 @@ __global__ void kb_copy_fp(const MolDev *mols, const int *active, WorkList wl)
 
 void diis_solve_batched(const MolDev *d_mols, const int *d_active, int nmol, cudaStream_t s);
 
-void batch_j(const BatchPlan &b, cudaStream_t s)
+void batch_j(const BatchPlan &b, cudaStream_t s, int use32)
 {
     const size_t shm = sizeof(double) * b.naux_max;
     if (shm > 48 * 1024) cudaFuncSetAttribute(kb_j_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
     kb_j_weights<<<b.nup256.total, 256, 0, s>>>(b.mols, b.active, b.nup256);
-    kb_j_tpart<<<b.jblk.total, JT_THREADS, 0, s>>>(b.mols, b.active, b.jblk);
+    kb_j_tpart<<<b.jblk.total, JT_THREADS, 0, s>>>(b.mols, b.active, b.jblk, use32);
     kb_j_treduce<<<b.naux256.total, 256, 0, s>>>(b.mols, b.active, b.naux256);
-    kb_j_rows<<<b.nup64.total, 256, sizeof(double) * b.naux_max, s>>>(b.mols, b.active, b.nup64);
+    kb_j_rows<<<b.nup64.total, 256, sizeof(double) * b.naux_max, s>>>(b.mols, b.active, b.nup64, use32);
     g_launches += 4;
 }
 

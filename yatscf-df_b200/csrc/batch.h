@@ -10,6 +10,7 @@ struct MolDev {
     const int *up_i, *up_j, *up_u, *csr_j, *csr_u, *displs;
     const int2 *tiles;   // upper tile pairs for ktile
     const double *B, *H, *S, *X;
+    const float *B32;   // FP32 copy of B for the mixed-precision molecules' J (null otherwise)
     double *D, *J, *K, *F, *Fp, *Cocc, *T, *Kpart, *Jt, *Jpart, *Jw, *epart, *E, *tmp, *tmp2, *F0, *R, *eigA;
     DiisState *diis;
 };
@@ -44,7 +45,9 @@ struct BatchPlan {
     BatchGemm g_xtf, g_tx_fp, g_fd, g_fds, g_xtt, g_t2x, g_tx_t2, g_cocc, g_dens;
 };
 
-void batch_j(const BatchPlan &b, cudaStream_t s);
+// use32: the molecules that have an FP32 copy of B read it (the iterations of
+// the mixed-precision form); 0 for the FP64 J of their final build
+void batch_j(const BatchPlan &b, cudaStream_t s, int use32 = 1);
 // kact: per-molecule flags of the molecules whose exchange is built here (FP64)
 void batch_k(const BatchPlan &b, const int *kact, cudaStream_t s);
 void batch_fock(const BatchPlan &b, double *d_Eall, cudaStream_t s);

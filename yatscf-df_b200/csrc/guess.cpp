@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "guess.h"
 
@@ -17,6 +18,7 @@ const int G_NFB[G_NTYPES] = {15, 5, 15, 5, 5};
 namespace {
 
 const double BOHR2A = 0.52917720859;
+const int kGuessThreads = 8;   // host threads that build the pair features of a large molecule
 
 // one-hot slot of the covered elements (0-based element index: H 0, C 5, N 6, O 7)
 int elem_slot(int eid)
@@ -57,23 +59,18 @@ bool unit(double *a)
 
 // Frame with e_z = z (unit) and e_x towards the first candidate point whose
 // distance from the z axis through `origin` exceeds 0.25 A (Bohr inputs).
-void make_frame(const double *origin, const double *z, const std::vector<const double *> &cands, double *Q)
+// Frame with e_z = z (unit) and e_x towards the point x_atom projected off
+// the z axis through `origin`; with no such point (x_atom null) any
+// perpendicular (the block is then symmetric about z).
+void make_frame(const double *origin, const double *z, const double *x_atom, double *Q)
 {
     double ex[3] = {0, 0, 0};
-    bool ok = false;
-    for (const double *c : cands) {
-        double v[3];
-        sub(c, origin, v);
-        double t = dot(v, z);
-        for (int k = 0; k < 3; k++) v[k] -= t * z[k];
-        if (std::sqrt(dot(v, v)) * BOHR2A > 0.25) {
-            for (int k = 0; k < 3; k++) ex[k] = v[k];
-            ok = unit(ex);
-            if (ok) break;
-        }
-    }
-    if (!ok) {
-        // no off-axis neighbour: any perpendicular (the block is then symmetric about z)
+    if (x_atom) {
+        sub(x_atom, origin, ex);
+        double t = dot(ex, z);
+        for (int k = 0; k < 3; k++) ex[k] -= t * z[k];
+        unit(ex);
+    } else {
         int m = 0;
         for (int k = 1; k < 3; k++)
             if (std::fabs(z[k]) < std::fabs(z[m])) m = k;
@@ -97,9 +94,34 @@ void make_frame(const double *origin, const double *z, const std::vector<const d
 // for every orientation of the molecule.
 std::pair<long long, int> dkey(double r_angstrom, int idx) { return {std::llround(r_angstrom * 1e4), idx}; }
 
+// The atom that fixes e_x: among all atoms but skip0..skip2, the one with the
+// smallest key (distance from `origin`, then index) whose distance from the
+// z axis through `origin` exceeds 0.25 A; -1 when there is none. One pass
+// over the atoms instead of sorting them.
+int x_atom(const GuessAtoms &g, const double *origin, const double *z, int skip0, int skip1, int skip2)
+{
+    int best = -1;
+    std::pair<long long, int> bkey;
+    for (int c = 0; c < g.natoms; c++) {
+        if (c == skip0 || c == skip1 || c == skip2) continue;
+        double v[3];
+        sub(g.xyz + 3 * c, origin, v);
+        const std::pair<long long, int> key = dkey(std::sqrt(dot(v, v)) * BOHR2A, c);
+        if (best >= 0 && !(key < bkey)) continue;
+        const double t = dot(v, z);
+        for (int k = 0; k < 3; k++) v[k] -= t * z[k];
+        if (std::sqrt(dot(v, v)) * BOHR2A > 0.25) {
+            best = c;
+            bkey = key;
+        }
+    }
+    return best;
+}
+
 double cutoff_fn(double r, double rc) { return r >= rc ? 0.0 : 0.5 * (std::cos(M_PI * r / rc) + 1.0); }
 
-void features(const GuessAtoms &g, int a, int b, const double *origin, const double *Q, float *f)
+void features(const GuessAtoms &g, int a, int b, const double *origin, const double *Q, float *f,
+              std::vector<std::pair<long long, int>> &env)
 {
     std::memset(f, 0, sizeof(float) * G_DIN);
     f[elem_slot(g.eid[a])] = 1.0f;
@@ -115,7 +137,7 @@ void features(const GuessAtoms &g, int a, int b, const double *origin, const dou
         }
     }
     // environment: nearest other atoms to the origin within kEnvCut, in the local frame
-    std::vector<std::pair<long long, int>> env;
+    env.clear();
     for (int c = 0; c < g.natoms; c++) {
         if (c == a || c == b) continue;
         double v[3];
@@ -123,8 +145,8 @@ void features(const GuessAtoms &g, int a, int b, const double *origin, const dou
         double r = std::sqrt(dot(v, v)) * BOHR2A;
         if (r < kEnvCut) env.push_back(dkey(r, c));
     }
-    std::sort(env.begin(), env.end());
     const int ne = std::min((int) env.size(), G_NENV);
+    std::partial_sort(env.begin(), env.begin() + ne, env.end());
     for (int k = 0; k < ne; k++) {
         const int c = env[k].second;
         double v[3];
@@ -138,82 +160,98 @@ void features(const GuessAtoms &g, int a, int b, const double *origin, const dou
     }
 }
 
+// Frame and features of block (a, b): a == b is a diagonal block (origin at
+// the atom, z to the nearest neighbour, x to the next off-axis one); a != b
+// is off-diagonal (origin at the midpoint, z from a to b).
+void fill_pair(const GuessAtoms &g, const std::vector<int> &nf, int a, int b, GuessPair &p,
+               std::vector<std::pair<long long, int>> &env)
+{
+    p.a = a;
+    p.b = b;
+    p.off_a = g.bf0[a];
+    p.off_b = g.bf0[b];
+    p.nf_a = nf[a];
+    p.nf_b = nf[b];
+    if (a == b) {
+        p.type = nf[a] == 15 ? 0 : 1;
+        int near = -1;
+        std::pair<long long, int> nkey;
+        for (int c = 0; c < g.natoms; c++)
+            if (c != a) {
+                double v[3];
+                sub(g.xyz + 3 * c, g.xyz + 3 * a, v);
+                const std::pair<long long, int> key = dkey(std::sqrt(dot(v, v)) * BOHR2A, c);
+                if (near < 0 || key < nkey) {
+                    near = c;
+                    nkey = key;
+                }
+            }
+        if (near < 0) {
+            const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+            std::memcpy(p.Qf, I, sizeof(I));
+        } else {
+            double z[3];
+            sub(g.xyz + 3 * near, g.xyz + 3 * a, z);
+            unit(z);
+            const int x = x_atom(g, g.xyz + 3 * a, z, a, near, -1);
+            make_frame(g.xyz + 3 * a, z, x >= 0 ? g.xyz + 3 * x : nullptr, p.Qf);
+        }
+        features(g, a, a, g.xyz + 3 * a, p.Qf, p.feat, env);
+        return;
+    }
+    p.type = (nf[a] == 15 && nf[b] == 15) ? 2 : (nf[a] == 15 ? 3 : 4);
+    double mid[3], z[3];
+    for (int k = 0; k < 3; k++) mid[k] = 0.5 * (g.xyz[3 * a + k] + g.xyz[3 * b + k]);
+    sub(g.xyz + 3 * b, g.xyz + 3 * a, z);
+    unit(z);
+    const int x = x_atom(g, mid, z, a, b, -1);
+    make_frame(mid, z, x >= 0 ? g.xyz + 3 * x : nullptr, p.Qf);
+    features(g, a, b, mid, p.Qf, p.feat, env);
+}
+
 }  // namespace
 
 int guess_pairs(const GuessAtoms &g, std::vector<GuessPair> &out)
 {
     out.clear();
     const int na = g.natoms;
-    std::vector<int> kind(na);
     std::vector<int> nf(na);
     for (int a = 0; a < na; a++) {
-        kind[a] = layout_kind(g.shell_am[a]);
-        if (kind[a] < 0 || elem_slot(g.eid[a]) < 0) return 1;
-        nf[a] = kind[a] ? 15 : 5;
+        const int kind = layout_kind(g.shell_am[a]);
+        if (kind < 0 || elem_slot(g.eid[a]) < 0) return 1;
+        nf[a] = kind ? 15 : 5;
     }
+    // blocks in output order: the diagonal ones, then pairs i < j closer than
+    // kPairCut with the atom of more functions first
+    std::vector<std::pair<int, int>> ab;
+    for (int a = 0; a < na; a++) ab.emplace_back(a, a);
     const double cut = kPairCut / BOHR2A;
-    for (int a = 0; a < na; a++) {
-        // diagonal block: origin at the atom, z to the nearest neighbour, x to the next off-axis one
-        std::vector<std::pair<long long, int>> nb;
-        for (int c = 0; c < na; c++)
-            if (c != a) {
-                double v[3];
-                sub(g.xyz + 3 * c, g.xyz + 3 * a, v);
-                nb.push_back(dkey(std::sqrt(dot(v, v)) * BOHR2A, c));
-            }
-        std::sort(nb.begin(), nb.end());
-        GuessPair p;
-        p.a = p.b = a;
-        p.type = kind[a] ? 0 : 1;
-        p.off_a = p.off_b = g.bf0[a];
-        p.nf_a = p.nf_b = nf[a];
-        if (nb.empty()) {
-            const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-            std::memcpy(p.Qf, I, sizeof(I));
-        } else {
-            double z[3];
-            sub(g.xyz + 3 * nb[0].second, g.xyz + 3 * a, z);
-            unit(z);
-            std::vector<const double *> cands;
-            for (size_t k = 1; k < nb.size(); k++) cands.push_back(g.xyz + 3 * nb[k].second);
-            make_frame(g.xyz + 3 * a, z, cands, p.Qf);
-        }
-        features(g, a, a, g.xyz + 3 * a, p.Qf, p.feat);
-        out.push_back(p);
-    }
     for (int i = 0; i < na; i++)
         for (int j = i + 1; j < na; j++) {
             double v[3];
             sub(g.xyz + 3 * j, g.xyz + 3 * i, v);
             if (std::sqrt(dot(v, v)) >= cut) continue;
-            int a = i, b = j;
-            if (nf[b] > nf[a]) std::swap(a, b);
-            GuessPair p;
-            p.a = a;
-            p.b = b;
-            p.type = (nf[a] == 15 && nf[b] == 15) ? 2 : (nf[a] == 15 ? 3 : 4);
-            p.off_a = g.bf0[a];
-            p.off_b = g.bf0[b];
-            p.nf_a = nf[a];
-            p.nf_b = nf[b];
-            double mid[3], z[3];
-            for (int k = 0; k < 3; k++) mid[k] = 0.5 * (g.xyz[3 * a + k] + g.xyz[3 * b + k]);
-            sub(g.xyz + 3 * b, g.xyz + 3 * a, z);
-            unit(z);
-            std::vector<std::pair<long long, int>> nb;
-            for (int c = 0; c < na; c++)
-                if (c != a && c != b) {
-                    double w[3];
-                    sub(g.xyz + 3 * c, mid, w);
-                    nb.push_back(dkey(std::sqrt(dot(w, w)) * BOHR2A, c));
-                }
-            std::sort(nb.begin(), nb.end());
-            std::vector<const double *> cands;
-            for (auto &q : nb) cands.push_back(g.xyz + 3 * q.second);
-            make_frame(mid, z, cands, p.Qf);
-            features(g, a, b, mid, p.Qf, p.feat);
-            out.push_back(p);
+            if (nf[j] > nf[i]) ab.emplace_back(j, i);
+            else ab.emplace_back(i, j);
         }
+    out.resize(ab.size());
+    // each block is independent: a few host threads share them (a block
+    // costs O(natoms), so small molecules stay on the calling thread)
+    const long long work = (long long) ab.size() * na;
+    const int hw = (int) std::max(1u, std::thread::hardware_concurrency());
+    const int nth = (int) std::min<long long>(std::min(hw, kGuessThreads), std::max(1LL, work / 16384));
+    auto run = [&](int t) {
+        std::vector<std::pair<long long, int>> env;
+        for (size_t k = t; k < ab.size(); k += nth) fill_pair(g, nf, ab[k].first, ab[k].second, out[k], env);
+    };
+    if (nth == 1) {
+        run(0);
+        return 0;
+    }
+    std::vector<std::thread> th;
+    for (int t = 1; t < nth; t++) th.emplace_back(run, t);
+    run(0);
+    for (std::thread &x : th) x.join();
     return 0;
 }
 

@@ -287,20 +287,41 @@ double read_loss(const MlpWork &w, cudaStream_t s)
 // transposed, to (b, a); diagonal blocks are symmetrised.
 struct PairDev {
     int type, row, off_a, off_b, nf_a, nf_b;
+    double Qt[9];   // transposed local frame: M(Qt) takes local functions to the molecule's
 };
 
+// Entry (r, c) of M(Q) for an atom with nf Cartesian functions, the same
+// products and sums as guess_atom_rotation (host), rounded the same way:
+// nf 5 is the shell layout s s p, nf 15 is s s s p p d.
+__device__ double rot_entry(const double *Q, int nf, int r, int c)
+{
+    const int ns = nf == 5 ? 2 : 3;   // leading s functions
+    if (r < ns || c < ns) return r == c ? 1.0 : 0.0;
+    const int np = nf == 5 ? 1 : 2;   // p shells
+    const int pr = (r - ns) / 3, pc = (c - ns) / 3;
+    if (pr < np || pc < np) {
+        if (pr != pc) return 0.0;
+        return Q[((c - ns) % 3) * 3 + (r - ns) % 3];
+    }
+    const int dr = r - ns - 3 * np, dc = c - ns - 3 * np;   // d shell: components xx xy xz yy yz zz
+    const int d0[6] = {0, 0, 0, 1, 1, 2}, d1[6] = {0, 1, 2, 1, 2, 2};
+    const int a = d0[dr], b = d1[dr], cc = d0[dc], dd = d1[dc];
+    double v = __dmul_rn(Q[cc * 3 + a], Q[dd * 3 + b]);
+    if (cc != dd) v = __dadd_rn(v, __dmul_rn(Q[dd * 3 + a], Q[cc * 3 + b]));
+    return v;
+}
+
 __global__ void k_assemble(const PairDev *pairs, const float *const *Y, const float *const *scale,
-                           const float *const *offset, const double *P, double *D, int nbf)
+                           const float *const *offset, double *D, int nbf)
 {
     __shared__ double L[G_MAXF * G_MAXF], T[G_MAXF * G_MAXF], Pa[G_MAXF * G_MAXF], Pb[G_MAXF * G_MAXF];
     const PairDev p = pairs[blockIdx.x];
     const int na = p.nf_a, nb = p.nf_b, nab = na * nb;
     const float *y = Y[p.type] + (size_t) p.row * nab;
     const float *sc = scale[p.type], *of = offset[p.type];
-    const double *Pg = P + (size_t) blockIdx.x * 2 * G_MAXF * G_MAXF;
     for (int i = threadIdx.x; i < nab; i += blockDim.x) L[i] = (double) y[i] * sc[i] + of[i];
-    for (int i = threadIdx.x; i < na * na; i += blockDim.x) Pa[i] = Pg[i];
-    for (int i = threadIdx.x; i < nb * nb; i += blockDim.x) Pb[i] = Pg[G_MAXF * G_MAXF + i];
+    for (int i = threadIdx.x; i < na * na; i += blockDim.x) Pa[i] = rot_entry(p.Qt, na, i / na, i % na);
+    for (int i = threadIdx.x; i < nb * nb; i += blockDim.x) Pb[i] = rot_entry(p.Qt, nb, i / nb, i % nb);
     __syncthreads();
     for (int i = threadIdx.x; i < nab; i += blockDim.x) {   // T = L Pb
         const int r = i / nb, c = i % nb;
@@ -372,7 +393,6 @@ struct GuessWork {
     int cap_pairs = 0, cap_rows = 0;
     float *dX = nullptr, *dY = nullptr;
     PairDev *dpd = nullptr;
-    double *dP = nullptr;
     const float **dptr = nullptr;   // [3][G_NTYPES]: Y, scale, offset of each type
     MlpWork w{};
     std::vector<void *> mem;
@@ -405,7 +425,6 @@ static int work_reserve(GuessNet *net, int np, int maxrows)
     if (!dal((void **) &gw->dX, sizeof(float) * (size_t) np * G_DIN) ||
         !dal((void **) &gw->dY, sizeof(float) * (size_t) np * G_MAXF * G_MAXF) ||
         !dal((void **) &gw->dpd, sizeof(PairDev) * np) ||
-        !dal((void **) &gw->dP, sizeof(double) * (size_t) np * 2 * G_MAXF * G_MAXF) ||
         !dal((void **) &gw->dptr, sizeof(float *) * 3 * G_NTYPES))
         return ERR_ALLOC;
     int rc = work_alloc(gw->w, net->din, net->hid, G_MAXF * G_MAXF, maxrows);
@@ -427,18 +446,20 @@ int guessnet_predict(GuessNet *net, const std::vector<GuessPair> &pairs, const G
     for (int t = 0; t < G_NTYPES; t++) yoff[t + 1] = yoff[t] + (size_t) cnt[t] * net->dout[t];
     std::vector<float> X((size_t) np * G_DIN);
     std::vector<PairDev> pd(np);
-    std::vector<double> P((size_t) np * 2 * G_MAXF * G_MAXF, 0.0);
     int fill[G_NTYPES] = {};
     for (int k = 0; k < np; k++) {
         const GuessPair &p = pairs[k];
         const int row = fill[p.type]++;
-        pd[k] = PairDev{p.type, row, p.off_a, p.off_b, p.nf_a, p.nf_b};
-        std::memcpy(&X[(size_t) (off[p.type] + row) * G_DIN], p.feat, sizeof(float) * G_DIN);
-        double Qt[9];
+        PairDev &q = pd[k];
+        q.type = p.type;
+        q.row = row;
+        q.off_a = p.off_a;
+        q.off_b = p.off_b;
+        q.nf_a = p.nf_a;
+        q.nf_b = p.nf_b;
         for (int i = 0; i < 3; i++)
-            for (int j = 0; j < 3; j++) Qt[i * 3 + j] = p.Qf[j * 3 + i];
-        guess_atom_rotation(g.shell_am[p.a], Qt, &P[(size_t) k * 2 * G_MAXF * G_MAXF], p.nf_a);
-        guess_atom_rotation(g.shell_am[p.b], Qt, &P[((size_t) k * 2 + 1) * G_MAXF * G_MAXF], p.nf_b);
+            for (int j = 0; j < 3; j++) q.Qt[i * 3 + j] = p.Qf[j * 3 + i];
+        std::memcpy(&X[(size_t) (off[p.type] + row) * G_DIN], p.feat, sizeof(float) * G_DIN);
     }
     int maxrows = 1;
     for (int t = 0; t < G_NTYPES; t++) maxrows = std::max(maxrows, cnt[t]);
@@ -448,7 +469,6 @@ int guessnet_predict(GuessNet *net, const std::vector<GuessPair> &pairs, const G
     cudaMemsetAsync(d_D, 0, sizeof(double) * (size_t) nbf * nbf, s);
     cudaMemcpyAsync(gw->dX, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(gw->dpd, pd.data(), sizeof(PairDev) * np, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(gw->dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice, s);
     const float *hp[3 * G_NTYPES];
     for (int t = 0; t < G_NTYPES; t++) {
         hp[t] = gw->dY + yoff[t];
@@ -464,8 +484,8 @@ int guessnet_predict(GuessNet *net, const std::vector<GuessPair> &pairs, const G
         cudaMemcpyAsync(gw->dY + yoff[t], gw->w.Y, sizeof(float) * (size_t) cnt[t] * net->dout[t],
                         cudaMemcpyDeviceToDevice, s);
     }
-    if (np > 0) k_assemble<<<np, 128, 0, s>>>(gw->dpd, gw->dptr, gw->dptr + G_NTYPES, gw->dptr + 2 * G_NTYPES, gw->dP,
-                                               d_D, nbf);
+    if (np > 0) k_assemble<<<np, 128, 0, s>>>(gw->dpd, gw->dptr, gw->dptr + G_NTYPES, gw->dptr + 2 * G_NTYPES, d_D,
+                                               nbf);
     g_launches++;
     // the host arrays above are staged by the copies: wait before they go out of scope
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ERR_CUDA;

@@ -38,6 +38,8 @@ const int ELEN = 50;
 // occupied-subspace refinement: residual bound (Eh) and step limit before a full eigensolve
 const double kRefineTol = 1e-9;
 const int kRefineSteps = 6;
+// subspace iterations that project the learned guess onto an idempotent density
+const int kGuessSubspaceIters = 6;
 const char *ETABLE[ELEN] = {"H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg", "Al",
                             "Si", "P",  "S",  "Cl", "Ar", "K",  "Ca", "Sc", "Ti", "V",  "Cr", "Mn", "Fe",
                             "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",
@@ -844,8 +846,9 @@ GuessAtoms guess_atoms(Engine *e)
 }
 
 // Predicted density blocks, then the idempotent density closest in the
-// orthogonal basis: the n_occ leading eigenvectors U of S^1/2 D S^1/2
-// (S^1/2 = S X), Cocc = X U^T, D = Cocc Cocc^T. Returns ERR_UNSUPPORTED when
+// orthogonal basis: the n_occ-dimensional dominant subspace U of S^1/2 D S^1/2
+// (S^1/2 = S X; subspace iteration for the learned guess, a full eigensolve
+// for projected SAD), Cocc = X U^T, D = Cocc Cocc^T. Returns ERR_UNSUPPORTED when
 // an atom is not covered by the network (the caller then uses SAD).
 int learned_guess(TinySCF_t t)
 {
@@ -867,8 +870,18 @@ int learned_guess(TinySCF_t t)
     dgemm(false, false, n, n, n, 1.0, e->S, n, e->X, n, 0.0, e->tmp, n, e->s);      // S^1/2
     dgemm(false, false, n, n, n, 1.0, e->tmp, n, e->D, n, 0.0, e->tmp2, n, e->s);
     dgemm(false, false, n, n, n, 1.0, e->tmp2, n, e->tmp, n, 0.0, e->F, n, e->s);   // S^1/2 D S^1/2
-    RC(eig_run(e->eig, e->F, e->w, e->V, e->s));
-    density_from_eig(e->X, e->V + (size_t) (n - o) * n, e->Cocc, e->D, n, o, e->s);
+    int prc = ERR_NUMERIC;
+    if (e->guess_mode == TINYSCF_GUESS_LEARNED) {
+        // the prediction is close to a rank-n_occ projector: a few subspace
+        // iterations find its occupied space at a fraction of an eigensolve
+        prc = dominant_subspace(e->eig, e->F, e->V, e->tmp, e->tmp2, n, o, kGuessSubspaceIters, e->s);
+        if (prc != OK && prc != ERR_NUMERIC) return prc;
+        if (prc == OK) density_from_rows(e->X, e->V, e->Cocc, e->D, n, o, e->s);
+    }
+    if (prc != OK) {   // projected SAD, or a Gram matrix that lost definiteness
+        RC(eig_run(e->eig, e->F, e->w, e->V, e->s));
+        density_from_eig(e->X, e->V + (size_t) (n - o) * n, e->Cocc, e->D, n, o, e->s);
+    }
     tstop(e, TINYSCF_T_GUESS);
     RC(cuda_rc("learned initial guess"));
     RC(sync_rc(e, "learned initial guess"));
@@ -1905,6 +1918,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         m.displs = e->csr_displs;
         m.tiles = e->ktile == 64 ? e->tiles : e->tiles128;
         m.B = e->B;
+        m.B32 = (e->kprec == TINYSCF_K_MIXED) ? e->B32 : nullptr;
         m.H = e->H;
         m.S = e->S;
         m.X = e->X;
@@ -2146,7 +2160,7 @@ int batch_scf_impl(TinySCF_batch_t b)
         TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_active, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
         TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_kact, act.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s));
         cudaEventRecord(b->pev[0], b->s);
-        batch_j(b->plan, b->s);
+        batch_j(b->plan, b->s, 0);
         batch_k(b->plan, b->d_kact, b->s);
         batch_fock(b->plan, b->d_Eall, b->s);
         cudaEventRecord(b->pev[1], b->s);

@@ -107,6 +107,14 @@ Eig *eig_create(int n, cudaStream_t s);
 void eig_destroy(Eig *e);
 int  eig_run(Eig *e, const double *d_A, double *d_w, double *d_V, cudaStream_t s);
 
+// Orthonormal rows U (o x n) spanning the dominant o-dimensional invariant
+// subspace of a symmetric M (n x n): iters products with M from a fixed
+// pseudo-random start, orthonormalised by Cholesky-QR every few products and
+// twice at the end; W (o x n) and G (o x o) are scratch. Uses e's cuSOLVER
+// handle. ERR_NUMERIC when a Cholesky factor or its inverse fails (the
+// caller then solves the eigenproblem instead).
+int dominant_subspace(Eig *e, const double *d_M, double *d_U, double *d_W, double *d_G, int n, int o, int iters,
+                      cudaStream_t s);
 // X = U diag(f(w)) U^T with f(w) = w^-1/2, U from eigenvectors in rows.
 void inv_sqrt_from_eig(const double *d_w, const double *d_V, double *d_X, double *d_tmp, int n, cudaStream_t s);
 
