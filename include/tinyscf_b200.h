@@ -183,8 +183,11 @@ TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *
  * device and the fastest kept for the process (and saved to / loaded from the
  * file named by TINYSCF_TUNE_FILE): the block size and thread order of each
  * 3-centre integral AM class, the tile shape of each FP64 GEMM shape
- * (FFMA 64x64, 32x32, 128x64, or 128x128 / 64x64 on the FP64 tensor cores), the tile
- * and split count of the FP64 exchange and the row blocks of the J first pass.
+ * (FFMA 64x64, 32x32, 128x64, or 128x128 / 64x64 / 32x32 with K split over
+ * the warps on the FP64 tensor cores), the tile and split count of the FP64
+ * exchange rank-k product, the exchange half-transform (FFMA 64x64 or 64x256,
+ * DMMA 64x256, or DMMA 64x256 in persistent CTAs with a cp.async pipeline)
+ * and the row blocks of the J first pass.
  * All candidates compute the same values (the FP64 tensor-core tiles up to
  * rounding in the last bits). */
 TINYSCF_API int TinySCF_set_autotune(int on);

@@ -34,3 +34,117 @@ def test_tuned_engine_matches_untuned():
     rep = tinyscf.autotune_report()
     for key in ("3c:", "dgemm:", "ksyrk:", "khalf:", "jrows:"):
         assert key in rep, rep
+
+
+_PINNED = r"""
+import sys
+import numpy as np
+import tinyscf
+from conftest import BAS, DFBAS
+e = tinyscf.TinySCF(BAS, DFBAS, sys.argv[2], 60)
+e.setup()
+e.s.iter = 0
+e.build_FockMat()
+np.save(sys.argv[1], e.mat("K_mat"))
+e.free()
+print(tinyscf.autotune_report())
+"""
+
+
+@pytest.mark.parametrize("name", ["c10h22", "hcn"])
+def test_pinned_half_transform_variants_match(tmp_path, name):
+    """Each exchange half-transform variant (64x64 FFMA, 64x256 FFMA, 64x256
+    DMMA, pipelined persistent DMMA), pinned through TINYSCF_TUNE_FILE in a
+    fresh process, builds the tuned engine's K from the same (SAD) density to
+    rounding. C10H22 has an even number of aux functions (16-byte row copies
+    in the pipelined kernel), HCN an odd one (8-byte copies)."""
+    import os
+    import subprocess
+    import sys
+    if name == "hcn":
+        path = tmp_path / "hcn.xyz"
+        path.write_text("3\n0\nH 0.0 0.0 -1.066\nC 0.0 0.0 0.0\nN 0.0 0.0 1.156\n")
+        path = str(path)
+    else:
+        path = xyz(name)
+    e = tinyscf.TinySCF(BAS, DFBAS, path, 60)
+    e.setup()
+    e.s.iter = 0
+    e.build_FockMat()
+    K = e.mat("K_mat")
+    nbf, nocc, naux = e.s.nbasfuncs, e.s.n_occ, e.s.df_nbf
+    e.free()
+    assert (naux % 2 == 0) == (name == "c10h22")
+    keys = [line.split()[0] for line in tinyscf.autotune_report().splitlines()
+            if line.startswith("khalf:%d:%d:%d:" % (nbf, nocc, naux))]
+    assert len(keys) == 1, keys
+    here = os.path.dirname(os.path.abspath(__file__))
+    for variant in (0, 1, 2, 3):
+        tune = tmp_path / ("tune%d.txt" % variant)
+        tune.write_text("%s %d 0.0\n" % (keys[0], variant))
+        out = tmp_path / ("K%d.npy" % variant)
+        env = dict(os.environ, TINYSCF_TUNE_FILE=str(tune),
+                   PYTHONPATH=os.pathsep.join([here, os.path.join(os.path.dirname(here), "yatscf-df_b200"),
+                                               os.environ.get("PYTHONPATH", "")]))
+        res = subprocess.run([sys.executable, "-c", _PINNED, str(out), path], env=env, capture_output=True,
+                             text=True, timeout=600)
+        assert res.returncode == 0, res.stderr[-2000:]
+        assert "%s -> %d" % (keys[0], variant) in res.stdout, res.stdout
+        assert np.abs(np.load(out) - K).max() < 1e-12 * max(1.0, np.abs(K).max()), variant
+
+
+_PINNED_FAST = r"""
+import sys
+import numpy as np
+import tinyscf
+from conftest import BAS, DFBAS, xyz
+e = tinyscf.TinySCF(BAS, DFBAS, xyz("c10h22"), 60)
+e.setup()
+e.set_k_precision(tinyscf.K_MIXED)
+e.set_density_solver(tinyscf.DENSITY_REFINE)
+e.set_graph(True)
+e.set_guess(tinyscf.GUESS_LEARNED)
+e.reset_scf()
+e.s.ene_tol = 1e-9
+e.do_SCF()
+np.save(sys.argv[1], np.array([e.energy, e.s.iter]))
+np.save(sys.argv[2], e.mat("D_mat"))
+e.free()
+print(tinyscf.autotune_report())
+"""
+
+
+def test_pinned_dgemm_variants_match(tmp_path):
+    """The accelerated form (learned guess, tensor-core K, subspace refinement,
+    CUDA graph) with every tuned FP64 GEMM shape pinned to one tile variant
+    (TINYSCF_TUNE_FILE, fresh process): 64x64 FFMA, 128x128 / 64x64 DMMA and
+    the 32x32 DMMA tile with K split over warps all reach the same energy and
+    density."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    env0 = dict(os.environ, PYTHONPATH=os.pathsep.join([here, os.path.join(os.path.dirname(here), "yatscf-df_b200"),
+                                                         os.environ.get("PYTHONPATH", "")]))
+    out = {}
+    keys = None
+    for variant in (None, 0, 3, 4, 5):
+        tune = tmp_path / ("tune%s.txt" % variant)
+        if variant is not None:
+            tune.write_text("".join("%s %d 0.0\n" % (k, variant) for k in keys))
+        e_out, d_out = tmp_path / ("E%s.npy" % variant), tmp_path / ("D%s.npy" % variant)
+        res = subprocess.run([sys.executable, "-c", _PINNED_FAST, str(e_out), str(d_out)],
+                             env=dict(env0, TINYSCF_TUNE_FILE=str(tune)), capture_output=True, text=True, timeout=600)
+        assert res.returncode == 0, res.stderr[-2000:]
+        if variant is None:
+            keys = [line.split()[0] for line in res.stdout.splitlines() if line.startswith("dgemm:")]
+            assert len(keys) >= 5, res.stdout
+        else:
+            for k in keys:
+                assert "%s -> %d" % (k, variant) in res.stdout, (k, variant)
+        out[variant] = (np.load(e_out), np.load(d_out))
+    E0, D0 = out[None]
+    for variant in (0, 3, 4, 5):
+        E, D = out[variant]
+        assert abs(E[0] - E0[0]) < 1e-8, (variant, E, E0)
+        assert np.abs(D - D0).max() < 1e-6, variant

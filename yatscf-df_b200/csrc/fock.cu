@@ -8,6 +8,7 @@
 // followed by K = T T^T over the flattened (s,P) index (upper tiles, split-K).
 // The DF tensor is stored once per unordered pair (B_u); every ordered CSR
 // entry of the reference (bf_pair_j / bf_mask_displs) maps to its row.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -142,6 +143,159 @@ __global__ void __launch_bounds__(256, 1) k_halftransform_dmma(const double *__r
     half_tile_dmma(B, C, csr_j, csr_u, displs, nocc, naux, T, blockIdx.z, blockIdx.y * KH_S, blockIdx.x * KH_P);
 }
 
+// ---- K half-transform on the FP64 tensor cores, persistent and pipelined.
+// CTA b takes the items b, b + grid, ... (item = row i, 64 occupied columns
+// s0.., 256 aux columns p0.., with the occupied tiles of one (i, p0) adjacent
+// so the gathered DF rows are reused from L2). The CSR chunks of 16 partner
+// rows (the K steps) of its items form one stream that cp.async copies
+// KH_STAGES - 1 steps ahead of the DMMA tiles: the gathers of the next chunks,
+// the tile math and the write-out of a finished item overlap. Each step's row
+// indices are read one step earlier still, so no copy waits on an index load.
+// Tiles and fragment layout are those of half_tile_dmma.
+constexpr int KH_STAGES = 4;
+constexpr int KH_AS = KH_S + 4, KH_BS = KH_P + 4;
+constexpr int KH_STAGE_DOUBLES = KT_K * (KH_AS + KH_BS);
+constexpr size_t KH_PIPE_SMEM = sizeof(double) * KH_STAGES * KH_STAGE_DOUBLES;
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, int bytes)
+{
+    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async16(double *dst, const double *src, int bytes)
+{
+    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+struct KhCursor {
+    int item, i, s0, p0, r0, r_end, step, nsteps;
+};
+
+__device__ __forceinline__ void kh_set(KhCursor &c, int item, int n_items, int stiles, int ptiles,
+                                       const int *__restrict__ displs)
+{
+    c.item = item;
+    if (item >= n_items) return;
+    const int per_row = stiles * ptiles;
+    c.i = item / per_row;
+    const int rem = item - c.i * per_row;
+    c.p0 = (rem / stiles) * KH_P;
+    c.s0 = (rem % stiles) * KH_S;
+    c.r0 = displs[c.i];
+    c.r_end = displs[c.i + 1];
+    c.step = 0;
+    c.nsteps = max(1, (c.r_end - c.r0 + KT_K - 1) / KT_K);   // a row without partners still writes its zeros
+}
+
+__device__ __forceinline__ void kh_next(KhCursor &c, int n_items, int stiles, int ptiles,
+                                        const int *__restrict__ displs)
+{
+    if (c.item >= n_items) return;
+    if (++c.step < c.nsteps) c.r0 += KT_K;
+    else kh_set(c, c.item + gridDim.x, n_items, stiles, ptiles, displs);
+}
+
+// VEC: 16-byte copies of the DF rows (naux even, so every row starts 16-byte aligned)
+template <bool VEC>
+__global__ void __launch_bounds__(256, 1)
+    k_halftransform_pipe(const double *__restrict__ B, const double *__restrict__ C, const int *__restrict__ csr_j,
+                         const int *__restrict__ csr_u, const int *__restrict__ displs, int nocc, int naux,
+                         double *__restrict__ T, int n_items, int stiles, int ptiles)
+{
+    extern __shared__ __align__(16) double khsm[];
+    constexpr int NBR = VEC ? 8 : 16;   // DF rows whose copies this thread issues per step
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ws = (warp >> 2) * 32, wp = (warp & 3) * 64;
+    const int fr = lane >> 2, fc = lane & 3;
+    int iu[NBR], ij[4];
+    KhCursor P, Q;   // P: the next step to copy; Q: the step the tiles consume
+    kh_set(P, blockIdx.x, n_items, stiles, ptiles, displs);
+    Q = P;
+    auto load_idx = [&]() {   // row indices of P's step (-1: past the row, zero fill)
+#pragma unroll
+        for (int q = 0; q < NBR; q++) {
+            const int r = P.r0 + (VEC ? 2 * q + (tid >> 7) : q);
+            iu[q] = (P.item < n_items && r < P.r_end) ? csr_u[r] : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int r = P.r0 + 4 * q + (tid >> 6);
+            ij[q] = (P.item < n_items && r < P.r_end) ? csr_j[r] : -1;
+        }
+    };
+    auto issue = [&](int buf) {   // copies of P's step into stage buffer buf, one commit group
+        double *As = khsm + (size_t) buf * KH_STAGE_DOUBLES, *Bs = As + KT_K * KH_AS;
+        if (P.item < n_items) {
+#pragma unroll
+            for (int q = 0; q < NBR; q++) {
+                const int kk = VEC ? 2 * q + (tid >> 7) : q, cc = VEC ? (tid & 127) * 2 : tid;
+                const int pg = P.p0 + cc;
+                const bool ok = iu[q] >= 0 && pg < naux;
+                const double *src = ok ? B + (size_t) iu[q] * naux + pg : B;
+                if (VEC) cp_async16(&Bs[kk * KH_BS + cc], src, ok ? 16 : 0);
+                else cp_async8(&Bs[kk * KH_BS + cc], src, ok ? 8 : 0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int kk = 4 * q + (tid >> 6), cc = tid & 63, sg = P.s0 + cc;
+                const bool ok = ij[q] >= 0 && sg < nocc;
+                cp_async8(&As[kk * KH_AS + cc], ok ? C + (size_t) ij[q] * nocc + sg : C, ok ? 8 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    for (int st = 0; st < KH_STAGES - 1; st++) {
+        load_idx();
+        issue(st);
+        kh_next(P, n_items, stiles, ptiles, displs);
+    }
+    load_idx();
+    double acc[4][8][2];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 8; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    for (int g = 0; Q.item < n_items; g++) {
+        cp_async_wait<KH_STAGES - 2>();   // this thread's copies of step g have landed
+        __syncthreads();                  // everyone's have, and step g - 1's buffer is free
+        issue((g + KH_STAGES - 1) % KH_STAGES);
+        kh_next(P, n_items, stiles, ptiles, displs);
+        load_idx();
+        const double *As = khsm + (size_t) (g % KH_STAGES) * KH_STAGE_DOUBLES, *Bs = As + KT_K * KH_AS;
+#pragma unroll
+        for (int k4 = 0; k4 < KT_K; k4 += 4) {
+            double a[4], b[8];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[(k4 + fc) * KH_AS + ws + 8 * x + fr];
+#pragma unroll
+            for (int y = 0; y < 8; y++) b[y] = Bs[(k4 + fc) * KH_BS + wp + 8 * y + fr];
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 8; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        if (++Q.step == Q.nsteps) {   // item done: write its tile, start the next
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+                const int sg = Q.s0 + ws + 8 * x + fr;
+                double *row = T + ((size_t) Q.i * nocc + (sg < nocc ? sg : 0)) * naux;
+#pragma unroll
+                for (int y = 0; y < 8; y++) {
+                    const int pg = Q.p0 + wp + 8 * y + 2 * fc;
+                    if (sg < nocc && pg < naux) row[pg] = acc[x][y][0];
+                    if (sg < nocc && pg + 1 < naux) row[pg + 1] = acc[x][y][1];
+                    acc[x][y][0] = acc[x][y][1] = 0.0;
+                }
+            }
+            kh_set(Q, Q.item + gridDim.x, n_items, stiles, ptiles, displs);
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // K partial tiles: upper tile pairs (bi <= bj) of 64x64, split over the
 // flattened Q = nocc*naux index. Kpart[split][i][j].
 __global__ void __launch_bounds__(256) k_syrk_part(const double *__restrict__ T, int nbf, long long Q, long long qchunk,
@@ -192,7 +346,26 @@ size_t build_K_part_elems(const FockPlan &p, int ksplit) { return (size_t) kspli
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide)
 {
     g_launches++;
-    if (wide) {
+    if (wide == 3) {
+        const int stiles = (p.nocc + KH_S - 1) / KH_S, ptiles = (p.naux + KH_P - 1) / KH_P;
+        const long long items = (long long) p.nbf * stiles * ptiles;
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_halftransform_pipe<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int) KH_PIPE_SMEM);
+        cudaFuncSetAttribute(k_halftransform_pipe<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int) KH_PIPE_SMEM);
+        const int grid = (int) std::min<long long>(items, sms > 0 ? sms : 148);
+        if (p.naux % 2 == 0)
+            k_halftransform_pipe<true><<<grid, 256, KH_PIPE_SMEM, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs,
+                                                                       p.nocc, p.naux, d_T, (int) items, stiles,
+                                                                       ptiles);
+        else
+            k_halftransform_pipe<false><<<grid, 256, KH_PIPE_SMEM, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u,
+                                                                        p.csr_displs, p.nocc, p.naux, d_T,
+                                                                        (int) items, stiles, ptiles);
+    } else if (wide) {
         dim3 g1((p.naux + KH_P - 1) / KH_P, (p.nocc + KH_S - 1) / KH_S, p.nbf);
         if (wide == 2)
             k_halftransform_dmma<<<g1, 256, 0, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T);

@@ -81,10 +81,130 @@ static void dgemm_dmma64(bool ta, bool tb, int m, int n, int k, double alpha, co
     else k_dgemm_dmma64<true, true><<<grid, 128, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
+// ---- 32 x 32 output tile per 256 threads on the FP64 tensor cores, the K
+// range split over the 8 warps: for the tall-skinny and small products of the
+// density refinement, DIIS and orbital alignment (n x n_occ outputs, n_occ^2
+// outputs with K = n), where the 64/128 tiles leave most SMs idle and a
+// single warp per tile would run the whole K loop alone. Each 64-wide K chunk
+// is prefetched into registers while the previous one is multiplied (warp w
+// takes chunk rows 8w..8w+7); the eight partial tiles are summed through
+// shared memory in a fixed order.
+constexpr int KS_T = 32, KS_K = 64, KS_LD = KS_K + 4;
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256) k_dgemm_dmma32ks(int m, int n, int k, double alpha,
+                                                        const double *__restrict__ A, int lda,
+                                                        const double *__restrict__ B, int ldb, double beta,
+                                                        double *C, int ldc)
+{
+    __shared__ double sm[2 * KS_T * KS_LD];   // As[32][68], Bs[32][68]; then the partial-tile slots
+    double *As = sm, *Bs = sm + KS_T * KS_LD;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int fr = lane >> 2, fc = lane & 3;
+    const int m0 = blockIdx.y * KS_T, n0 = blockIdx.x * KS_T;
+    double acc[4][4][2];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    double pa[8], pb[8];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = tid + 256 * r;
+            int row, kk;
+            if (!TA) { row = l / KS_K; kk = l % KS_K; } else { kk = l / KS_T; row = l % KS_T; }
+            const int gi = m0 + row, gk = k0 + kk;
+            pa[r] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
+            int col;
+            if (!TB) { kk = l / KS_T; col = l % KS_T; } else { col = l / KS_K; kk = l % KS_K; }
+            const int gj = n0 + col, gk2 = k0 + kk;
+            pb[r] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
+        }
+    };
+    fetch(0);
+    for (int k0 = 0; k0 < k; k0 += KS_K) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = tid + 256 * r;
+            if (!TA) As[(l / KS_K) * KS_LD + l % KS_K] = pa[r];
+            else As[(l % KS_T) * KS_LD + l / KS_T] = pa[r];
+            if (!TB) Bs[(l % KS_T) * KS_LD + l / KS_T] = pb[r];
+            else Bs[(l / KS_K) * KS_LD + l % KS_K] = pb[r];
+        }
+        __syncthreads();
+        if (k0 + KS_K < k) fetch(k0 + KS_K);
+#pragma unroll
+        for (int k4 = 0; k4 < 8; k4 += 4) {
+            const int kc = 8 * warp + k4 + fc;
+            double a[4], b[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) a[x] = As[(8 * x + fr) * KS_LD + kc];
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[(8 * y + fr) * KS_LD + kc];
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        __syncthreads();
+    }
+    // warps 4-7 into 0-3, then 2-3 into 0-1, then 1 into 0 (slots of 32 x 32 per warp)
+    double *red = sm;
+    for (int half = 4; half >= 1; half >>= 1) {
+        if (warp >= half && warp < 2 * half) {
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) red[(warp - half) * 1024 + ((x * 4 + y) * 2 + h) * 32 + lane] = acc[x][y][h];
+        }
+        __syncthreads();
+        if (warp < half) {
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) acc[x][y][h] += red[warp * 1024 + ((x * 4 + y) * 2 + h) * 32 + lane];
+        }
+        __syncthreads();
+    }
+    if (warp != 0) return;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        const int gi = m0 + 8 * x + fr;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int gj = n0 + 8 * y + 2 * fc + h;
+                if (gj >= n) continue;
+                double *c = C + (size_t) gi * ldc + gj;
+                *c = (beta == 0.0) ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * *c;
+            }
+        }
+    }
+}
+
+static void dgemm_dmma32ks(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
+                           const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
+{
+    dim3 grid((n + KS_T - 1) / KS_T, (m + KS_T - 1) / KS_T);
+    g_launches++;
+    if (!ta && !tb) k_dgemm_dmma32ks<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (!ta && tb) k_dgemm_dmma32ks<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (ta && !tb) k_dgemm_dmma32ks<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else k_dgemm_dmma32ks<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
 static void dgemm_variant(int v, bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
                           const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s)
 {
-    if (v == 4) dgemm_dmma64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    if (v == 5) dgemm_dmma32ks(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    else if (v == 4) dgemm_dmma64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else if (v == 3) dgemm_dmma(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else if (v == 1) dgemm_shape<32, 32>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
     else if (v == 2) dgemm_shape<128, 64>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
@@ -112,7 +232,7 @@ void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
         const size_t ea = ta ? (size_t) k * lda : (size_t) m * lda, eb = tb ? (size_t) n * ldb : (size_t) k * ldb;
         if (tune_enabled() && cs == cudaStreamCaptureStatusNone && beta == 0.0 && disjoint(A, ea) && disjoint(B, eb) &&
             (double) m * n * k >= 2e6) {
-            v = tune_run(key, {0, 1, 2, 3, 4}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
+            v = tune_run(key, {0, 1, 2, 3, 4, 5}, [&](int c) { dgemm_variant(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s); }, s);
             return;
         }
     }

@@ -972,8 +972,9 @@ int autotune_fock(TinySCF_t t)
     }
     snprintf(key, sizeof(key), "khalf:%d:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf, e->nnz);
     c = tune_lookup(key);
-    if (c < 0) c = tune_run(key, {0, 1, 2}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
-    if (c >= 0 && c <= 2) e->khwide = c;
+    if (c < 0)
+        c = tune_run(key, {0, 1, 2, 3}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
+    if (c >= 0 && c <= 3) e->khwide = c;
     snprintf(key, sizeof(key), "jrows:%d:%d", e->nup, t->df_nbf);
     c = tune_lookup(key);
     if (c < 0) {
@@ -1950,7 +1951,7 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         c_nup64.push_back((e->nup + 63) / 64);
         c_half.push_back(e->khwide ? 0 : n * ((o + 63) / 64) * ((na + 63) / 64));
         c_halfw.push_back(e->khwide == 1 ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);
-        c_halfd.push_back(e->khwide == 2 ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);
+        c_halfd.push_back(e->khwide >= 2 ? n * ((o + 63) / 64) * ((na + 255) / 256) : 0);   // DMMA tiles
         const int nt2 = (n + 127) / 128;
         c_syrk.push_back(e->ktile == 64 ? nt * (nt + 1) / 2 * e->ksplit : 0);
         c_syrk128.push_back(e->ktile == 128 ? nt2 * (nt2 + 1) / 2 * e->ksplit : 0);

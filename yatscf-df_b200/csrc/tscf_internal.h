@@ -152,7 +152,9 @@ void build_J_f32(const FockPlan &p, const float *B32, const double *d_D, double 
 void convert_f32(const double *in, float *out, size_t n, cudaStream_t s);
 // K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
 // wide = 1: 64 x 256 FFMA tiles (k_halftransform_wide), 2: 64 x 256 DMMA tiles
-// (k_halftransform_dmma), 0: 64 x 64 FFMA tiles
+// (k_halftransform_dmma), 3: the same DMMA tiles in persistent CTAs with a
+// cp.async pipeline over the CSR chunks (k_halftransform_pipe), 0: 64 x 64
+// FFMA tiles
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide = 0);
 // ... then K = T T^T over upper 64x64 tiles (d_tiles: (bi,bj), bi <= bj), split-K, mirrored.
 // tile = 64 (k_syrk_part, FFMA), 128 (k_syrk_part128, FFMA) or KSYRK_DMMA
