@@ -55,8 +55,8 @@ print(tinyscf.autotune_report())
 def test_pinned_half_transform_variants_match(tmp_path, name):
     """Each exchange half-transform variant (64x64 FFMA, 64x256 FFMA, 64x256
     DMMA, pipelined persistent DMMA), pinned through TINYSCF_TUNE_FILE in a
-    fresh process, builds the tuned engine's K from the same (SAD) density to
-    rounding. C10H22 has an even number of aux functions (16-byte row copies
+    fresh process, builds the tuned engine's K from the same (SAD) density up
+    to summation-order rounding. C10H22 has an even number of aux functions (16-byte row copies
     in the pipelined kernel), HCN an odd one (8-byte copies)."""
     import os
     import subprocess
@@ -90,7 +90,9 @@ def test_pinned_half_transform_variants_match(tmp_path, name):
                              text=True, timeout=600)
         assert res.returncode == 0, res.stderr[-2000:]
         assert "%s -> %d" % (keys[0], variant) in res.stdout, res.stdout
-        assert np.abs(np.load(out) - K).max() < 1e-12 * max(1.0, np.abs(K).max()), variant
+        # summation order differs between the FFMA and DMMA tiles: a few 1e-12
+        # on C10H22; the parity tests hold K to 1e-10 against the golden files
+        assert np.abs(np.load(out) - K).max() < 1e-10, variant
 
 
 _PINNED_FAST = r"""
@@ -146,5 +148,7 @@ def test_pinned_dgemm_variants_match(tmp_path):
     E0, D0 = out[None]
     for variant in (0, 3, 4, 5):
         E, D = out[variant]
+        # converged to 1e-9 Eh from slightly different rounding: the energies
+        # agree to the convergence threshold, the densities to its square root
         assert abs(E[0] - E0[0]) < 1e-8, (variant, E, E0)
-        assert np.abs(D - D0).max() < 1e-6, variant
+        assert np.abs(D - D0).max() < 1e-4, variant
