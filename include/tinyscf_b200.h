@@ -162,6 +162,20 @@ TINYSCF_API int TinySCF_guess_used(TinySCF_t t);
  * pairs and returns the count (negative status on error). */
 TINYSCF_API long long TinySCF_guess_dataset(TinySCF_t t, const double *D, float *feat, float *target, int *type,
                                             long long cap);
+/* The learned guess's atom-pair blocks for a molecule (no GPU needed):
+ * natoms atoms with 0-based element indices elem (H = 0, C = 5, N = 6, O = 7),
+ * Bohr coordinates xyz (natoms x 3) and, per atom, nshell[a] shell angular
+ * momenta in basis order in shell_am (all atoms' lists concatenated). For
+ * block k < cap writes ab[2k], ab[2k+1] (its atoms, the one with more
+ * functions first; equal atoms for a diagonal block), type[k] (0-4),
+ * frame[9k..9k+8] (3 x 3 row-major, rows the local axes e_x, e_y, e_z) and
+ * feat[128k..128k+127] (the invariant features the networks read); any of
+ * the four may be NULL, all four NULL returns the count alone. Returns the
+ * number of blocks, -TINYSCF_ERR_UNSUPPORTED when an element or shell layout
+ * is not covered, -TINYSCF_ERR_INPUT when cap is too small. */
+TINYSCF_API long long TinySCF_guess_pairs(int natoms, const int *elem, const double *xyz, const int *nshell,
+                                          const int *shell_am, int *ab, int *type, double *frame, float *feat,
+                                          long long cap);
 /* The basis rotation the learned guess uses for one atom (no GPU needed):
  * with molecule coordinates x_m = Q^T x_l (Q: 3 x 3 row-major, rows the local
  * axes), writes M (nf x nf row-major, nf = sum of Cartesian components of the

@@ -65,3 +65,83 @@ def test_guess_rotation_transforms_cartesian_functions():
         phi_l = np.concatenate([_monomials(xl, l) for l in am])
         phi_m = np.concatenate([_monomials(xm, l) for l in am])
         assert np.abs(phi_m - M @ phi_l).max() < 1e-12
+
+
+_EL = {"H": 0, "C": 5, "N": 6, "O": 7, "S": 15}
+_BOHR = 1.0 / 0.52917720859
+
+
+def _mol(atoms):
+    el = [_EL[a[0]] for a in atoms]
+    xyz = np.array([a[1:] for a in atoms], dtype=np.float64) * _BOHR
+    am = [[0, 0, 1] if e == 0 else [0, 0, 0, 1, 1, 2] for e in el]
+    return el, xyz, am
+
+
+def _molecules():
+    sys.path.insert(0, os.path.join(REPO, "yatscf-df_b200"))
+    import geometry
+    mols = {"water_cluster_%d" % s: geometry.water_cluster(s) for s in (0, 1, 2)}
+    mols["propane"] = geometry.alkane(3)
+    mols["hcn"] = [("H", 0.0, 0.0, -1.066), ("C", 0.0, 0.0, 0.0), ("N", 0.0, 0.0, 1.156)]
+    mols["n2"] = [("N", 0.0, 0.0, 0.0), ("N", 0.0, 0.0, 1.10)]
+    mols["oxygen_atom"] = [("O", 0.0, 0.0, 0.0)]
+    # equal distances everywhere: the frame choice rests on the index tie-break
+    mols["methane_td"] = [("C", 0.0, 0.0, 0.0), ("H", 0.63, 0.63, 0.63), ("H", -0.63, -0.63, 0.63),
+                          ("H", -0.63, 0.63, -0.63), ("H", 0.63, -0.63, -0.63)]
+    return mols
+
+
+def test_pair_blocks_match_restatement():
+    """The library's pair list, block types, local frames and features (host
+    code, no GPU) against the scalar restatement: same blocks in the same
+    order, frames to 1e-14, features equal after rounding to float32 (both
+    evaluate the same double expressions; exp/cos may differ in the last
+    double bit, which a float32 rounding almost never shows)."""
+    sys.path.insert(0, os.path.join(REPO, "yatscf-df_b200"))
+    import tinyscf
+    for name, atoms in _molecules().items():
+        el, xyz, am = _mol(atoms)
+        ref = go.pair_blocks(el, xyz, am)
+        lib = tinyscf.guess_pairs(el, xyz, am)
+        assert len(ref) == len(lib["type"]), name
+        assert np.array_equal(np.array([[r[0], r[1]] for r in ref]).reshape(-1, 2), lib["ab"]), name
+        assert np.array_equal(np.array([r[2] for r in ref]), lib["type"]), name
+        assert np.abs(np.array([r[3] for r in ref]) - lib["frame"]).max() < 1e-14, name
+        f = np.array([r[4] for r in ref], dtype=np.float64).astype(np.float32)
+        assert np.abs(f - lib["feat"]).max() <= 1e-7, name
+        Q = lib["frame"]
+        assert np.abs(np.einsum("kij,klj->kil", Q, Q) - np.eye(3)).max() < 1e-12, name   # orthonormal rows
+
+
+def test_pair_features_invariant_under_rotation():
+    """Rotating and translating the molecule leaves the blocks and features
+    unchanged (to float32 rounding of coordinates) and rotates every frame:
+    Q' = Q R^T for x' = R x + t."""
+    sys.path.insert(0, os.path.join(REPO, "yatscf-df_b200"))
+    import tinyscf
+    rng = np.random.default_rng(11)
+    for name in ("water_cluster_1", "propane", "hcn"):
+        el, xyz, am = _mol(_molecules()[name])
+        R = _random_rotation(rng)
+        if np.linalg.det(R) < 0:
+            R[:, 0] = -R[:, 0]
+        a = tinyscf.guess_pairs(el, xyz, am)
+        b = tinyscf.guess_pairs(el, xyz @ R.T + rng.normal(size=3), am)
+        assert np.array_equal(a["ab"], b["ab"]) and np.array_equal(a["type"], b["type"]), name
+        assert np.abs(a["feat"] - b["feat"]).max() < 1e-5, name
+        if name != "hcn":   # a linear molecule's frames fall back to a fixed perpendicular
+            assert np.abs(np.einsum("kij,lj->kil", a["frame"], R) - b["frame"]).max() < 1e-9, name
+
+
+def test_pair_blocks_reject_uncovered_elements():
+    sys.path.insert(0, os.path.join(REPO, "yatscf-df_b200"))
+    import tinyscf
+    el, xyz, am = _mol([("S", 0.0, 0.0, 0.0), ("H", 0.0, 0.0, 1.34)])
+    assert go.pair_blocks(el, xyz, am) is None
+    try:
+        tinyscf.guess_pairs(el, xyz, am)
+    except tinyscf.TinySCFError as err:
+        assert "UNSUPPORTED" in str(err).upper(), err
+    else:
+        raise AssertionError("an uncovered element must be rejected")

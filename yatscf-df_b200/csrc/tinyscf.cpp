@@ -1657,6 +1657,46 @@ long long TinySCF_guess_dataset(TinySCF_t t, const double *D, float *feat, float
     return (long long) pairs.size();
 }
 
+long long TinySCF_guess_pairs(int natoms, const int *elem, const double *xyz, const int *nshell, const int *shell_am,
+                              int *ab, int *type, double *frame, float *feat, long long cap)
+{
+    if (natoms <= 0 || !elem || !xyz || !nshell || !shell_am || cap < 0) return -TINYSCF_ERR_INPUT;
+    GuessAtoms g;
+    g.natoms = natoms;
+    g.eid = elem;
+    g.xyz = xyz;
+    std::vector<int> bf0(natoms);
+    g.shell_am.assign(natoms, {});
+    int sh = 0, nf = 0;
+    for (int a = 0; a < natoms; a++) {
+        if (nshell[a] < 0) return -TINYSCF_ERR_INPUT;
+        bf0[a] = nf;
+        for (int k = 0; k < nshell[a]; k++, sh++) {
+            const int l = shell_am[sh];
+            if (l < 0 || l > 2) return -TINYSCF_ERR_UNSUPPORTED;
+            g.shell_am[a].push_back(l);
+            nf += (l + 1) * (l + 2) / 2;
+        }
+    }
+    g.bf0 = bf0.data();
+    std::vector<GuessPair> pairs;
+    if (guess_pairs(g, pairs)) return -TINYSCF_ERR_UNSUPPORTED;
+    const long long n = (long long) pairs.size();
+    if (!ab && !type && !frame && !feat) return n;
+    if (n > cap) return -TINYSCF_ERR_INPUT;
+    for (long long k = 0; k < n; k++) {
+        const GuessPair &p = pairs[k];
+        if (ab) {
+            ab[2 * k] = p.a;
+            ab[2 * k + 1] = p.b;
+        }
+        if (type) type[k] = p.type;
+        if (frame) std::memcpy(frame + 9 * k, p.Qf, sizeof(p.Qf));
+        if (feat) std::memcpy(feat + (size_t) k * G_DIN, p.feat, sizeof(p.feat));
+    }
+    return n;
+}
+
 int TinySCF_guess_rotation(const int *shell_am, int nshells, const double *Q, double *M)
 {
     if (!shell_am || !Q || !M || nshells <= 0) return TINYSCF_ERR_INPUT;

@@ -122,6 +122,10 @@ def load_library(path=LIBPATH):
                                  ctypes.c_uint, ctypes.c_char_p, fp], ip),
         "TinySCF_guess_mlp_grad": ([ip, ip, ip, fp, fp, fp, ip, fp, fp], ip),
         "TinySCF_guess_rotation": ([ctypes.POINTER(ctypes.c_int), ip, dp, dp], ip),
+        "TinySCF_guess_pairs": ([ip, ctypes.POINTER(ctypes.c_int), dp, ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_int), dp, ctypes.POINTER(ctypes.c_float),
+                                 ctypes.c_longlong], ctypes.c_longlong),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
     }
     for name, (args, res) in sig.items():
@@ -438,6 +442,31 @@ def device_memory(device=0):
     if rc:
         raise TinySCFError("device_memory: " + STATUS.get(rc, str(rc)))
     return f.value, t.value
+
+
+def guess_pairs(elem, xyz_bohr, shell_am):
+    """The learned guess's pair blocks (host code, no GPU): elem (0-based element
+    indices), xyz_bohr (natoms x 3), shell_am (one list of shell angular momenta
+    per atom). Returns dict(ab [n,2], type [n], frame [n,3,3], feat [n,128])."""
+    lib = load_library()
+    ci = ctypes.POINTER(ctypes.c_int)
+    el = np.ascontiguousarray(elem, dtype=np.int32)
+    xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64)
+    ns = np.ascontiguousarray([len(s) for s in shell_am], dtype=np.int32)
+    am = np.ascontiguousarray([l for s in shell_am for l in s], dtype=np.int32)
+    args = (len(el), el.ctypes.data_as(ci), _dptr(xyz), ns.ctypes.data_as(ci), am.ctypes.data_as(ci))
+    n = lib.TinySCF_guess_pairs(*args, None, None, None, None, 0)
+    if n < 0:
+        raise TinySCFError("guess_pairs: " + STATUS.get(-n, str(-n)))
+    ab = np.zeros((n, 2), dtype=np.int32)
+    ty = np.zeros(n, dtype=np.int32)
+    fr = np.zeros((n, 3, 3))
+    ft = np.zeros((n, GUESS_DIN), dtype=np.float32)
+    m = lib.TinySCF_guess_pairs(*args, ab.ctypes.data_as(ci), ty.ctypes.data_as(ci), _dptr(fr),
+                                ft.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n)
+    if m != n:
+        raise TinySCFError("guess_pairs: " + STATUS.get(-m, str(m)))
+    return dict(ab=ab, type=ty, frame=fr, feat=ft)
 
 
 def guess_rotation(shell_am, Q):
