@@ -1,7 +1,7 @@
 /*
  * ORACLE — test infrastructure only. Nothing in the product links this file;
  * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it,
- * and only as the checker.
+ * and there only to check results.
  *
  * Cartesian Gaussian integral engine (McMurchie–Davidson) restating the
  * integrals the reference obtains from the un-vendored Simint library

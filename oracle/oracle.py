@@ -2,14 +2,16 @@
 
 A numpy restatement of the reference's DF-RHF path (huanghua1994/YATSCF-DF),
 used only by tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline
-leg, and only as the checker. Every function names the reference file:line it
+leg, and there only to check results, never as the computation measured or
+shipped. Every function names the reference file:line it
 follows. Integrals come from the oracle's own McMurchie–Davidson engine
 (ints.c, oracle_bulk.c via ctypes) because the reference's Simint is not
 available; linear algebra is numpy/scipy LAPACK, standing in for MKL.
 
 The restatement is pinned against the reference's own C sources compiled by
 ``oracle/Makefile`` (``oracle/_ref/ref_dump``) on the same inputs: see
-tests/test_oracle_vs_ref.py and the fixtures in tests/golden/.
+tests/test_oracle_golden.py and the fixtures in tests/golden/ (written by
+tests/golden/make_fixtures.py).
 """
 import ctypes
 import math
