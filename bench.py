@@ -345,18 +345,24 @@ def run_ours(args, rank, world, local_rank):
         note = ("algorithmic flops of one G = dT S^T build over k_gemm's average device time (CUDA events around "
                 "each launch); tensor_pipe_frac counts the 3 BF16 products executed per algorithmic flop")
     # achieved rates of the set-up and FP64 kernels per unit of work: 3-centre output bytes and quartets,
-    # DF GEMM 2 nu naux^2 flops, J 2 nu naux 8 bytes (two streams of the DF tensor), FP64 K flops; set-up
+    # DF GEMM 2 nu naux^2 flops, J 2 nu naux x 8 (FP64) or 4 (FP32 copy) bytes (two streams of the DF
+    # tensor), FP64 K flops; set-up
     # phases from the e2e engine (the autotuner's table already filled, so no tuning runs inside)
     su = setup_tuned if setup_tuned is not None else st
     nu = (nnz + nbf) // 2                      # unique pairs: rows of the DF tensor
+    # bytes per DF-tensor element the timed J builds stream: the mixed form's iterations read the FP32 copy,
+    # its one final build per solve the FP64 tensor
+    jcnt = max(1, stats["J"][1])
+    jb = 8.0 if args.precision == "fp64" else (4.0 * max(0, jcnt - args.steps) + 8.0 * min(jcnt, args.steps)) / jcnt
     rates = {
         "3c_integrals": {"ms": su["3C"], "bytes_written": nu * naux * 8,
                          "GB_per_s": nu * naux * 8 / (su["3C"] * 1e-3) / 1e9,
                          "quartets_per_s": (n3c / (su["3C"] * 1e-3)) if n3c else None},
         "df_gemm": {"ms": su["DFGEMM"], "TFLOP_per_s": 2.0 * nu * naux * naux / (su["DFGEMM"] * 1e-3) / 1e12},
         "j_build": {"ms": stats["J"][0] / max(1, stats["J"][1]),
-                    "GB_per_s": 2.0 * nu * naux * 8 / (stats["J"][0] / max(1, stats["J"][1]) * 1e-3) / 1e9,
-                    "frac_of_hbm": 2.0 * nu * naux * 8 / (stats["J"][0] / max(1, stats["J"][1]) * 1e-3) / 1e9 / hbm},
+                    "bytes_per_element": jb,
+                    "GB_per_s": 2.0 * nu * naux * jb / (stats["J"][0] / max(1, stats["J"][1]) * 1e-3) / 1e9,
+                    "frac_of_hbm": 2.0 * nu * naux * jb / (stats["J"][0] / max(1, stats["J"][1]) * 1e-3) / 1e9 / hbm},
         "k_fp64_halftransform": {"ms": stats["K_HT"][0] / max(1, stats["K_HT"][1]),
                                  "TFLOP_per_s": fht / (stats["K_HT"][0] / max(1, stats["K_HT"][1]) * 1e-3) / 1e12},
         "k_fp64_rank_k": {"ms": stats["K_SYRK"][0] / max(1, stats["K_SYRK"][1]),
