@@ -94,16 +94,16 @@ void make_frame(const double *origin, const double *z, const double *x_atom, dou
 // for every orientation of the molecule.
 std::pair<long long, int> dkey(double r_angstrom, int idx) { return {std::llround(r_angstrom * 1e4), idx}; }
 
-// The atom that fixes e_x: among all atoms but skip0..skip2, the one with the
+// The atom that fixes e_x: among all atoms but skip0 and skip1, the one with the
 // smallest key (distance from `origin`, then index) whose distance from the
 // z axis through `origin` exceeds 0.25 A; -1 when there is none. One pass
 // over the atoms instead of sorting them.
-int x_atom(const GuessAtoms &g, const double *origin, const double *z, int skip0, int skip1, int skip2)
+int x_atom(const GuessAtoms &g, const double *origin, const double *z, int skip0, int skip1)
 {
     int best = -1;
     std::pair<long long, int> bkey;
     for (int c = 0; c < g.natoms; c++) {
-        if (c == skip0 || c == skip1 || c == skip2) continue;
+        if (c == skip0 || c == skip1) continue;
         double v[3];
         sub(g.xyz + 3 * c, origin, v);
         const std::pair<long long, int> key = dkey(std::sqrt(dot(v, v)) * BOHR2A, c);
@@ -193,7 +193,7 @@ void fill_pair(const GuessAtoms &g, const std::vector<int> &nf, int a, int b, Gu
             double z[3];
             sub(g.xyz + 3 * near, g.xyz + 3 * a, z);
             unit(z);
-            const int x = x_atom(g, g.xyz + 3 * a, z, a, near, -1);
+            const int x = x_atom(g, g.xyz + 3 * a, z, a, near);
             make_frame(g.xyz + 3 * a, z, x >= 0 ? g.xyz + 3 * x : nullptr, p.Qf);
         }
         features(g, a, a, g.xyz + 3 * a, p.Qf, p.feat, env);
@@ -204,7 +204,7 @@ void fill_pair(const GuessAtoms &g, const std::vector<int> &nf, int a, int b, Gu
     for (int k = 0; k < 3; k++) mid[k] = 0.5 * (g.xyz[3 * a + k] + g.xyz[3 * b + k]);
     sub(g.xyz + 3 * b, g.xyz + 3 * a, z);
     unit(z);
-    const int x = x_atom(g, mid, z, a, b, -1);
+    const int x = x_atom(g, mid, z, a, b);
     make_frame(mid, z, x >= 0 ? g.xyz + 3 * x : nullptr, p.Qf);
     features(g, a, b, mid, p.Qf, p.feat, env);
 }
@@ -249,8 +249,15 @@ int guess_pairs(const GuessAtoms &g, std::vector<GuessPair> &out)
         return 0;
     }
     std::vector<std::thread> th;
-    for (int t = 1; t < nth; t++) th.emplace_back(run, t);
-    run(0);
+    std::vector<int> here{0};   // shares run on this thread (all of them if no thread can be started)
+    for (int t = 1; t < nth; t++) {
+        try {
+            th.emplace_back(run, t);
+        } catch (...) {
+            here.push_back(t);
+        }
+    }
+    for (int t : here) run(t);
     for (std::thread &x : th) x.join();
     return 0;
 }
