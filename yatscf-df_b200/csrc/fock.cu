@@ -345,6 +345,7 @@ size_t build_K_part_elems(const FockPlan &p, int ksplit) { return (size_t) kspli
 
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide)
 {
+    if (p.nbf <= 0 || p.nocc <= 0 || p.naux <= 0) return;   // T is empty: no grid to launch
     g_launches++;
     if (wide == 3) {
         const int stiles = (p.nocc + KH_S - 1) / KH_S, ptiles = (p.naux + KH_P - 1) / KH_P;
