@@ -218,8 +218,8 @@ TINYSCF_API int TinySCF_autotune_report(char *buf, int len);
  * FP64 Fock build on the converged densities gives its energy, as
  * TinySCF_do_SCF does). TinySCF_batch_do_SCF then iterates all of
  * them together: every SCF phase (J, K, Fock + energy, DIIS, density) is one
- * launch over all molecules still iterating, the eigensolves one batched
- * cuSOLVER call per group of equal basis size. Each molecule follows its own
+ * launch over all molecules still iterating; the density eigensolves run
+ * molecule by molecule on the engine's eigensolver. Each molecule follows its own
  * reference loop (ene_tol, niters, iteration count, DIIS history) and ends
  * with its host mirrors filled as after TinySCF_do_SCF. The handles must stay
  * alive until TinySCF_batch_free (which frees only the batch). */
@@ -234,6 +234,16 @@ TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iter
  * of the molecules set to TINYSCF_K_MIXED; min(n, 6) values. */
 TINYSCF_API int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n);
 TINYSCF_API int TinySCF_batch_free(TinySCF_batch_t b);
+/* The engine's FP64 symmetric eigensolver on host buffers: A (n x n,
+ * row-major, symmetric) -> w (n eigenvalues, ascending) and V (n x n, row k =
+ * eigenvector k). It is what replaces the reference's LAPACKE_dsyev calls
+ * (TinySCF.c:65 for X = S^-1/2, build_DF_tensor.c:217 for (P|Q)^-1/2,
+ * build_density.c:54 for the Fock eigensolve): Householder
+ * tridiagonalisation, divide and conquer, back-transformation, all as this
+ * library's kernels. n <= 8192. Allocates and frees its own workspace on the
+ * device; synchronous. TINYSCF_ERR_CUDA if a grid barrier of the
+ * tridiagonalisation gave up waiting. */
+TINYSCF_API int TinySCF_eigh(int device, int n, const double *A, double *w, double *V);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

@@ -1,0 +1,1132 @@
+// FP64 symmetric eigensolver of the SCF: X = S^-1/2 (TinySCF.c:58-76), the
+// DF metric's (P|Q)^-1/2 (build_DF_tensor.c:205-237) and the orthogonalised
+// Fock eigensolve (build_density.c:37-69), where the reference calls
+// LAPACKE_dsyev. Three stages, all on the device:
+//
+//  1. Householder tridiagonalisation Q^T A Q = T (LAPACK dsytrd/dlatrd's
+//     recurrence). Panels of TRD_NB columns: one cooperative kernel per panel
+//     runs the column steps -- update the column with the panel's earlier
+//     reflectors, form the reflector, the symmetric matrix-vector product with
+//     the trailing matrix (not yet updated for the panel), the panel
+//     corrections -- separated by grid barriers; then two GEMMs apply the
+//     rank-2*TRD_NB update to the trailing matrix.
+//  2. Divide and conquer on T (Cuppen): T is torn by rank-one updates down to
+//     1 x 1 pieces; each merge of two solved halves deflates small and close
+//     components (LAPACK dlaed2's tests, Givens rotations for close pairs),
+//     finds the roots of the secular equation by bisection on the offset from
+//     the nearer pole, recomputes z from the roots (Gu-Eisenstat, so that the
+//     eigenvectors come out orthogonal) and multiplies the halves' vectors by
+//     the merge's vectors. All merges of one tree level run in the same launches.
+//  3. Back-transformation with the compact WY form of each panel
+//     (H_p..H_(p+nb-1) = I - V T V^T), three GEMMs per panel.
+//
+// Every grid barrier spins a bounded number of times; a barrier that runs out
+// sets the object's error flag and every CTA returns (eig_error() reports it).
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "tiles.cuh"
+#include "tscf_internal.h"
+
+namespace tscf {
+
+namespace {
+
+constexpr int TRD_THREADS = 512;
+constexpr int TRD_NB = 32;        // columns per panel
+constexpr int TRD_NG = 8;         // CTAs that form the panel's dot products
+constexpr int DC_CHUNK = 256;     // items per CTA of the thread-per-item D&C kernels
+constexpr int DC_WCHUNK = 8;      // items per CTA of the warp-per-item D&C kernels (256 threads)
+constexpr long long kBarrierSpins = 1LL << 22;
+constexpr size_t kMaxDynSmem = 227 * 1024;
+
+__device__ __forceinline__ double warp_sum_bcast(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffff, v, o);
+    return __shfl_sync(0xffffffff, v, 0);
+}
+
+__device__ __forceinline__ double warp_prod_bcast(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v *= __shfl_down_sync(0xffffffff, v, o);
+    return __shfl_sync(0xffffffff, v, 0);
+}
+
+// Sum over the block in a fixed order (warp trees, then warp 0 over the
+// warps); the result is returned to every thread.
+template <int NT>
+__device__ double block_sum_all(double v, double *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffff, v, o);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double x = lane < NT / 32 ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffff, x, o);
+        if (lane == 0) sh[32] = x;
+    }
+    __syncthreads();
+    const double r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+template <int NT>
+__device__ double block_max_all(double v, double *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffff, v, o));
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double x = lane < NT / 32 ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffff, x, o));
+        if (lane == 0) sh[32] = x;
+    }
+    __syncthreads();
+    const double r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// Grid barrier for a cooperative launch (all CTAs co-resident): an arrival
+// counter and a generation word. The wait is bounded; on time-out the error
+// flag is set. Returns false (in every thread of the CTA) once the flag is
+// set, and the caller returns.
+__device__ bool grid_barrier(unsigned *bar, int *err, unsigned nblk)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblk - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g) {
+                if (++spins > kBarrierSpins) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = (*(volatile int *) err == 0);
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// ------------------------------------------------------------------ tridiagonalisation
+struct TrdArgs {
+    double *A;      // n x n work matrix (trailing part updated after each panel)
+    double *Vh;     // n x n reflectors: column j holds v_j (v_j[j+1] = 1), zero elsewhere
+    double *Wp;     // n x TRD_NB panel W
+    double *d, *e, *tau;
+    double *col, *y;
+    double *part;   // [G] norms | [TRD_NG][2 TRD_NB] panel dots | [G] w.v
+    unsigned *bar;
+    int *err;
+    int n, p, cols, G;
+};
+
+__global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
+{
+    extern __shared__ double sv[];   // v of the current column, by absolute row
+    __shared__ double s_a2[TRD_NB], s_wv[TRD_NB], s_vv[TRD_NB], s_vj[TRD_NB], s_wj[TRD_NB];
+    __shared__ double s_red[33];
+    __shared__ double s_dw[TRD_THREADS / TRD_NB][TRD_NB], s_dv[TRD_THREADS / TRD_NB][TRD_NB];
+    __shared__ double s_tau, s_scal, s_beta;
+    const int n = a.n, p = a.p, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int gtid = blockIdx.x * TRD_THREADS + tid, GT = a.G * TRD_THREADS;
+    const int gw = blockIdx.x * (TRD_THREADS / 32) + wid, GW = a.G * (TRD_THREADS / 32);
+    double *part_n = a.part, *part_d = a.part + a.G, *part_w = part_d + TRD_NG * 2 * TRD_NB;
+    const int NG = min(a.G, TRD_NG);   // CTAs that form the panel dot products
+    const double *A = a.A;
+    const double *Vh = a.Vh;
+    // W of an earlier panel column cc (its final value: w + a2 v)
+    auto Wf = [&](int r, int cc) {
+        return a.Wp[(size_t) r * TRD_NB + cc] + s_a2[cc] * Vh[(size_t) r * n + p + cc];
+    };
+    for (int c = 0; c < a.cols; c++) {
+        const int j = p + c;
+        // ---- phase 1: column j (rows j..n-1) minus the panel's earlier corrections
+        if (tid < c) {
+            s_vj[tid] = Vh[(size_t) j * n + p + tid];
+            s_wj[tid] = Wf(j, tid);
+        }
+        __syncthreads();
+        double ss = 0.0;
+        for (int r = j + gtid; r < n; r += GT) {
+            double v = A[(size_t) r * n + j];
+            for (int cc = 0; cc < c; cc++) v -= Vh[(size_t) r * n + p + cc] * s_wj[cc] + Wf(r, cc) * s_vj[cc];
+            a.col[r] = v;
+            if (r >= j + 2) ss += v * v;
+        }
+        ss = block_sum_all<TRD_THREADS>(ss, s_red);
+        if (tid == 0) part_n[blockIdx.x] = ss;
+        if (!grid_barrier(a.bar, a.err, a.G)) return;
+        if (j == n - 1) {
+            if (gtid == 0) a.d[j] = a.col[j];
+            break;
+        }
+        // ---- phase 2: reflector (every CTA forms the same one), v, y = A v, panel dots
+        if (wid == 0) {
+            double s = 0.0;
+            for (int b = lane; b < a.G; b += 32) s += part_n[b];
+            s = warp_sum_bcast(s);
+            if (lane == 0) {
+                const double alpha = a.col[j + 1];
+                if (s == 0.0) {
+                    s_tau = 0.0;
+                    s_beta = alpha;
+                    s_scal = 0.0;
+                } else {
+                    const double nrm = sqrt(alpha * alpha + s);
+                    const double beta = alpha >= 0.0 ? -nrm : nrm;
+                    s_tau = (beta - alpha) / beta;
+                    s_beta = beta;
+                    s_scal = 1.0 / (alpha - beta);
+                }
+            }
+        }
+        __syncthreads();
+        const double tau = s_tau;
+        for (int r = j + 1 + tid; r < n; r += TRD_THREADS) sv[r] = (r == j + 1) ? 1.0 : a.col[r] * s_scal;
+        __syncthreads();
+        if (gtid == 0) {
+            a.d[j] = a.col[j];
+            a.e[j] = s_beta;
+            a.tau[j] = tau;
+        }
+        for (int r = j + 1 + gtid; r < n; r += GT) a.Vh[(size_t) r * n + j] = sv[r];
+        for (int r = j + 1 + gw; r < n; r += GW) {
+            const double *row = A + (size_t) r * n;
+            double acc = 0.0;
+            for (int c2 = j + 1 + lane; c2 < n; c2 += 32) acc += row[c2] * sv[c2];
+            acc = warp_sum_bcast(acc);
+            if (lane == 0) a.y[r] = acc;
+        }
+        if (c > 0 && (int) blockIdx.x < NG) {
+            const int m = n - j - 1, chunk = (m + NG - 1) / NG;
+            const int r0 = j + 1 + blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+            const int cc = tid % TRD_NB, rg = tid / TRD_NB;
+            double aw = 0.0, av = 0.0;
+            if (cc < c)
+                for (int r = r0 + rg; r < r1; r += TRD_THREADS / TRD_NB) {
+                    const double vr = sv[r];
+                    aw += Wf(r, cc) * vr;
+                    av += Vh[(size_t) r * n + p + cc] * vr;
+                }
+            s_dw[rg][cc] = aw;
+            s_dv[rg][cc] = av;
+            __syncthreads();
+            if (tid < TRD_NB) {
+                double sw = 0.0, sx = 0.0;
+                for (int g = 0; g < TRD_THREADS / TRD_NB; g++) {
+                    sw += s_dw[g][tid];
+                    sx += s_dv[g][tid];
+                }
+                part_d[blockIdx.x * 2 * TRD_NB + tid] = sw;
+                part_d[blockIdx.x * 2 * TRD_NB + TRD_NB + tid] = sx;
+            }
+        }
+        if (!grid_barrier(a.bar, a.err, a.G)) return;
+        // ---- phase 3: w = tau (y - V (W^T v) - W (V^T v)), partial w.v
+        if (tid < c) {
+            double sw = 0.0, sx = 0.0;
+            for (int b = 0; b < NG; b++) {
+                sw += part_d[b * 2 * TRD_NB + tid];
+                sx += part_d[b * 2 * TRD_NB + TRD_NB + tid];
+            }
+            s_wv[tid] = sw;
+            s_vv[tid] = sx;
+        }
+        __syncthreads();
+        double wd = 0.0;
+        for (int r = j + 1 + gtid; r < n; r += GT) {
+            double t = a.y[r];
+            for (int cc = 0; cc < c; cc++) t -= Vh[(size_t) r * n + p + cc] * s_wv[cc] + Wf(r, cc) * s_vv[cc];
+            const double w = tau * t;
+            a.Wp[(size_t) r * TRD_NB + c] = w;
+            wd += w * sv[r];
+        }
+        wd = block_sum_all<TRD_THREADS>(wd, s_red);
+        if (tid == 0) part_w[blockIdx.x] = wd;
+        if (!grid_barrier(a.bar, a.err, a.G)) return;
+        // ---- phase 4: w += a2 v with a2 = -tau/2 (w.v); kept as s_a2 and folded in lazily
+        if (wid == 0) {
+            double s = 0.0;
+            for (int b = lane; b < a.G; b += 32) s += part_w[b];
+            s = warp_sum_bcast(s);
+            if (lane == 0) s_a2[c] = -0.5 * tau * s;
+        }
+        __syncthreads();
+    }
+    // final W of the rows the trailing update reads
+    const int q = p + a.cols;
+    for (int r = q + gtid; r < n; r += GT)
+        for (int cc = 0; cc < a.cols; cc++) a.Wp[(size_t) r * TRD_NB + cc] = Wf(r, cc);
+}
+
+// T of the compact WY form of each panel: H_p ... H_(p+cols-1) = I - V T V^T,
+// T upper triangular (LAPACK dlarft, forward, columnwise). One CTA per panel.
+__global__ void __launch_bounds__(256) k_wy_tfactor(const double *Vh, const double *tau, double *Tf, int n)
+{
+    __shared__ double G[TRD_NB][TRD_NB + 1];
+    __shared__ double Vs[64][TRD_NB + 1];
+    __shared__ double T[TRD_NB][TRD_NB + 1];
+    const int P = blockIdx.x, p = P * TRD_NB, cols = min(TRD_NB, n - p), tid = threadIdx.x;
+    // G = V^T V over rows p+1..n-1: thread owns entries (a, b) = (tid / 32 + 8 i, tid % 32)
+    double acc[TRD_NB * TRD_NB / 256] = {};
+    for (int r0 = p + 1; r0 < n; r0 += 64) {
+        for (int l = tid; l < 64 * TRD_NB; l += 256) {
+            const int rr = l / TRD_NB, cc = l % TRD_NB, r = r0 + rr;
+            Vs[rr][cc] = (r < n && cc < cols) ? Vh[(size_t) r * n + p + cc] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < TRD_NB * TRD_NB / 256; i++) {
+            const int aa = tid / TRD_NB + (256 / TRD_NB) * i, bb = tid % TRD_NB;
+            double s = 0.0;
+            for (int rr = 0; rr < 64; rr++) s += Vs[rr][aa] * Vs[rr][bb];
+            acc[i] += s;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < TRD_NB * TRD_NB / 256; i++) G[tid / TRD_NB + (256 / TRD_NB) * i][tid % TRD_NB] = acc[i];
+    for (int l = tid; l < TRD_NB * TRD_NB; l += 256) T[l / TRD_NB][l % TRD_NB] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < cols; c++) {
+        const double tc = (p + c < n - 1) ? tau[p + c] : 0.0;
+        if (tid < c) {
+            double s = 0.0;
+            for (int l = tid; l < c; l++) s += T[tid][l] * G[l][c];
+            T[tid][c] = -tc * s;
+        }
+        if (tid == 0) T[c][c] = tc;
+        __syncthreads();
+    }
+    for (int l = tid; l < TRD_NB * TRD_NB; l += 256) Tf[(size_t) P * TRD_NB * TRD_NB + l] = T[l / TRD_NB][l % TRD_NB];
+}
+
+// ------------------------------------------------------------------ divide and conquer
+struct DcNodes {
+    const int *lo, *mid, *hi;
+    double *rho;      // per node, 2 |e[mid-1]|
+    int *kcnt, *rcnt; // per node: non-deflated count, rotation count
+};
+
+struct DcPos {        // per position of the tridiagonal (node-local arrays start at lo)
+    double *lam;      // eigenvalues of the solved pieces (ascending within each piece)
+    double *ds;       // sorted, deflation-modified d
+    double *dK, *zK;  // non-deflated d and z (compact)
+    double *lamb, *tau;  // root j = lamb[j] + tau[j], lamb the nearer pole
+    double *zh, *nrm;
+    double *lamnew;
+    int *perm;        // sorted position -> index into the concatenated children
+    int *keep, *defl; // sorted positions kept / deflated (compact)
+    int *rowinfo;     // sorted position -> kept index i, or -(deflated index + 1)
+    int *colsrc;      // output column -> secular root j (< k) or k + deflated index
+    int2 *rot;        // Givens rotations of the close pairs (rows pj, nj, sorted positions)
+    double2 *rotcs;   // their (C, S)
+};
+
+__global__ void k_dc_init(const double *d, const double *e, double *lam, double *Q, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // every boundary i|i+1 is the split point of exactly one merge: tear both sides
+    double v = d[i];
+    if (i + 1 < n) v -= fabs(e[i]);
+    if (i > 0) v -= fabs(e[i - 1]);
+    lam[i] = v;
+    Q[(size_t) i * n + i] = 1.0;
+}
+
+// Sorting of the two halves, z, the tolerance and the deflation scan. One CTA per node.
+__global__ void __launch_bounds__(512) k_dc_deflate(DcNodes nd, DcPos ps, const double *Q, const double *e, int n,
+                                                    int node0)
+{
+    extern __shared__ double dsm[];
+    __shared__ double s_red[33];
+    const int node = node0 + blockIdx.x;
+    const int lo = nd.lo[node], mid = nd.mid[node], hi = nd.hi[node];
+    const int m = hi - lo, m1 = mid - lo, m2 = hi - mid;
+    double *sd = dsm, *sz = dsm + m;
+    int *sp = (int *) (dsm + 2 * m);
+    const double rho_raw = e[mid - 1];
+    const double rho = 2.0 * fabs(rho_raw), sg = rho_raw >= 0.0 ? 1.0 : -1.0;
+    const double *L1 = ps.lam + lo, *L2 = ps.lam + mid;
+    const double rs2 = 1.0 / sqrt(2.0);
+    // every slot holds a valid index even if non-finite values make the merge below collide
+    for (int idx = threadIdx.x; idx < m; idx += blockDim.x) {
+        sd[idx] = 0.0;
+        sz[idx] = 0.0;
+        sp[idx] = idx;
+    }
+    __syncthreads();
+    double dmax = 0.0, zmax = 0.0;
+    for (int idx = threadIdx.x; idx < m; idx += blockDim.x) {
+        double x, zz;
+        int pos;
+        if (idx < m1) {
+            x = L1[idx];
+            zz = Q[(size_t) (mid - 1) * n + lo + idx];
+            int a = 0, b = m2;   // first L2 >= x
+            while (a < b) {
+                const int c = (a + b) >> 1;
+                if (L2[c] < x) a = c + 1; else b = c;
+            }
+            pos = idx + a;
+        } else {
+            const int i2 = idx - m1;
+            x = L2[i2];
+            zz = sg * Q[(size_t) mid * n + mid + i2];
+            int a = 0, b = m1;   // first L1 > x
+            while (a < b) {
+                const int c = (a + b) >> 1;
+                if (L1[c] <= x) a = c + 1; else b = c;
+            }
+            pos = i2 + a;
+        }
+        pos = min(max(pos, 0), m - 1);
+        zz *= rs2;
+        sd[pos] = x;
+        sz[pos] = zz;
+        sp[pos] = idx;
+        dmax = fmax(dmax, fabs(x));
+        zmax = fmax(zmax, fabs(zz));
+    }
+    dmax = block_max_all<512>(dmax, s_red);
+    zmax = block_max_all<512>(zmax, s_red);
+    const double tol = 8.0 * DBL_EPSILON * fmax(dmax, zmax);
+    int *keep = ps.keep + lo, *defl = ps.defl + lo, *rowinfo = ps.rowinfo + lo;
+    if (threadIdx.x == 0) {
+        int k = 0, nd_ = 0, nr = 0;
+        if (rho * zmax <= tol) {
+            for (int s = 0; s < m; s++) {
+                rowinfo[s] = -(nd_ + 1);
+                defl[nd_++] = s;
+            }
+        } else {
+            int pj = -1;
+            for (int s = 0; s < m; s++) {
+                if (rho * fabs(sz[s]) <= tol) {
+                    rowinfo[s] = -(nd_ + 1);
+                    defl[nd_++] = s;
+                    continue;
+                }
+                if (pj < 0) {
+                    pj = s;
+                    continue;
+                }
+                double S = sz[pj], C = sz[s];
+                const double tt = hypot(C, S), t = sd[s] - sd[pj];
+                C /= tt;
+                S = -S / tt;
+                if (fabs(t * C * S) <= tol) {
+                    sz[s] = tt;
+                    sz[pj] = 0.0;
+                    ps.rot[lo + nr] = make_int2(pj, s);
+                    ps.rotcs[lo + nr] = make_double2(C, S);
+                    nr++;
+                    const double dp = sd[pj] * C * C + sd[s] * S * S;
+                    sd[s] = sd[pj] * S * S + sd[s] * C * C;
+                    sd[pj] = dp;
+                    rowinfo[pj] = -(nd_ + 1);
+                    defl[nd_++] = pj;
+                    pj = s;
+                } else {
+                    rowinfo[pj] = k;
+                    keep[k++] = pj;
+                    pj = s;
+                }
+            }
+            if (pj >= 0) {
+                rowinfo[pj] = k;
+                keep[k++] = pj;
+            }
+        }
+        nd.kcnt[node] = k;
+        nd.rcnt[node] = nr;
+        nd.rho[node] = rho;
+    }
+    __syncthreads();
+    const int k = nd.kcnt[node];
+    for (int s = threadIdx.x; s < m; s += blockDim.x) {
+        ps.ds[lo + s] = sd[s];
+        ps.perm[lo + s] = sp[s];
+    }
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const int s = keep[i];
+        ps.dK[lo + i] = sd[s];
+        ps.zK[lo + i] = sz[s];
+    }
+}
+
+// Block tables: entry b = (node, first item) for the items [first, first + chunk) of that node.
+__device__ double secular_f(const double *sd, const double *sz, int k, double rho, double dorg, double t, int lane)
+{
+    double s = 0.0;
+    for (int i = lane; i < k; i += 32) s += sz[i] * sz[i] / ((sd[i] - dorg) - t);
+    return 1.0 + rho * warp_sum_bcast(s);
+}
+
+// Roots of 1 + rho sum_i z_i^2 / (d_i - lambda) = 0, one warp per root:
+// lambda_j = pole + tau, pole the nearer of d_j, d_(j+1), tau found by
+// bisection (geometric while the bracket spans more than a factor 4).
+__global__ void __launch_bounds__(256) k_dc_secular(DcNodes nd, DcPos ps, const int2 *tab)
+{
+    extern __shared__ double dsm[];
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], k = nd.kcnt[node];
+    if (tb.y >= k) return;
+    double *sd = dsm, *sz = dsm + k;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        sd[i] = ps.dK[lo + i];
+        sz[i] = ps.zK[lo + i];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, j = tb.y + (threadIdx.x >> 5);
+    if (j >= k) return;
+    const double rho = nd.rho[node];
+    int org;
+    double tau;
+    if (k == 1) {
+        org = 0;
+        tau = rho * sz[0] * sz[0];
+    } else {
+        bool pos;
+        double hi;
+        if (j == k - 1) {
+            double s = 0.0;
+            for (int i = lane; i < k; i += 32) s += sz[i] * sz[i];
+            hi = rho * warp_sum_bcast(s);
+            org = j;
+            pos = true;
+        } else {
+            const double delta = sd[j + 1] - sd[j];
+            const double fm = secular_f(sd, sz, k, rho, sd[j], 0.5 * delta, lane);
+            pos = fm > 0.0;
+            org = pos ? j : j + 1;
+            hi = 0.5 * delta;
+        }
+        const double sgn = pos ? 1.0 : -1.0, dorg = sd[org];
+        double lo_ = 0.0;
+        const double tiny = hi * 0x1p-200;
+        const double ft = secular_f(sd, sz, k, rho, dorg, sgn * tiny, lane);
+        if (pos ? (ft < 0.0) : (ft > 0.0)) lo_ = tiny;
+        for (int it = 0; it < 400; it++) {
+            const double midv = (lo_ > 0.0 && hi > 4.0 * lo_) ? sqrt(lo_ * hi) : 0.5 * (lo_ + hi);
+            if (!(midv > lo_ && midv < hi)) break;
+            const double fm = secular_f(sd, sz, k, rho, dorg, sgn * midv, lane);
+            if (pos ? (fm < 0.0) : (fm > 0.0)) lo_ = midv; else hi = midv;
+        }
+        tau = sgn * 0.5 * (lo_ + hi);
+    }
+    if (lane == 0) {
+        ps.lamb[lo + j] = sd[org];
+        ps.tau[lo + j] = tau;
+    }
+}
+
+// z recomputed from the roots (Gu-Eisenstat): zh_i^2 = -(d_i - l_i) prod_(j != i) (d_i - l_j) / (d_i - d_j).
+__global__ void __launch_bounds__(256) k_dc_zhat(DcNodes nd, DcPos ps, const int2 *tab)
+{
+    extern __shared__ double dsm[];
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], k = nd.kcnt[node];
+    if (tb.y >= k) return;
+    double *sd = dsm, *sl = dsm + k, *st = dsm + 2 * k;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        sd[i] = ps.dK[lo + i];
+        sl[i] = ps.lamb[lo + i];
+        st[i] = ps.tau[lo + i];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, i = tb.y + (threadIdx.x >> 5);
+    if (i >= k) return;
+    const double di = sd[i];
+    double pr = 1.0;
+    for (int j = lane; j < k; j += 32) {
+        const double del = (di - sl[j]) - st[j];
+        pr *= (j == i) ? del : del / (di - sd[j]);
+    }
+    pr = warp_prod_bcast(pr);
+    if (lane == 0) ps.zh[lo + i] = copysign(sqrt(fmax(-pr, 0.0)), ps.zK[lo + i]);
+}
+
+// Norm of each secular eigenvector u_j(i) = zh_i / (d_i - l_j).
+__global__ void __launch_bounds__(256) k_dc_norms(DcNodes nd, DcPos ps, const int2 *tab)
+{
+    extern __shared__ double dsm[];
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], k = nd.kcnt[node];
+    if (tb.y >= k) return;
+    double *sd = dsm, *sz = dsm + k;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        sd[i] = ps.dK[lo + i];
+        sz[i] = ps.zh[lo + i];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, j = tb.y + (threadIdx.x >> 5);
+    if (j >= k) return;
+    const double lb = ps.lamb[lo + j], tj = ps.tau[lo + j];
+    double s = 0.0;
+    for (int i = lane; i < k; i += 32) {
+        const double u = sz[i] / ((sd[i] - lb) - tj);
+        s += u * u;
+    }
+    s = warp_sum_bcast(s);
+    if (lane == 0) ps.nrm[lo + j] = sqrt(s);
+}
+
+// Output order of the node's eigenvalues (ascending; ties by source index) by rank counting.
+__global__ void __launch_bounds__(DC_CHUNK) k_dc_order(DcNodes nd, DcPos ps, const int2 *tab)
+{
+    extern __shared__ double dsm[];
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], m = nd.hi[node] - lo, k = nd.kcnt[node];
+    double *sv = dsm;
+    for (int a = threadIdx.x; a < m; a += blockDim.x)
+        sv[a] = (a < k) ? ps.lamb[lo + a] + ps.tau[lo + a] : ps.ds[lo + ps.defl[lo + a - k]];
+    __syncthreads();
+    const int a = tb.y + threadIdx.x;
+    if (a >= m) return;
+    const double x = sv[a];
+    int r = 0;
+    for (int b = 0; b < m; b++) {
+        const double y = sv[b];
+        r += (y < x || (y == x && b < a)) ? 1 : 0;
+    }
+    r = min(r, m - 1);
+    ps.lamnew[lo + r] = x;
+    ps.colsrc[lo + r] = a;
+}
+
+// The merge's eigenvector matrix in sorted-row order, one warp per row:
+// column c = secular vector j (normalised) or the unit vector of a deflated position.
+__global__ void __launch_bounds__(256) k_dc_build(DcNodes nd, DcPos ps, const int2 *tab, double *Us, int n)
+{
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], m = nd.hi[node] - lo, k = nd.kcnt[node];
+    const int lane = threadIdx.x & 31, s = tb.y + (threadIdx.x >> 5);
+    if (s >= m) return;
+    const int info = ps.rowinfo[lo + s];
+    const double di = info >= 0 ? ps.dK[lo + info] : 0.0, zi = info >= 0 ? ps.zh[lo + info] : 0.0;
+    double *row = Us + (size_t) (lo + s) * n + lo;
+    for (int c = lane; c < m; c += 32) {
+        const int src = ps.colsrc[lo + c];
+        double v;
+        if (src >= 0 && src < k) v = info >= 0 ? zi / ((di - ps.lamb[lo + src]) - ps.tau[lo + src]) / ps.nrm[lo + src] : 0.0;
+        else v = (info < 0 && -(info + 1) == src - k) ? 1.0 : 0.0;
+        row[c] = v;
+    }
+}
+
+// Givens rotations of the deflation, applied to the rows of Us in reverse order; a thread per column.
+__global__ void __launch_bounds__(DC_CHUNK) k_dc_rotate(DcNodes nd, DcPos ps, const int2 *tab, double *Us, int n)
+{
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], m = nd.hi[node] - lo, nr = nd.rcnt[node];
+    const int c = tb.y + threadIdx.x;
+    if (nr == 0 || c >= m) return;
+    double *U = Us + (size_t) lo * n + lo + c;
+    for (int r = nr - 1; r >= 0; r--) {
+        const int2 pr = ps.rot[lo + r];
+        const double2 cs = ps.rotcs[lo + r];
+        const double x = U[(size_t) pr.x * n], y = U[(size_t) pr.y * n];
+        U[(size_t) pr.x * n] = cs.x * x - cs.y * y;
+        U[(size_t) pr.y * n] = cs.y * x + cs.x * y;
+    }
+}
+
+// Qg = the node's block of Q with its columns in sorted order.
+__global__ void __launch_bounds__(256) k_dc_gather(DcNodes nd, DcPos ps, const int2 *tab, const double *Q, double *Qg,
+                                                   int n)
+{
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], m = nd.hi[node] - lo;
+    const int lane = threadIdx.x & 31, r = tb.y + (threadIdx.x >> 5);
+    if (r >= m) return;
+    const double *src = Q + (size_t) (lo + r) * n + lo;
+    double *dst = Qg + (size_t) (lo + r) * n + lo;
+    for (int s = lane; s < m; s += 32) dst[s] = src[ps.perm[lo + s]];
+}
+
+__global__ void k_dc_commit_lam(DcNodes nd, DcPos ps, const int2 *tab)
+{
+    const int2 tb = tab[blockIdx.x];
+    const int node = tb.x, lo = nd.lo[node], m = nd.hi[node] - lo;
+    const int a = tb.y + threadIdx.x;
+    if (a < m) ps.lam[lo + a] = ps.lamnew[lo + a];
+}
+
+// Q(node block) = Qg(node block) Us(node block), 64 x 64 tiles on the FP64 tensor cores.
+__global__ void __launch_bounds__(128) k_dc_gemm(DcNodes nd, const int4 *tiles, const double *Qg, const double *Us,
+                                                 double *Q, int n)
+{
+    const int4 t = tiles[blockIdx.x];
+    const int lo = nd.lo[t.x], m = nd.hi[t.x] - lo;
+    const size_t off = (size_t) lo * n + lo;
+    dgemm_tile_dmma64<false, false>(m, m, m, 1.0, Qg + off, n, Us + off, n, 0.0, Q + off, n, t.y * 64, t.z * 64);
+}
+
+__global__ void k_transpose(const double *in, double *out, int n)
+{
+    __shared__ double tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int i = by + r, j = bx + threadIdx.x;
+        if (i < n && j < n) tile[r][threadIdx.x] = in[(size_t) i * n + j];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int i = bx + r, j = by + threadIdx.x;
+        if (i < n && j < n) out[(size_t) i * n + j] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void k_copy_scalar_eig(const double *A, double *w, double *V)
+{
+    w[0] = A[0];
+    V[0] = 1.0;
+}
+
+// ------------------------------------------------------------------ small Cholesky-QR helpers
+// Lower Cholesky factor of a symmetric positive definite o x o matrix, in place
+// (row-major, lower triangle), left-looking, one warp per row; a non-positive
+// or non-finite pivot sets *fail.
+__global__ void __launch_bounds__(1024) k_potrf_lower(double *G, int o, int *fail)
+{
+    __shared__ double s_piv;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = 0; j < o; j++) {
+        if (wid == 0) {
+            double s = 0.0;
+            for (int c = lane; c < j; c += 32) s += G[(size_t) j * o + c] * G[(size_t) j * o + c];
+            s = warp_sum_bcast(s);
+            if (lane == 0) {
+                const double ajj = G[(size_t) j * o + j] - s;
+                if (!(ajj > 0.0) || !isfinite(ajj)) *fail = 1;
+                const double l = (ajj > 0.0 && isfinite(ajj)) ? sqrt(ajj) : 1.0;
+                G[(size_t) j * o + j] = l;
+                s_piv = l;
+            }
+        }
+        __syncthreads();
+        const double rinv = 1.0 / s_piv;
+        for (int r = j + 1 + wid; r < o; r += nw) {
+            double s = 0.0;
+            for (int c = lane; c < j; c += 32) s += G[(size_t) r * o + c] * G[(size_t) j * o + c];
+            s = warp_sum_bcast(s);
+            if (lane == 0) G[(size_t) r * o + j] = (G[(size_t) r * o + j] - s) * rinv;
+        }
+        __syncthreads();
+    }
+}
+
+// Xc = (L^-1)^T stored row-major (column j of L^-1 in row j of Xc), upper part
+// of L^-1 zero; one thread per column of the inverse.
+__global__ void k_trtri_lower(const double *L, double *Xc, int o)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= o) return;
+    double *x = Xc + (size_t) j * o;
+    for (int i = 0; i < j; i++) x[i] = 0.0;
+    x[j] = 1.0 / L[(size_t) j * o + j];
+    for (int i = j + 1; i < o; i++) {
+        double s = 0.0;
+        for (int kk = j; kk < i; kk++) s += L[(size_t) i * o + kk] * x[kk];
+        x[i] = -s / L[(size_t) i * o + i];
+    }
+}
+
+__global__ void k_hash_fill(double *A, size_t n)
+{
+    size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long h = (i + 1) * 0x9E3779B97F4A7C15ULL;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ULL;
+    h ^= h >> 29;
+    A[i] = (double) (h >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+struct Eig {
+    int n = 0, G = 1, npanels = 0;
+    double *A = nullptr, *Vh = nullptr, *Wp = nullptr, *d = nullptr, *e = nullptr, *tau = nullptr, *col = nullptr,
+           *y = nullptr, *part = nullptr, *Tf = nullptr, *Y = nullptr, *Y2 = nullptr;
+    unsigned *bar = nullptr;
+    int *err = nullptr;
+    // divide and conquer
+    double *Q = nullptr, *Us = nullptr;   // Qg reuses A
+    DcNodes nodes{};
+    DcPos pos{};
+    int *node_mem = nullptr;
+    double *node_rho = nullptr;
+    int2 *tab_c = nullptr, *tab_w = nullptr;
+    int4 *tiles = nullptr;
+    struct Level {
+        int node0, nnodes, maxm, c0, nc, w0, nw, t0, nt;
+    };
+    std::vector<Level> levels;
+    // Cholesky-QR of dominant_subspace
+    double *Gx = nullptr;
+    int go = 0;
+    int *acc = nullptr;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+template <typename T>
+bool ealloc(Eig *e, T **p, size_t count)
+{
+    void *q = nullptr;
+    if (cudaMalloc(&q, sizeof(T) * (count ? count : 1)) != cudaSuccess) return false;
+    e->allocs.push_back(q);
+    *p = (T *) q;
+    return true;
+}
+
+bool dc_plan(Eig *E)
+{
+    const int n = E->n;
+    struct Node {
+        int dep, lo, mid, hi;
+    };
+    std::vector<Node> nodes;
+    std::vector<Node> stack{{0, 0, 0, n}};
+    while (!stack.empty()) {
+        Node x = stack.back();
+        stack.pop_back();
+        if (x.hi - x.lo <= 1) continue;
+        x.mid = x.lo + (x.hi - x.lo) / 2;
+        nodes.push_back(x);
+        stack.push_back({x.dep + 1, x.lo, 0, x.mid});
+        stack.push_back({x.dep + 1, x.mid, 0, x.hi});
+    }
+    std::stable_sort(nodes.begin(), nodes.end(), [](const Node &a, const Node &b) { return a.dep > b.dep; });
+    std::vector<int> lo, mid, hi;
+    std::vector<int2> tc, tw;
+    std::vector<int4> tt;
+    E->levels.clear();
+    size_t i = 0;
+    while (i < nodes.size()) {
+        Eig::Level L{};
+        L.node0 = (int) i;
+        L.c0 = (int) tc.size();
+        L.w0 = (int) tw.size();
+        L.t0 = (int) tt.size();
+        const int dep = nodes[i].dep;
+        for (; i < nodes.size() && nodes[i].dep == dep; i++) {
+            const int id = (int) i, m = nodes[i].hi - nodes[i].lo;
+            lo.push_back(nodes[i].lo);
+            mid.push_back(nodes[i].mid);
+            hi.push_back(nodes[i].hi);
+            L.maxm = std::max(L.maxm, m);
+            for (int f = 0; f < m; f += DC_CHUNK) tc.push_back(make_int2(id, f));
+            for (int f = 0; f < m; f += DC_WCHUNK) tw.push_back(make_int2(id, f));
+            const int nt = (m + 63) / 64;
+            for (int a = 0; a < nt; a++)
+                for (int b = 0; b < nt; b++) tt.push_back(make_int4(id, a, b, 0));
+        }
+        L.nnodes = (int) i - L.node0;
+        L.nc = (int) tc.size() - L.c0;
+        L.nw = (int) tw.size() - L.w0;
+        L.nt = (int) tt.size() - L.t0;
+        E->levels.push_back(L);
+    }
+    const size_t nn = nodes.size();
+    if (!ealloc(E, &E->node_mem, 5 * nn) || !ealloc(E, &E->node_rho, nn)) return false;
+    std::vector<int> packed(5 * nn, 0);
+    std::copy(lo.begin(), lo.end(), packed.begin());
+    std::copy(mid.begin(), mid.end(), packed.begin() + nn);
+    std::copy(hi.begin(), hi.end(), packed.begin() + 2 * nn);
+    if (nn && cudaMemcpy(E->node_mem, packed.data(), sizeof(int) * 5 * nn, cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    E->nodes.lo = E->node_mem;
+    E->nodes.mid = E->node_mem + nn;
+    E->nodes.hi = E->node_mem + 2 * nn;
+    E->nodes.kcnt = E->node_mem + 3 * nn;
+    E->nodes.rcnt = E->node_mem + 4 * nn;
+    E->nodes.rho = E->node_rho;
+    if (!ealloc(E, &E->tab_c, tc.size()) || !ealloc(E, &E->tab_w, tw.size()) || !ealloc(E, &E->tiles, tt.size()))
+        return false;
+    if (!tc.empty() && cudaMemcpy(E->tab_c, tc.data(), sizeof(int2) * tc.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    if (!tw.empty() && cudaMemcpy(E->tab_w, tw.data(), sizeof(int2) * tw.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    if (!tt.empty() && cudaMemcpy(E->tiles, tt.data(), sizeof(int4) * tt.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    return true;
+}
+
+bool smem_optin()
+{
+    static bool done = false;
+    if (done) return true;
+    const int mx = (int) kMaxDynSmem;
+    if (cudaFuncSetAttribute(k_sytrd_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024 + 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dc_deflate, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dc_secular, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dc_zhat, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dc_norms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dc_order, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
+        return false;
+    done = true;
+    return true;
+}
+
+}  // namespace
+
+Eig *eig_create(int n, cudaStream_t s)
+{
+    (void) s;
+    if (n < 1 || n > EIG_MAX_N) return nullptr;
+    if (!smem_optin()) return nullptr;
+    Eig *E = new Eig();
+    E->n = n;
+    int dev = 0, nsm = 1, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const size_t dyn = sizeof(double) * (size_t) n;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sytrd_panel, TRD_THREADS, dyn);
+    E->G = std::max(1, std::min({nsm * std::max(per, 1), nsm, (n + 31) / 32}));
+    E->npanels = (n + TRD_NB - 1) / TRD_NB;
+    const size_t nn = (size_t) n * n;
+    bool ok = ealloc(E, &E->A, nn) && ealloc(E, &E->Vh, nn) && ealloc(E, &E->Q, nn) && ealloc(E, &E->Us, nn) &&
+              ealloc(E, &E->Wp, (size_t) n * TRD_NB) && ealloc(E, &E->Y, (size_t) n * TRD_NB) &&
+              ealloc(E, &E->Y2, (size_t) n * TRD_NB) && ealloc(E, &E->d, n) && ealloc(E, &E->e, n) &&
+              ealloc(E, &E->tau, n) && ealloc(E, &E->col, n) && ealloc(E, &E->y, n) &&
+              ealloc(E, &E->part, 2 * (size_t) E->G + TRD_NG * 2 * TRD_NB) &&
+              ealloc(E, &E->Tf, (size_t) E->npanels * TRD_NB * TRD_NB) && ealloc(E, &E->bar, 2) &&
+              ealloc(E, &E->err, 1) && ealloc(E, &E->acc, 1);
+    DcPos &P = E->pos;
+    ok = ok && ealloc(E, &P.lam, n) && ealloc(E, &P.ds, n) && ealloc(E, &P.dK, n) && ealloc(E, &P.zK, n) &&
+         ealloc(E, &P.lamb, n) && ealloc(E, &P.tau, n) && ealloc(E, &P.zh, n) && ealloc(E, &P.nrm, n) &&
+         ealloc(E, &P.lamnew, n) && ealloc(E, &P.perm, n) && ealloc(E, &P.keep, n) && ealloc(E, &P.defl, n) &&
+         ealloc(E, &P.rowinfo, n) && ealloc(E, &P.colsrc, n) && ealloc(E, &P.rot, n) && ealloc(E, &P.rotcs, n);
+    ok = ok && dc_plan(E);
+    if (!ok) {
+        eig_destroy(E);
+        return nullptr;
+    }
+    cudaMemset(P.colsrc, 0, sizeof(int) * n);
+    cudaMemset(P.perm, 0, sizeof(int) * n);
+    cudaMemset(E->bar, 0, 2 * sizeof(unsigned));
+    cudaMemset(E->err, 0, sizeof(int));
+    if (cudaGetLastError() != cudaSuccess) {
+        eig_destroy(E);
+        return nullptr;
+    }
+    return E;
+}
+
+void eig_destroy(Eig *e)
+{
+    if (!e) return;
+    for (void *p : e->allocs) cudaFree(p);
+    delete e;
+}
+
+int eig_error(Eig *e)
+{
+    int v = 0;
+    if (!e) return ERR_STATE;
+    if (cudaMemcpy(&v, e->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_CUDA;
+    return v ? ERR_CUDA : OK;
+}
+
+namespace {
+
+int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
+{
+    const int n = E->n;
+    const size_t nn = (size_t) n * n;
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(E->A, d_A, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->Vh, 0, sizeof(double) * nn, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->tau, 0, sizeof(double) * n, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->e, 0, sizeof(double) * n, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->bar, 0, 2 * sizeof(unsigned), s));
+    const size_t dyn = sizeof(double) * (size_t) n;
+    for (int P = 0; P < E->npanels; P++) {
+        TrdArgs a;
+        a.A = E->A;
+        a.Vh = E->Vh;
+        a.Wp = E->Wp;
+        a.d = E->d;
+        a.e = E->e;
+        a.tau = E->tau;
+        a.col = E->col;
+        a.y = E->y;
+        a.part = E->part;
+        a.bar = E->bar;
+        a.err = E->err;
+        a.n = n;
+        a.p = P * TRD_NB;
+        a.cols = std::min(TRD_NB, n - a.p);
+        a.G = E->G;
+        void *args[] = {&a};
+        g_launches++;
+        TSCF_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *) k_sytrd_panel, dim3(E->G), dim3(TRD_THREADS), args,
+                                                    dyn, s));
+        const int q = a.p + a.cols, mt = n - q;
+        if (mt > 0) {
+            // A22 -= V W^T + W V^T
+            const double *V = E->Vh + (size_t) q * n + a.p;
+            const double *W = E->Wp + (size_t) q * TRD_NB;
+            double *A22 = E->A + (size_t) q * n + q;
+            dgemm_untuned(false, true, mt, mt, a.cols, -1.0, V, n, W, TRD_NB, 1.0, A22, n, s);
+            dgemm_untuned(false, true, mt, mt, a.cols, -1.0, W, TRD_NB, V, n, 1.0, A22, n, s);
+        }
+    }
+    return cuda_launch_rc("tridiagonalisation");
+}
+
+int divide_conquer(Eig *E, cudaStream_t s)
+{
+    const int n = E->n;
+    const size_t nn = (size_t) n * n;
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->Q, 0, sizeof(double) * nn, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->Us, 0, sizeof(double) * nn, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->A, 0, sizeof(double) * nn, s));   // Qg
+    g_launches++;
+    k_dc_init<<<(n + 255) / 256, 256, 0, s>>>(E->d, E->e, E->pos.lam, E->Q, n);
+    double *Qg = E->A;
+    for (const auto &L : E->levels) {
+        const size_t m = (size_t) L.maxm;
+        k_dc_deflate<<<L.nnodes, 512, 20 * m, s>>>(E->nodes, E->pos, E->Q, E->e, n, L.node0);
+        k_dc_secular<<<L.nw, 256, 16 * m, s>>>(E->nodes, E->pos, E->tab_w + L.w0);
+        k_dc_zhat<<<L.nw, 256, 24 * m, s>>>(E->nodes, E->pos, E->tab_w + L.w0);
+        k_dc_norms<<<L.nw, 256, 16 * m, s>>>(E->nodes, E->pos, E->tab_w + L.w0);
+        k_dc_order<<<L.nc, DC_CHUNK, 8 * m, s>>>(E->nodes, E->pos, E->tab_c + L.c0);
+        k_dc_build<<<L.nw, 256, 0, s>>>(E->nodes, E->pos, E->tab_w + L.w0, E->Us, n);
+        k_dc_rotate<<<L.nc, DC_CHUNK, 0, s>>>(E->nodes, E->pos, E->tab_c + L.c0, E->Us, n);
+        k_dc_gather<<<L.nw, 256, 0, s>>>(E->nodes, E->pos, E->tab_w + L.w0, E->Q, Qg, n);
+        k_dc_commit_lam<<<L.nc, DC_CHUNK, 0, s>>>(E->nodes, E->pos, E->tab_c + L.c0);
+        k_dc_gemm<<<L.nt, 128, 0, s>>>(E->nodes, E->tiles + L.t0, Qg, E->Us, E->Q, n);
+        g_launches += 10;
+    }
+    return cuda_launch_rc("divide and conquer");
+}
+
+int back_transform(Eig *E, double *d_V, cudaStream_t s)
+{
+    const int n = E->n;
+    g_launches += 2;
+    k_wy_tfactor<<<E->npanels, 256, 0, s>>>(E->Vh, E->tau, E->Tf, n);
+    k_transpose<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(E->Q, d_V, n);
+    for (int P = E->npanels - 1; P >= 0; P--) {
+        const int p = P * TRD_NB, cols = std::min(TRD_NB, n - p), mv = n - p - 1;
+        if (mv <= 0) continue;
+        const double *V = E->Vh + (size_t) (p + 1) * n + p;
+        // Y = Vout[:, p+1:] V;  Y2 = Y T^T;  Vout[:, p+1:] -= Y2 V^T
+        dgemm_untuned(false, false, n, cols, mv, 1.0, d_V + p + 1, n, V, n, 0.0, E->Y, TRD_NB, s);
+        dgemm_untuned(false, true, n, cols, cols, 1.0, E->Y, TRD_NB, E->Tf + (size_t) P * TRD_NB * TRD_NB, TRD_NB, 0.0,
+                      E->Y2, TRD_NB, s);
+        dgemm_untuned(false, true, n, mv, cols, -1.0, E->Y2, TRD_NB, V, n, 1.0, d_V + p + 1, n, s);
+    }
+    return cuda_launch_rc("back-transformation");
+}
+
+}  // namespace
+
+// Eigenvalues ascending into d_w, eigenvectors as rows of d_V (V[k*n + i] =
+// entry i of eigenvector k). d_V may alias d_A.
+int eig_run(Eig *E, const double *d_A, double *d_w, double *d_V, cudaStream_t s)
+{
+    if (!E) return ERR_STATE;
+    const int n = E->n;
+    if (n == 1) {
+        g_launches++;
+        k_copy_scalar_eig<<<1, 1, 0, s>>>(d_A, d_w, d_V);
+        return cuda_launch_rc("eigensolve (n = 1)");
+    }
+    RC_(tridiagonalize(E, d_A, s));
+    RC_(divide_conquer(E, s));
+    RC_(back_transform(E, d_V, s));
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(d_w, E->pos.lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return OK;
+}
+
+// ------------------------------------------------------------------ dominant subspace
+// Rows of U (o x n) become an orthonormal basis of the dominant o-dimensional
+// invariant subspace of a symmetric n x n matrix M, by subspace iteration from
+// a fixed pseudo-random start: W <- W M, orthonormalised every kOrthoEvery
+// products and at the end by Cholesky-QR (G = W W^T = L L^T, W <- L^-1 W,
+// with L^-1 from a triangular inverse so the update is one GEMM), the last one
+// applied twice for orthogonality to rounding. For a matrix close to a rank-o
+// projector (a predicted density in the orthogonal basis) each product
+// shrinks the other directions by the ratio of the (o+1)-th to the o-th
+// eigenvalue, while the kept directions, with eigenvalues near 1, stay well
+// conditioned between orthonormalisations.
+namespace {
+const int kOrthoEvery = 3;
+
+// W <- L^-1 U for G = U U^T = L L^T (U, W: o x n row-major; G: o x o scratch).
+// A failed factorisation sets E->acc on the device.
+void chol_qr(Eig *E, const double *U, double *W, double *G, int n, int o, cudaStream_t s)
+{
+    dgemm(false, true, o, o, n, 1.0, U, n, U, n, 0.0, G, o, s);   // G = U U^T
+    k_potrf_lower<<<1, 1024, 0, s>>>(G, o, E->acc);
+    k_trtri_lower<<<(o + 127) / 128, 128, 0, s>>>(G, E->Gx, o);
+    g_launches += 2;
+    // row-major Gx is (L^-1)^T, so W = Gx^T U
+    dgemm(true, false, o, n, o, 1.0, E->Gx, o, U, n, 0.0, W, n, s);
+}
+}  // namespace
+
+int dominant_subspace(Eig *E, const double *d_M, double *d_U, double *d_W, double *d_G, int n, int o, int iters,
+                      cudaStream_t s)
+{
+    if (!E || o <= 0 || o > n || iters < 1) return ERR_INPUT;
+    if (E->go < o) {
+        if (E->Gx) {
+            cudaFree(E->Gx);
+            E->allocs.erase(std::find(E->allocs.begin(), E->allocs.end(), (void *) E->Gx));
+            E->Gx = nullptr;
+        }
+        if (!ealloc(E, &E->Gx, (size_t) o * o)) return ERR_ALLOC;
+        E->go = o;
+    }
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->acc, 0, sizeof(int), s));
+    const size_t on = (size_t) o * n;
+    double *cur = d_W, *nxt = d_U;   // cur: the basis (or an unorthonormalised product of it)
+    k_hash_fill<<<(unsigned) ((on + 255) / 256), 256, 0, s>>>(cur, on);
+    g_launches++;
+    for (int it = 1; it <= iters; it++) {
+        dgemm(false, false, o, n, n, 1.0, cur, n, d_M, n, 0.0, nxt, n, s);   // nxt = cur M (M symmetric)
+        if (it % kOrthoEvery == 0 || it == iters) chol_qr(E, nxt, cur, d_G, n, o, s);
+        else std::swap(cur, nxt);
+    }
+    chol_qr(E, cur, nxt, d_G, n, o, s);   // second pass: orthonormal to rounding
+    if (nxt != d_U) TSCF_CUDA_CHECK(cudaMemcpyAsync(d_U, nxt, sizeof(double) * on, cudaMemcpyDeviceToDevice, s));
+    int acc = 0;
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(&acc, E->acc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TSCF_CUDA_CHECK(cudaStreamSynchronize(s));
+    return acc == 0 ? OK : ERR_NUMERIC;
+}
+
+}  // namespace tscf

@@ -1,11 +1,10 @@
-// Dense FP64 building blocks for the SCF: a tiled DGEMM, the symmetric
-// eigensolver wrapper (cuSOLVER syevd), inverse square roots from
-// eigenpairs (TinySCF.c:58-76, build_DF_tensor.c:205-237), and the pivoted
-// Cholesky of the initial guess (TinySCF.c:282-322, LAPACK dpstf2 semantics).
+// Dense FP64 building blocks for the SCF: a tiled DGEMM, inverse square
+// roots from eigenpairs (TinySCF.c:58-76, build_DF_tensor.c:205-237), and the
+// pivoted Cholesky of the initial guess (TinySCF.c:282-322, LAPACK dpstf2
+// semantics). The eigensolver itself is in eigh.cu.
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
-#include <cusolverDn.h>
 
 #include <utility>
 #include <vector>
@@ -239,178 +238,26 @@ void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
     dgemm_variant(v, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
 
-// ------------------------------------------------------------------ eigensolver
-struct Eig {
-    int n;
-    cusolverDnHandle_t h;
-    double *work;
-    int lwork;
-    int *info;
-    // dominant_subspace: potrf and trtri workspaces for po x po, failure flag
-    double *pwork = nullptr;
-    void *twork = nullptr;
-    size_t tdev = 0;
-    std::vector<char> thost;
-    int plwork = 0, po = 0;
-    int *acc = nullptr;
-};
-
-Eig *eig_create(int n, cudaStream_t s)
+// Tile shape from the call shape alone, for the many distinct shapes of the
+// eigensolver's panel updates (tuning each one would cost more than it saves):
+// the K-split tile for narrow outputs with a long K, the 128 x 128 DMMA tile
+// for large outputs, the 64 x 64 DMMA tile otherwise.
+void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda, const double *B,
+                   int ldb, double beta, double *C, int ldc, cudaStream_t s)
 {
-    Eig *e = new Eig();
-    e->n = n;
-    if (cusolverDnCreate(&e->h) != CUSOLVER_STATUS_SUCCESS) { delete e; return nullptr; }
-    cusolverDnSetStream(e->h, s);
-    int lw = 0;
-    if (cusolverDnDsyevd_bufferSize(e->h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, nullptr, n, nullptr,
-                                    &lw) != CUSOLVER_STATUS_SUCCESS) {
-        cusolverDnDestroy(e->h);
-        delete e;
-        return nullptr;
-    }
-    e->lwork = lw;
-    if (cudaMalloc(&e->work, sizeof(double) * (size_t) (lw > 0 ? lw : 1)) != cudaSuccess ||
-        cudaMalloc(&e->info, sizeof(int)) != cudaSuccess) {
-        cusolverDnDestroy(e->h);
-        delete e;
-        return nullptr;
-    }
-    return e;
+    if (m <= 0 || n <= 0) return;
+    int v = 4;
+    if ((m <= 64 || n <= 64) && k >= 128) v = 5;
+    else if ((double) m * n >= 4.0 * 148 * 128 * 128) v = 3;
+    dgemm_variant(v, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
 
-void eig_destroy(Eig *e)
+int cuda_launch_rc(const char *what)
 {
-    if (!e) return;
-    if (e->pwork) cudaFree(e->pwork);
-    if (e->twork) cudaFree(e->twork);
-    if (e->acc) cudaFree(e->acc);
-    cudaFree(e->work);
-    cudaFree(e->info);
-    cusolverDnDestroy(e->h);
-    delete e;
-}
-
-// A symmetric, so row- and column-major agree; cuSOLVER leaves the eigenvectors
-// in the columns of its column-major output, i.e. in the rows of our row-major view.
-int eig_run(Eig *e, const double *d_A, double *d_w, double *d_V, cudaStream_t s)
-{
-    if (d_V != d_A) cudaMemcpyAsync(d_V, d_A, sizeof(double) * (size_t) e->n * e->n, cudaMemcpyDeviceToDevice, s);
-    cusolverDnSetStream(e->h, s);
-    cusolverStatus_t st = cusolverDnDsyevd(e->h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, e->n, d_V, e->n,
-                                           d_w, e->work, e->lwork, e->info);
-    return st == CUSOLVER_STATUS_SUCCESS ? OK : ERR_NUMERIC;
-}
-
-// ------------------------------------------------------------------ dominant subspace
-// Rows of U (o x n) become an orthonormal basis of the dominant o-dimensional
-// invariant subspace of a symmetric n x n matrix M, by subspace iteration from
-// a fixed pseudo-random start: W <- W M, orthonormalised every kOrthoEvery
-// products and at the end by Cholesky-QR (G = W W^T = L L^T, W <- L^-1 W,
-// with L^-1 from a triangular inverse so the update is one GEMM), the last one
-// applied twice for orthogonality to rounding. For a matrix close to a rank-o
-// projector (a predicted density in the orthogonal basis) each product
-// shrinks the other directions by the ratio of the (o+1)-th to the o-th
-// eigenvalue, while the kept directions, with eigenvalues near 1, stay well
-// conditioned between orthonormalisations.
-__global__ void k_hash_fill(double *A, size_t n)
-{
-    size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    unsigned long long h = (i + 1) * 0x9E3779B97F4A7C15ULL;
-    h ^= h >> 31;
-    h *= 0xBF58476D1CE4E5B9ULL;
-    h ^= h >> 29;
-    A[i] = (double) (h >> 11) * (1.0 / 9007199254740992.0) - 0.5;
-}
-
-// Zero the part of the column-major o x o array G above the diagonal, so that
-// read row-major it is the lower triangular factor's transpose and nothing else.
-__global__ void k_zero_upper_cm(double *G, int o)
-{
-    const size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (size_t) o * o) return;
-    const int col = (int) (idx / o), row = (int) (idx % o);
-    if (row < col) G[idx] = 0.0;
-}
-
-// acc |= (info != 0): failures of the factorisations of one call, read once at the end
-__global__ void k_or_info(const int *info, int *acc)
-{
-    if (*info != 0) *acc = 1;
-}
-
-namespace {
-const int kOrthoEvery = 3;
-
-// W <- L^-1 U for G = U U^T = L L^T (U, W: o x n row-major; G: o x o scratch).
-// A failed factorisation sets e->acc on the device.
-int chol_qr(Eig *e, const double *U, double *W, double *G, int n, int o, cudaStream_t s)
-{
-    dgemm(false, true, o, o, n, 1.0, U, n, U, n, 0.0, G, o, s);   // G = U U^T
-    if (cusolverDnDpotrf(e->h, CUBLAS_FILL_MODE_LOWER, o, G, o, e->pwork, e->plwork, e->info) !=
-        CUSOLVER_STATUS_SUCCESS)
-        return ERR_NUMERIC;
-    k_or_info<<<1, 1, 0, s>>>(e->info, e->acc);
-    if (cusolverDnXtrtri(e->h, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, o, CUDA_R_64F, G, o, e->twork,
-                         e->tdev, e->thost.data(), e->thost.size(), e->info) != CUSOLVER_STATUS_SUCCESS)
-        return ERR_NUMERIC;
-    k_or_info<<<1, 1, 0, s>>>(e->info, e->acc);
-    k_zero_upper_cm<<<(unsigned) (((size_t) o * o + 255) / 256), 256, 0, s>>>(G, o);
-    g_launches += 3;
-    // L^-1(i, k) = G[k*o + i]: row-major G is (L^-1)^T, so W = G^T U
-    dgemm(true, false, o, n, o, 1.0, G, o, U, n, 0.0, W, n, s);
-    return OK;
-}
-}  // namespace
-
-int dominant_subspace(Eig *e, const double *d_M, double *d_U, double *d_W, double *d_G, int n, int o, int iters,
-                      cudaStream_t s)
-{
-    if (o <= 0 || o > n || iters < 1) return ERR_INPUT;
-    cusolverDnSetStream(e->h, s);
-    if (e->po != o) {   // potrf and trtri workspaces for this o
-        int lw = 0;
-        size_t dev = 0, host = 0;
-        if (cusolverDnDpotrf_bufferSize(e->h, CUBLAS_FILL_MODE_LOWER, o, d_G, o, &lw) != CUSOLVER_STATUS_SUCCESS ||
-            cusolverDnXtrtri_bufferSize(e->h, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, o, CUDA_R_64F, d_G, o,
-                                        &dev, &host) != CUSOLVER_STATUS_SUCCESS)
-            return ERR_CUDA;
-        if (e->pwork) cudaFree(e->pwork);
-        if (e->twork) cudaFree(e->twork);
-        e->pwork = nullptr;
-        e->twork = nullptr;
-        e->po = 0;
-        if ((!e->acc && cudaMalloc(&e->acc, sizeof(int)) != cudaSuccess) ||
-            cudaMalloc(&e->pwork, sizeof(double) * (size_t) (lw > 0 ? lw : 1)) != cudaSuccess ||
-            cudaMalloc(&e->twork, dev > 0 ? dev : 16) != cudaSuccess)
-            return ERR_ALLOC;
-        e->thost.assign(host > 0 ? host : 1, 0);
-        e->plwork = lw;
-        e->tdev = dev;
-        e->po = o;
-    }
-    cudaMemsetAsync(e->acc, 0, sizeof(int), s);
-    const size_t on = (size_t) o * n;
-    double *cur = d_W, *nxt = d_U;   // cur: the basis (or an unorthonormalised product of it)
-    k_hash_fill<<<(unsigned) ((on + 255) / 256), 256, 0, s>>>(cur, on);
-    g_launches++;
-    for (int it = 1; it <= iters; it++) {
-        dgemm(false, false, o, n, n, 1.0, cur, n, d_M, n, 0.0, nxt, n, s);   // nxt = cur M (M symmetric)
-        if (it % kOrthoEvery == 0 || it == iters) {
-            const int rc = chol_qr(e, nxt, cur, d_G, n, o, s);
-            if (rc != OK) return rc;
-        } else {
-            std::swap(cur, nxt);
-        }
-    }
-    const int rc = chol_qr(e, cur, nxt, d_G, n, o, s);   // second pass: orthonormal to rounding
-    if (rc != OK) return rc;
-    if (nxt != d_U) cudaMemcpyAsync(d_U, nxt, sizeof(double) * on, cudaMemcpyDeviceToDevice, s);
-    int acc = 0;
-    if (cudaMemcpyAsync(&acc, e->acc, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-        return ERR_CUDA;
-    return acc == 0 ? OK : ERR_NUMERIC;
+    const cudaError_t err = cudaPeekAtLastError();
+    if (err == cudaSuccess) return OK;
+    fprintf(stderr, "[tinyscf] CUDA error in %s: %s\n", what, cudaGetErrorString(err));
+    return ERR_CUDA;
 }
 
 __global__ void k_scale_rows_invsqrt(const double *w, const double *V, double *out, int n)

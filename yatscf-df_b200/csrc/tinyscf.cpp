@@ -27,7 +27,6 @@
 #include "batch.h"
 #include "tune.h"
 
-#include <cusolverDn.h>
 
 using namespace tscf;
 
@@ -1812,16 +1811,9 @@ struct TinySCF_batch_struct {
         int n = 0;
         std::vector<int> members;
         double *A = nullptr, *W = nullptr;
-        int *info = nullptr;
-        void *dwork = nullptr;
-        std::vector<char> hwork;
-        size_t dbytes = 0;
-        bool batched = true;
         Eig *eig = nullptr;
     };
     std::vector<Group> groups;
-    cusolverDnHandle_t h = nullptr;
-    cusolverDnParams_t params = nullptr;
     double *d_Eall = nullptr;
     int *d_active = nullptr;
     int *d_kact = nullptr;             // molecules whose K the batched FP64 kernels build this iteration
@@ -1892,9 +1884,6 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     TSCF_CUDA_CHECK(cudaEventCreate(&b->ev0));
     TSCF_CUDA_CHECK(cudaEventCreate(&b->ev1));
     for (auto &ev : b->pev) TSCF_CUDA_CHECK(cudaEventCreate(&ev));
-    if (cusolverDnCreate(&b->h) != CUSOLVER_STATUS_SUCCESS || cusolverDnCreateParams(&b->params) != CUSOLVER_STATUS_SUCCESS)
-        return ERR_CUDA;
-    cusolverDnSetStream(b->h, b->s);
     // eigensolver groups of equal basis size
     std::map<int, int> gid;
     std::vector<int> slot(nmol);
@@ -1913,22 +1902,8 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
         const int64_t cnt = (int64_t) g.members.size(), n = g.n;
         RC(balloc(b, &g.A, (size_t) cnt * n * n));
         RC(balloc(b, &g.W, (size_t) cnt * n));
-        RC(balloc(b, &g.info, (size_t) cnt));
-        size_t dws = 0, hws = 0;
-        cusolverStatus_t st = cusolverDnXsyevBatched_bufferSize(b->h, b->params, CUSOLVER_EIG_MODE_VECTOR,
-                                                                CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, g.A, n,
-                                                                CUDA_R_64F, g.W, CUDA_R_64F, &dws, &hws, cnt);
-        if (st == CUSOLVER_STATUS_SUCCESS) {
-            g.dbytes = dws;
-            char *w = nullptr;
-            RC(balloc(b, &w, dws));
-            g.dwork = w;
-            g.hwork.resize(hws ? hws : 1);
-        } else {
-            g.batched = false;   // one syevd per member
-            g.eig = eig_create(g.n, b->s);
-            if (!g.eig) return ERR_CUDA;
-        }
+        g.eig = eig_create(g.n, b->s);
+        if (!g.eig) return ERR_ALLOC;
     }
     // per-molecule descriptors and work lists
     std::vector<MolDev> md(nmol);
@@ -2048,38 +2023,14 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     return OK;
 }
 
-// Eigensolves of the flagged molecules: one batched call per group when every
-// member needs one, else one syevd per flagged member.
+// Eigensolves of the flagged molecules, one per molecule with the engine's
+// solver of its group's size.
 int batch_eigs(TinySCF_batch_t b, const std::vector<int> &need)
 {
     for (auto &g : b->groups) {
         const int64_t cnt = (int64_t) g.members.size(), n = g.n;
-        int64_t nneed = 0;
-        for (int m : g.members) nneed += need[m] ? 1 : 0;
-        if (nneed == 0) continue;
-        if (nneed < cnt) {
-            if (!g.eig && !(g.eig = eig_create(g.n, b->s))) return ERR_CUDA;
-            for (int64_t k = 0; k < cnt; k++)
-                if (need[g.members[k]]) RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
-            continue;
-        }
-        if (g.batched) {
-            cusolverStatus_t st = cusolverDnXsyevBatched(b->h, b->params, CUSOLVER_EIG_MODE_VECTOR,
-                                                         CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, g.A, n, CUDA_R_64F,
-                                                         g.W, CUDA_R_64F, g.dwork, g.dbytes, g.hwork.data(),
-                                                         g.hwork.size(), g.info, cnt);
-            if (st != CUSOLVER_STATUS_SUCCESS) {
-                // this size is not taken by the batched solver: one syevd per member from now on
-                g.batched = false;
-                g.eig = eig_create(g.n, b->s);
-                if (!g.eig) return ERR_CUDA;
-            }
-        }
-        if (!g.batched) {
-            if (!g.eig && !(g.eig = eig_create(g.n, b->s))) return ERR_CUDA;
-            for (int64_t k = 0; k < cnt; k++)
-                RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
-        }
+        for (int64_t k = 0; k < cnt; k++)
+            if (need[g.members[k]]) RC(eig_run(g.eig, g.A + k * n * n, g.W + k * n, g.A + k * n * n, b->s));
     }
     return OK;
 }
@@ -2247,8 +2198,6 @@ void batch_free_impl(TinySCF_batch_t b)
     if (b->s) cudaStreamSynchronize(b->s);
     for (auto &g : b->groups) eig_destroy(g.eig);
     for (void *p : b->mem) cudaFree(p);
-    if (b->params) cusolverDnDestroyParams(b->params);
-    if (b->h) cusolverDnDestroy(b->h);
     for (auto &ev : b->pev)
         if (ev) cudaEventDestroy(ev);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -2334,6 +2283,37 @@ int TinySCF_batch_free(TinySCF_batch_t b)
     batch_free_impl(b);
     delete b;
     return TINYSCF_OK;
+}
+
+int TinySCF_eigh(int device, int n, const double *A, double *w, double *V)
+{
+    if (n < 1 || n > EIG_MAX_N || !A || !w || !V) return TINYSCF_ERR_INPUT;
+    if (cudaSetDevice(device) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    const size_t nn = (size_t) n * n;
+    double *dA = nullptr, *dw = nullptr, *dV = nullptr;
+    Eig *eg = nullptr;
+    int rc = TINYSCF_OK;
+    if (cudaMalloc(&dA, sizeof(double) * nn) != cudaSuccess || cudaMalloc(&dw, sizeof(double) * n) != cudaSuccess ||
+        cudaMalloc(&dV, sizeof(double) * nn) != cudaSuccess || !(eg = eig_create(n, s))) {
+        rc = TINYSCF_ERR_ALLOC;
+    } else if (cudaMemcpyAsync(dA, A, sizeof(double) * nn, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        rc = TINYSCF_ERR_CUDA;
+    } else {
+        rc = eig_run(eg, dA, dw, dV, s);
+        if (rc == OK && (cudaMemcpyAsync(w, dw, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaMemcpyAsync(V, dV, sizeof(double) * nn, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaStreamSynchronize(s) != cudaSuccess))
+            rc = TINYSCF_ERR_CUDA;
+        if (rc == OK) rc = eig_error(eg);
+    }
+    eig_destroy(eg);
+    cudaFree(dA);
+    cudaFree(dw);
+    cudaFree(dV);
+    cudaStreamDestroy(s);
+    return rc;
 }
 
 // ---- the reference's void API (abort on failure, like its asserts)

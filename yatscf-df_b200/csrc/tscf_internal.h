@@ -99,20 +99,31 @@ void launch_two_center_grouped(const DevShells &aux, const int *d_ids, const int
 void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
            const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s);
 
-// Symmetric eigen-decomposition (ascending eigenvalues). A is row-major n x n
-// symmetric; on return V holds eigenvectors as ROWS (V[k*n + i] = i-th entry of
-// eigenvector k). Workspace is owned by the Eig object.
+// The same product with the tile picked from the call shape (no tuning run).
+void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
+                   const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s);
+// ERR_CUDA (with a message) when a launch since the last check failed; the error is not cleared.
+int cuda_launch_rc(const char *what);
+
+// Symmetric eigen-decomposition (eigh.cu; ascending eigenvalues). A is
+// row-major n x n symmetric; on return V holds eigenvectors as ROWS (V[k*n + i]
+// = i-th entry of eigenvector k); V may alias A. Workspace (four n x n
+// matrices) is owned by the Eig object; n <= EIG_MAX_N. Asynchronous on s;
+// eig_error() (synchronous) reports a grid barrier of the tridiagonalisation
+// that gave up waiting.
+constexpr int EIG_MAX_N = 8192;
 struct Eig;
 Eig *eig_create(int n, cudaStream_t s);
 void eig_destroy(Eig *e);
 int  eig_run(Eig *e, const double *d_A, double *d_w, double *d_V, cudaStream_t s);
+int  eig_error(Eig *e);
 
 // Orthonormal rows U (o x n) spanning the dominant o-dimensional invariant
 // subspace of a symmetric M (n x n): iters products with M from a fixed
 // pseudo-random start, orthonormalised by Cholesky-QR every few products and
-// twice at the end; W (o x n) and G (o x o) are scratch. Uses e's cuSOLVER
-// handle. ERR_NUMERIC when a Cholesky factor or its inverse fails (the
-// caller then solves the eigenproblem instead).
+// twice at the end; W (o x n) and G (o x o) are scratch; the Cholesky factor
+// and its inverse are this library's kernels. ERR_NUMERIC when a Cholesky
+// factor fails (the caller then solves the eigenproblem instead).
 int dominant_subspace(Eig *e, const double *d_M, double *d_U, double *d_W, double *d_G, int n, int o, int iters,
                       cudaStream_t s);
 // X = U diag(f(w)) U^T with f(w) = w^-1/2, U from eigenvectors in rows.
@@ -221,6 +232,12 @@ void density_from_eig(const double *d_X, const double *d_V, double *d_Cocc, doub
                       cudaStream_t s);
 
 }  // namespace tscf
+
+#define RC_(x)                      \
+    do {                            \
+        const int rc__ = (x);       \
+        if (rc__) return rc__;      \
+    } while (0)
 
 #define TSCF_CUDA_CHECK(x)                                                            \
     do {                                                                              \

@@ -127,6 +127,7 @@ def load_library(path=LIBPATH):
                                  ctypes.POINTER(ctypes.c_int), dp, ctypes.POINTER(ctypes.c_float),
                                  ctypes.c_longlong], ctypes.c_longlong),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
+        "TinySCF_eigh": ([ip, ip, dp, dp, dp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -432,6 +433,20 @@ def autotune_report():
 
 def set_autotune(on):
     load_library().TinySCF_set_autotune(int(bool(on)))
+
+
+def eigh(A, device=0):
+    """(w, V) of a symmetric matrix from the engine's device eigensolver:
+    eigenvalues ascending, V[k] the k-th eigenvector."""
+    lib = load_library()
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n = A.shape[0]
+    w = np.zeros(n)
+    V = np.zeros((n, n))
+    rc = lib.TinySCF_eigh(int(device), n, _dptr(A), _dptr(w), _dptr(V))
+    if rc:
+        raise TinySCFError("eigh: " + STATUS.get(rc, str(rc)))
+    return w, V
 
 
 def device_memory(device=0):
