@@ -41,7 +41,6 @@ constexpr int TRD_NG = 8;         // CTAs that form the panel's dot products
 constexpr int DC_CHUNK = 256;     // items per CTA of the thread-per-item D&C kernels
 constexpr int DC_WCHUNK = 8;      // items per CTA of the warp-per-item D&C kernels (256 threads)
 constexpr long long kBarrierSpins = 1LL << 22;
-constexpr size_t kMaxDynSmem = 227 * 1024;
 
 __device__ __forceinline__ double warp_sum_bcast(double v)
 {
@@ -883,19 +882,28 @@ bool dc_plan(Eig *E)
     return true;
 }
 
+// Opt in to the dynamic shared memory the kernels ask for: the device's
+// per-block opt-in maximum less each kernel's static shared memory.
+template <typename K>
+bool optin_one(K kern, int optin)
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return false;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int) fa.sharedSizeBytes) == cudaSuccess;
+}
+
 bool smem_optin()
 {
-    static bool done = false;
-    if (done) return true;
-    const int mx = (int) kMaxDynSmem;
-    if (cudaFuncSetAttribute(k_sytrd_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024 + 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(k_dc_deflate, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-        cudaFuncSetAttribute(k_dc_secular, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-        cudaFuncSetAttribute(k_dc_zhat, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-        cudaFuncSetAttribute(k_dc_norms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-        cudaFuncSetAttribute(k_dc_order, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
+    static int done_dev = -1;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (done_dev == dev) return true;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    if (!optin_one(k_sytrd_panel, optin) || !optin_one(k_dc_deflate, optin) || !optin_one(k_dc_secular, optin) ||
+        !optin_one(k_dc_zhat, optin) || !optin_one(k_dc_norms, optin) || !optin_one(k_dc_order, optin))
         return false;
-    done = true;
+    done_dev = dev;
     return true;
 }
 
@@ -905,7 +913,11 @@ Eig *eig_create(int n, cudaStream_t s)
 {
     (void) s;
     if (n < 1 || n > EIG_MAX_N) return nullptr;
-    if (!smem_optin()) return nullptr;
+    if (!smem_optin()) {
+        fprintf(stderr, "[tinyscf] eigensolver: shared-memory opt-in failed: %s\n",
+                cudaGetErrorString(cudaGetLastError()));
+        return nullptr;
+    }
     Eig *E = new Eig();
     E->n = n;
     int dev = 0, nsm = 1, per = 0;
@@ -930,6 +942,7 @@ Eig *eig_create(int n, cudaStream_t s)
          ealloc(E, &P.rowinfo, n) && ealloc(E, &P.colsrc, n) && ealloc(E, &P.rot, n) && ealloc(E, &P.rotcs, n);
     ok = ok && dc_plan(E);
     if (!ok) {
+        fprintf(stderr, "[tinyscf] eigensolver workspace for n = %d: %s\n", n, cudaGetErrorString(cudaGetLastError()));
         eig_destroy(E);
         return nullptr;
     }
@@ -937,7 +950,9 @@ Eig *eig_create(int n, cudaStream_t s)
     cudaMemset(P.perm, 0, sizeof(int) * n);
     cudaMemset(E->bar, 0, 2 * sizeof(unsigned));
     cudaMemset(E->err, 0, sizeof(int));
-    if (cudaGetLastError() != cudaSuccess) {
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {
+        fprintf(stderr, "[tinyscf] eigensolver set-up for n = %d: %s\n", n, cudaGetErrorString(err));
         eig_destroy(E);
         return nullptr;
     }
