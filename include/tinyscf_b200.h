@@ -227,7 +227,8 @@ typedef struct TinySCF_batch_struct *TinySCF_batch_t;
 TINYSCF_API int TinySCF_batch_create(TinySCF_batch_t *out, TinySCF_t *mols, int nmol);
 TINYSCF_API int TinySCF_batch_do_SCF(TinySCF_batch_t b);
 /* Device time of the last TinySCF_batch_do_SCF (ms), its number of batched
- * iterations (the slowest molecule's count) and the kernels it launched. */
+ * iterations (the slowest molecule's count) and the kernels it launched
+ * outside the per-molecule eigensolves. */
 TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iterations, long long *launches);
 /* Device time (ms) of the last TinySCF_batch_do_SCF by phase: [0] J,
  * [1] K, [2] Fock + energy, [3] DIIS, [4] density, [5] final FP64 Fock build

@@ -33,6 +33,8 @@
 
 namespace tscf {
 
+long long g_eig_launches = 0;
+
 namespace {
 
 constexpr int TRD_THREADS = 512;
@@ -1005,6 +1007,7 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
         a.G = E->G;
         void *args[] = {&a};
         g_launches++;
+        g_eig_launches++;
         TSCF_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *) k_sytrd_panel, dim3(E->G), dim3(TRD_THREADS), args,
                                                     dyn, s));
         const int q = a.p + a.cols, mt = n - q;
@@ -1015,6 +1018,7 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
             double *A22 = E->A + (size_t) q * n + q;
             dgemm_untuned(false, true, mt, mt, a.cols, -1.0, V, n, W, TRD_NB, 1.0, A22, n, s);
             dgemm_untuned(false, true, mt, mt, a.cols, -1.0, W, TRD_NB, V, n, 1.0, A22, n, s);
+            g_eig_launches += 2;
         }
     }
     return cuda_launch_rc("tridiagonalisation");
@@ -1028,6 +1032,7 @@ int divide_conquer(Eig *E, cudaStream_t s)
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->Us, 0, sizeof(double) * nn, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->A, 0, sizeof(double) * nn, s));   // Qg
     g_launches++;
+    g_eig_launches++;
     k_dc_init<<<(n + 255) / 256, 256, 0, s>>>(E->d, E->e, E->pos.lam, E->Q, n);
     double *Qg = E->A;
     for (const auto &L : E->levels) {
@@ -1043,6 +1048,7 @@ int divide_conquer(Eig *E, cudaStream_t s)
         k_dc_commit_lam<<<L.nc, DC_CHUNK, 0, s>>>(E->nodes, E->pos, E->tab_c + L.c0);
         k_dc_gemm<<<L.nt, 128, 0, s>>>(E->nodes, E->tiles + L.t0, Qg, E->Us, E->Q, n);
         g_launches += 10;
+        g_eig_launches += 10;
     }
     return cuda_launch_rc("divide and conquer");
 }
@@ -1051,6 +1057,7 @@ int back_transform(Eig *E, double *d_V, cudaStream_t s)
 {
     const int n = E->n;
     g_launches += 2;
+    g_eig_launches += 2;
     k_wy_tfactor<<<E->npanels, 256, 0, s>>>(E->Vh, E->tau, E->Tf, n);
     k_transpose<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(E->Q, d_V, n);
     for (int P = E->npanels - 1; P >= 0; P--) {
@@ -1062,6 +1069,7 @@ int back_transform(Eig *E, double *d_V, cudaStream_t s)
         dgemm_untuned(false, true, n, cols, cols, 1.0, E->Y, TRD_NB, E->Tf + (size_t) P * TRD_NB * TRD_NB, TRD_NB, 0.0,
                       E->Y2, TRD_NB, s);
         dgemm_untuned(false, true, n, mv, cols, -1.0, E->Y2, TRD_NB, V, n, 1.0, d_V + p + 1, n, s);
+        g_eig_launches += 3;
     }
     return cuda_launch_rc("back-transformation");
 }
@@ -1076,6 +1084,7 @@ int eig_run(Eig *E, const double *d_A, double *d_w, double *d_V, cudaStream_t s)
     const int n = E->n;
     if (n == 1) {
         g_launches++;
+        g_eig_launches++;
         k_copy_scalar_eig<<<1, 1, 0, s>>>(d_A, d_w, d_V);
         return cuda_launch_rc("eigensolve (n = 1)");
     }

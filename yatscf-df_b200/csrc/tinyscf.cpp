@@ -2055,7 +2055,7 @@ int batch_scf_impl(TinySCF_batch_t b)
         return cudaMemcpyAsync(b->d_kact, kact.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, b->s);
     };
     TSCF_CUDA_CHECK(upload_flags());
-    const long long l0 = g_launches;
+    const long long l0 = g_launches, le0 = g_eig_launches;
     for (double &v : b->phase_ms) v = 0.0;
     for (int k = 0; k < nmol; k++)   // a molecule's incremental K restarts with each batched solve
         if (b->mixed[k]) kmix_reset(E_(b->mols[k])->kmix, b->s);
@@ -2175,7 +2175,7 @@ int batch_scf_impl(TinySCF_batch_t b)
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->scf_ms = ms;
     b->iterations = it;
-    b->launches = g_launches - l0;
+    b->launches = (g_launches - l0) - (g_eig_launches - le0);
     // eigenvalues (of the last full eigensolve) and host mirrors of every molecule
     for (auto &g : b->groups)
         for (size_t k = 0; k < g.members.size(); k++) {

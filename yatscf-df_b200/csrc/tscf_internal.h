@@ -13,6 +13,8 @@ namespace tscf {
 // Number of engine kernels launched by this process (host-side count, read by
 // the benchmark; library kernels such as cuSOLVER's are not included).
 extern long long g_launches;
+// The part of g_launches that the eigensolver (eigh.cu) launched.
+extern long long g_eig_launches;
 
 // ---------------------------------------------------------------- limits
 constexpr int MAX_L_ORB = 2;           // orbital shells up to d
