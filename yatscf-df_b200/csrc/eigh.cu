@@ -40,6 +40,7 @@ namespace {
 constexpr int TRD_THREADS = 512;
 constexpr int TRD_NB = 32;        // columns per panel
 constexpr int TRD_NG = 8;         // CTAs that form the panel's dot products
+constexpr int BT_NB = 128;        // reflectors per block of the back-transformation
 constexpr int DC_CHUNK = 256;     // items per CTA of the thread-per-item D&C kernels
 constexpr int DC_WCHUNK = 8;      // items per CTA of the warp-per-item D&C kernels (256 threads)
 constexpr long long kBarrierSpins = 1LL << 22;
@@ -134,10 +135,15 @@ __device__ bool grid_barrier(unsigned *bar, int *err, unsigned nblk)
 }
 
 // ------------------------------------------------------------------ tridiagonalisation
+// Storage: reflector j is row j of VT (v_j[j+1] = 1, zero before); within a
+// panel, PVW rows 0..NB-1 hold the panel's v and rows NB..2NB-1 its w, PWV the
+// same two halves swapped, so that the trailing update A22 -= V W^T + W V^T is
+// one GEMM PVW^T PWV with K = 2 NB, and every in-panel access to v or w runs
+// along a row (coalesced).
 struct TrdArgs {
     double *A;      // n x n work matrix (trailing part updated after each panel)
-    double *Vh;     // n x n reflectors: column j holds v_j (v_j[j+1] = 1), zero elsewhere
-    double *Wp;     // n x TRD_NB panel W
+    double *VT;     // n x n reflectors as rows
+    double *PVW, *PWV;   // 2 TRD_NB x n each
     double *d, *e, *tau;
     double *col, *y;
     double *part;   // [G] norms | [TRD_NG][2 TRD_NB] panel dots | [G] w.v
@@ -151,7 +157,6 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
     extern __shared__ double sv[];   // v of the current column, by absolute row
     __shared__ double s_a2[TRD_NB], s_wv[TRD_NB], s_vv[TRD_NB], s_vj[TRD_NB], s_wj[TRD_NB];
     __shared__ double s_red[33];
-    __shared__ double s_dw[TRD_THREADS / TRD_NB][TRD_NB], s_dv[TRD_THREADS / TRD_NB][TRD_NB];
     __shared__ double s_tau, s_scal, s_beta;
     const int n = a.n, p = a.p, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int gtid = blockIdx.x * TRD_THREADS + tid, GT = a.G * TRD_THREADS;
@@ -159,23 +164,26 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
     double *part_n = a.part, *part_d = a.part + a.G, *part_w = part_d + TRD_NG * 2 * TRD_NB;
     const int NG = min(a.G, TRD_NG);   // CTAs that form the panel dot products
     const double *A = a.A;
-    const double *Vh = a.Vh;
-    // W of an earlier panel column cc (its final value: w + a2 v)
-    auto Wf = [&](int r, int cc) {
-        return a.Wp[(size_t) r * TRD_NB + cc] + s_a2[cc] * Vh[(size_t) r * n + p + cc];
-    };
+    const double *PV = a.PVW;          // row cc: v of panel column cc
+    double *PW = a.PWV;                // row cc: w of panel column cc (before its a2 v term)
     for (int c = 0; c < a.cols; c++) {
         const int j = p + c;
-        // ---- phase 1: column j (rows j..n-1) minus the panel's earlier corrections
+        // ---- phase 1: column j (rows j..n-1; row j of the symmetric matrix) minus the panel's corrections
         if (tid < c) {
-            s_vj[tid] = Vh[(size_t) j * n + p + tid];
-            s_wj[tid] = Wf(j, tid);
+            const double vj = PV[(size_t) tid * n + j];
+            s_vj[tid] = vj;
+            s_wj[tid] = PW[(size_t) tid * n + j] + s_a2[tid] * vj;
         }
         __syncthreads();
         double ss = 0.0;
         for (int r = j + gtid; r < n; r += GT) {
-            double v = A[(size_t) r * n + j];
-            for (int cc = 0; cc < c; cc++) v -= Vh[(size_t) r * n + p + cc] * s_wj[cc] + Wf(r, cc) * s_vj[cc];
+            double v = A[(size_t) j * n + r];
+#pragma unroll 8
+            for (int cc = 0; cc < c; cc++) {
+                const double vr = PV[(size_t) cc * n + r];
+                const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
+                v -= vr * s_wj[cc] + wr * s_vj[cc];
+            }
             a.col[r] = v;
             if (r >= j + 2) ss += v * v;
         }
@@ -215,36 +223,43 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             a.e[j] = s_beta;
             a.tau[j] = tau;
         }
-        for (int r = j + 1 + gtid; r < n; r += GT) a.Vh[(size_t) r * n + j] = sv[r];
+        for (int r = j + 1 + gtid; r < n; r += GT) {
+            const double vr = sv[r];
+            a.VT[(size_t) j * n + r] = vr;
+            a.PVW[(size_t) c * n + r] = vr;
+            a.PWV[(size_t) (TRD_NB + c) * n + r] = vr;
+        }
         for (int r = j + 1 + gw; r < n; r += GW) {
             const double *row = A + (size_t) r * n;
-            double acc = 0.0;
-            for (int c2 = j + 1 + lane; c2 < n; c2 += 32) acc += row[c2] * sv[c2];
-            acc = warp_sum_bcast(acc);
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int c2 = j + 1 + lane;
+            for (; c2 + 96 < n; c2 += 128) {
+                a0 += row[c2] * sv[c2];
+                a1 += row[c2 + 32] * sv[c2 + 32];
+                a2 += row[c2 + 64] * sv[c2 + 64];
+                a3 += row[c2 + 96] * sv[c2 + 96];
+            }
+            for (; c2 < n; c2 += 32) a0 += row[c2] * sv[c2];
+            const double acc = warp_sum_bcast((a0 + a1) + (a2 + a3));
             if (lane == 0) a.y[r] = acc;
         }
         if (c > 0 && (int) blockIdx.x < NG) {
+            // this CTA's rows; warp w forms the dots of panel columns w and w + 16
             const int m = n - j - 1, chunk = (m + NG - 1) / NG;
             const int r0 = j + 1 + blockIdx.x * chunk, r1 = min(n, r0 + chunk);
-            const int cc = tid % TRD_NB, rg = tid / TRD_NB;
-            double aw = 0.0, av = 0.0;
-            if (cc < c)
-                for (int r = r0 + rg; r < r1; r += TRD_THREADS / TRD_NB) {
-                    const double vr = sv[r];
-                    aw += Wf(r, cc) * vr;
-                    av += Vh[(size_t) r * n + p + cc] * vr;
+            for (int cc = wid; cc < c; cc += TRD_THREADS / 32) {
+                double aw = 0.0, av = 0.0;
+                for (int r = r0 + lane; r < r1; r += 32) {
+                    const double vr = sv[r], pv = PV[(size_t) cc * n + r];
+                    aw += (PW[(size_t) cc * n + r] + s_a2[cc] * pv) * vr;
+                    av += pv * vr;
                 }
-            s_dw[rg][cc] = aw;
-            s_dv[rg][cc] = av;
-            __syncthreads();
-            if (tid < TRD_NB) {
-                double sw = 0.0, sx = 0.0;
-                for (int g = 0; g < TRD_THREADS / TRD_NB; g++) {
-                    sw += s_dw[g][tid];
-                    sx += s_dv[g][tid];
+                aw = warp_sum_bcast(aw);
+                av = warp_sum_bcast(av);
+                if (lane == 0) {
+                    part_d[blockIdx.x * 2 * TRD_NB + cc] = aw;
+                    part_d[blockIdx.x * 2 * TRD_NB + TRD_NB + cc] = av;
                 }
-                part_d[blockIdx.x * 2 * TRD_NB + tid] = sw;
-                part_d[blockIdx.x * 2 * TRD_NB + TRD_NB + tid] = sx;
             }
         }
         if (!grid_barrier(a.bar, a.err, a.G)) return;
@@ -262,9 +277,14 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
         double wd = 0.0;
         for (int r = j + 1 + gtid; r < n; r += GT) {
             double t = a.y[r];
-            for (int cc = 0; cc < c; cc++) t -= Vh[(size_t) r * n + p + cc] * s_wv[cc] + Wf(r, cc) * s_vv[cc];
+#pragma unroll 8
+            for (int cc = 0; cc < c; cc++) {
+                const double vr = PV[(size_t) cc * n + r];
+                const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
+                t -= vr * s_wv[cc] + wr * s_vv[cc];
+            }
             const double w = tau * t;
-            a.Wp[(size_t) r * TRD_NB + c] = w;
+            PW[(size_t) c * n + r] = w;
             wd += w * sv[r];
         }
         wd = block_sum_all<TRD_THREADS>(wd, s_red);
@@ -279,52 +299,40 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
         }
         __syncthreads();
     }
-    // final W of the rows the trailing update reads
+    // final w of the rows the trailing update reads, in both stacked panels
     const int q = p + a.cols;
     for (int r = q + gtid; r < n; r += GT)
-        for (int cc = 0; cc < a.cols; cc++) a.Wp[(size_t) r * TRD_NB + cc] = Wf(r, cc);
+        for (int cc = 0; cc < a.cols; cc++) {
+            const double w = PW[(size_t) cc * n + r] + s_a2[cc] * PV[(size_t) cc * n + r];
+            PW[(size_t) cc * n + r] = w;
+            a.PVW[(size_t) (TRD_NB + cc) * n + r] = w;
+        }
 }
 
-// T of the compact WY form of each panel: H_p ... H_(p+cols-1) = I - V T V^T,
-// T upper triangular (LAPACK dlarft, forward, columnwise). One CTA per panel.
-__global__ void __launch_bounds__(256) k_wy_tfactor(const double *Vh, const double *tau, double *Tf, int n)
+// T of the compact WY form of each block of BT_NB reflectors:
+// H_p0 ... H_(p0+bb-1) = I - V T V^T, T upper triangular (LAPACK dlarft,
+// forward, columnwise), from the block's Gram matrix G = V^T V. One CTA per block.
+__global__ void __launch_bounds__(256) k_wy_tfactor(const double *Gall, const double *tau, double *Tf, int nref)
 {
-    __shared__ double G[TRD_NB][TRD_NB + 1];
-    __shared__ double Vs[64][TRD_NB + 1];
-    __shared__ double T[TRD_NB][TRD_NB + 1];
-    const int P = blockIdx.x, p = P * TRD_NB, cols = min(TRD_NB, n - p), tid = threadIdx.x;
-    // G = V^T V over rows p+1..n-1: thread owns entries (a, b) = (tid / 32 + 8 i, tid % 32)
-    double acc[TRD_NB * TRD_NB / 256] = {};
-    for (int r0 = p + 1; r0 < n; r0 += 64) {
-        for (int l = tid; l < 64 * TRD_NB; l += 256) {
-            const int rr = l / TRD_NB, cc = l % TRD_NB, r = r0 + rr;
-            Vs[rr][cc] = (r < n && cc < cols) ? Vh[(size_t) r * n + p + cc] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < TRD_NB * TRD_NB / 256; i++) {
-            const int aa = tid / TRD_NB + (256 / TRD_NB) * i, bb = tid % TRD_NB;
-            double s = 0.0;
-            for (int rr = 0; rr < 64; rr++) s += Vs[rr][aa] * Vs[rr][bb];
-            acc[i] += s;
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < TRD_NB * TRD_NB / 256; i++) G[tid / TRD_NB + (256 / TRD_NB) * i][tid % TRD_NB] = acc[i];
-    for (int l = tid; l < TRD_NB * TRD_NB; l += 256) T[l / TRD_NB][l % TRD_NB] = 0.0;
+    extern __shared__ double tsm[];
+    double *T = tsm;                       // BT_NB x (BT_NB + 1)
+    const int B = blockIdx.x, p0 = B * BT_NB, bb = min(BT_NB, nref - p0), tid = threadIdx.x;
+    const double *G = Gall + (size_t) B * BT_NB * BT_NB;
+    constexpr int LD = BT_NB + 1;
+    for (int l = tid; l < BT_NB * LD; l += blockDim.x) T[l] = 0.0;
     __syncthreads();
-    for (int c = 0; c < cols; c++) {
-        const double tc = (p + c < n - 1) ? tau[p + c] : 0.0;
+    for (int c = 0; c < bb; c++) {
+        const double tc = tau[p0 + c];
         if (tid < c) {
             double s = 0.0;
-            for (int l = tid; l < c; l++) s += T[tid][l] * G[l][c];
-            T[tid][c] = -tc * s;
+            for (int l = tid; l < c; l++) s += T[tid * LD + l] * G[(size_t) l * BT_NB + c];
+            T[tid * LD + c] = -tc * s;
         }
-        if (tid == 0) T[c][c] = tc;
+        if (tid == 0) T[c * LD + c] = tc;
         __syncthreads();
     }
-    for (int l = tid; l < TRD_NB * TRD_NB; l += 256) Tf[(size_t) P * TRD_NB * TRD_NB + l] = T[l / TRD_NB][l % TRD_NB];
+    for (int l = tid; l < BT_NB * BT_NB; l += blockDim.x)
+        Tf[(size_t) B * BT_NB * BT_NB + l] = T[(l / BT_NB) * LD + l % BT_NB];
 }
 
 // ------------------------------------------------------------------ divide and conquer
@@ -349,7 +357,9 @@ struct DcPos {        // per position of the tridiagonal (node-local arrays star
     double2 *rotcs;   // their (C, S)
 };
 
-__global__ void k_dc_init(const double *d, const double *e, double *lam, double *Q, int n)
+// Both eigenvector buffers start as the identity: a piece of size one keeps
+// its vector in both, so a merge finds it whichever buffer it reads.
+__global__ void k_dc_init(const double *d, const double *e, double *lam, double *Qa, double *Qb, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -358,7 +368,8 @@ __global__ void k_dc_init(const double *d, const double *e, double *lam, double 
     if (i + 1 < n) v -= fabs(e[i]);
     if (i > 0) v -= fabs(e[i - 1]);
     lam[i] = v;
-    Q[(size_t) i * n + i] = 1.0;
+    Qa[(size_t) i * n + i] = 1.0;
+    Qb[(size_t) i * n + i] = 1.0;
 }
 
 // Sorting of the two halves, z, the tolerance and the deflation scan. One CTA per node.
@@ -438,11 +449,10 @@ __global__ void __launch_bounds__(512) k_dc_deflate(DcNodes nd, DcPos ps, const 
                     pj = s;
                     continue;
                 }
-                double S = sz[pj], C = sz[s];
-                const double tt = hypot(C, S), t = sd[s] - sd[pj];
-                C /= tt;
-                S = -S / tt;
-                if (fabs(t * C * S) <= tol) {
+                // close pair: |t C S| <= tol with C = z_s / h, S = -z_pj / h, h = hypot(z_s, z_pj)
+                const double zp = sz[pj], zs = sz[s], t = sd[s] - sd[pj];
+                if (fabs(t * zs * zp) <= tol * (zs * zs + zp * zp)) {
+                    const double tt = hypot(zs, zp), C = zs / tt, S = -zp / tt;
                     sz[s] = tt;
                     sz[pj] = 0.0;
                     ps.rot[lo + nr] = make_int2(pj, s);
@@ -622,8 +632,9 @@ __global__ void __launch_bounds__(DC_CHUNK) k_dc_order(DcNodes nd, DcPos ps, con
     ps.colsrc[lo + r] = a;
 }
 
-// The merge's eigenvector matrix in sorted-row order, one warp per row:
-// column c = secular vector j (normalised) or the unit vector of a deflated position.
+// The merge's eigenvector matrix U, one warp per sorted position s (written to
+// row perm[s], i.e. in the children's order): column c = secular vector j
+// (normalised) or the unit vector of a deflated position.
 __global__ void __launch_bounds__(256) k_dc_build(DcNodes nd, DcPos ps, const int2 *tab, double *Us, int n)
 {
     const int2 tb = tab[blockIdx.x];
@@ -632,7 +643,7 @@ __global__ void __launch_bounds__(256) k_dc_build(DcNodes nd, DcPos ps, const in
     if (s >= m) return;
     const int info = ps.rowinfo[lo + s];
     const double di = info >= 0 ? ps.dK[lo + info] : 0.0, zi = info >= 0 ? ps.zh[lo + info] : 0.0;
-    double *row = Us + (size_t) (lo + s) * n + lo;
+    double *row = Us + (size_t) (lo + ps.perm[lo + s]) * n + lo;   // row of the child-order basis
     for (int c = lane; c < m; c += 32) {
         const int src = ps.colsrc[lo + c];
         double v;
@@ -642,7 +653,8 @@ __global__ void __launch_bounds__(256) k_dc_build(DcNodes nd, DcPos ps, const in
     }
 }
 
-// Givens rotations of the deflation, applied to the rows of Us in reverse order; a thread per column.
+// Givens rotations of the deflation (on sorted positions, i.e. rows perm[.]
+// of U), applied in reverse order; a thread per column.
 __global__ void __launch_bounds__(DC_CHUNK) k_dc_rotate(DcNodes nd, DcPos ps, const int2 *tab, double *Us, int n)
 {
     const int2 tb = tab[blockIdx.x];
@@ -650,26 +662,15 @@ __global__ void __launch_bounds__(DC_CHUNK) k_dc_rotate(DcNodes nd, DcPos ps, co
     const int c = tb.y + threadIdx.x;
     if (nr == 0 || c >= m) return;
     double *U = Us + (size_t) lo * n + lo + c;
+    const int *perm = ps.perm + lo;
     for (int r = nr - 1; r >= 0; r--) {
         const int2 pr = ps.rot[lo + r];
         const double2 cs = ps.rotcs[lo + r];
-        const double x = U[(size_t) pr.x * n], y = U[(size_t) pr.y * n];
-        U[(size_t) pr.x * n] = cs.x * x - cs.y * y;
-        U[(size_t) pr.y * n] = cs.y * x + cs.x * y;
+        const size_t ix = (size_t) perm[pr.x] * n, iy = (size_t) perm[pr.y] * n;
+        const double x = U[ix], y = U[iy];
+        U[ix] = cs.x * x - cs.y * y;
+        U[iy] = cs.y * x + cs.x * y;
     }
-}
-
-// Qg = the node's block of Q with its columns in sorted order.
-__global__ void __launch_bounds__(256) k_dc_gather(DcNodes nd, DcPos ps, const int2 *tab, const double *Q, double *Qg,
-                                                   int n)
-{
-    const int2 tb = tab[blockIdx.x];
-    const int node = tb.x, lo = nd.lo[node], m = nd.hi[node] - lo;
-    const int lane = threadIdx.x & 31, r = tb.y + (threadIdx.x >> 5);
-    if (r >= m) return;
-    const double *src = Q + (size_t) (lo + r) * n + lo;
-    double *dst = Qg + (size_t) (lo + r) * n + lo;
-    for (int s = lane; s < m; s += 32) dst[s] = src[ps.perm[lo + s]];
 }
 
 __global__ void k_dc_commit_lam(DcNodes nd, DcPos ps, const int2 *tab)
@@ -680,14 +681,21 @@ __global__ void k_dc_commit_lam(DcNodes nd, DcPos ps, const int2 *tab)
     if (a < m) ps.lam[lo + a] = ps.lamnew[lo + a];
 }
 
-// Q(node block) = Qg(node block) Us(node block), 64 x 64 tiles on the FP64 tensor cores.
-__global__ void __launch_bounds__(128) k_dc_gemm(DcNodes nd, const int4 *tiles, const double *Qg, const double *Us,
-                                                 double *Q, int n)
+// New vectors of a node: [Q1 0; 0 Q2] U, one half at a time (rows of child
+// 1 with child 1's block, rows of child 2 with child 2's), read from Qin and
+// written to Qout; 64 x 64 tiles on the FP64 tensor cores. Tile entry:
+// (node, half, tile row, tile column).
+__global__ void __launch_bounds__(128) k_dc_gemm(DcNodes nd, const int4 *tiles, const double *Qin, const double *Us,
+                                                 double *Qout, int n)
 {
     const int4 t = tiles[blockIdx.x];
-    const int lo = nd.lo[t.x], m = nd.hi[t.x] - lo;
-    const size_t off = (size_t) lo * n + lo;
-    dgemm_tile_dmma64<false, false>(m, m, m, 1.0, Qg + off, n, Us + off, n, 0.0, Q + off, n, t.y * 64, t.z * 64);
+    const int node = t.x >> 1, half = t.x & 1;
+    const int lo = nd.lo[node], mid = nd.mid[node], hi = nd.hi[node], m = hi - lo;
+    const int r0 = half ? mid : lo, mh = half ? hi - mid : mid - lo;
+    const double *Ab = Qin + (size_t) r0 * n + r0;
+    const double *Bb = Us + (size_t) r0 * n + lo;
+    double *Cb = Qout + (size_t) r0 * n + lo;
+    dgemm_tile_dmma64<false, false>(mh, m, mh, 1.0, Ab, n, Bb, n, 0.0, Cb, n, t.y * 64, t.z * 64);
 }
 
 __global__ void k_transpose(const double *in, double *out, int n)
@@ -775,13 +783,14 @@ __global__ void k_hash_fill(double *A, size_t n)
 
 // ------------------------------------------------------------------ host side
 struct Eig {
-    int n = 0, G = 1, npanels = 0;
-    double *A = nullptr, *Vh = nullptr, *Wp = nullptr, *d = nullptr, *e = nullptr, *tau = nullptr, *col = nullptr,
-           *y = nullptr, *part = nullptr, *Tf = nullptr, *Y = nullptr, *Y2 = nullptr;
+    int n = 0, G = 1, npanels = 0, nblk = 0;
+    // tridiagonalisation and back-transformation
+    double *A = nullptr, *VT = nullptr, *PVW = nullptr, *PWV = nullptr, *d = nullptr, *e = nullptr, *tau = nullptr,
+           *col = nullptr, *y = nullptr, *part = nullptr, *Gb = nullptr, *Tf = nullptr, *Y = nullptr, *Y2 = nullptr;
     unsigned *bar = nullptr;
     int *err = nullptr;
-    // divide and conquer
-    double *Q = nullptr, *Us = nullptr;   // Qg reuses A
+    // divide and conquer: eigenvector buffers of alternate tree levels (Qa reuses A) and the merge's U
+    double *Qb = nullptr, *Us = nullptr;
     DcNodes nodes{};
     DcPos pos{};
     int *node_mem = nullptr;
@@ -789,7 +798,7 @@ struct Eig {
     int2 *tab_c = nullptr, *tab_w = nullptr;
     int4 *tiles = nullptr;
     struct Level {
-        int node0, nnodes, maxm, c0, nc, w0, nw, t0, nt;
+        int depth, node0, nnodes, maxm, c0, nc, w0, nw, t0, nt;
     };
     std::vector<Level> levels;
     // Cholesky-QR of dominant_subspace
@@ -841,6 +850,7 @@ bool dc_plan(Eig *E)
         L.w0 = (int) tw.size();
         L.t0 = (int) tt.size();
         const int dep = nodes[i].dep;
+        L.depth = dep;
         for (; i < nodes.size() && nodes[i].dep == dep; i++) {
             const int id = (int) i, m = nodes[i].hi - nodes[i].lo;
             lo.push_back(nodes[i].lo);
@@ -849,9 +859,12 @@ bool dc_plan(Eig *E)
             L.maxm = std::max(L.maxm, m);
             for (int f = 0; f < m; f += DC_CHUNK) tc.push_back(make_int2(id, f));
             for (int f = 0; f < m; f += DC_WCHUNK) tw.push_back(make_int2(id, f));
-            const int nt = (m + 63) / 64;
-            for (int a = 0; a < nt; a++)
-                for (int b = 0; b < nt; b++) tt.push_back(make_int4(id, a, b, 0));
+            const int ntc = (m + 63) / 64;
+            for (int h = 0; h < 2; h++) {
+                const int mh = h ? nodes[i].hi - nodes[i].mid : nodes[i].mid - nodes[i].lo;
+                for (int a = 0; a < (mh + 63) / 64; a++)
+                    for (int b = 0; b < ntc; b++) tt.push_back(make_int4(2 * id + h, a, b, 0));
+            }
         }
         L.nnodes = (int) i - L.node0;
         L.nc = (int) tc.size() - L.c0;
@@ -902,7 +915,8 @@ bool smem_optin()
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (done_dev == dev) return true;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
-    if (!optin_one(k_sytrd_panel, optin) || !optin_one(k_dc_deflate, optin) || !optin_one(k_dc_secular, optin) ||
+    if (!optin_one(k_sytrd_panel, optin) || !optin_one(k_wy_tfactor, optin) || !optin_one(k_dc_deflate, optin) ||
+        !optin_one(k_dc_secular, optin) ||
         !optin_one(k_dc_zhat, optin) || !optin_one(k_dc_norms, optin) || !optin_one(k_dc_order, optin))
         return false;
     done_dev = dev;
@@ -929,13 +943,15 @@ Eig *eig_create(int n, cudaStream_t s)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sytrd_panel, TRD_THREADS, dyn);
     E->G = std::max(1, std::min({nsm * std::max(per, 1), nsm, (n + 31) / 32}));
     E->npanels = (n + TRD_NB - 1) / TRD_NB;
+    E->nblk = (n - 1 + BT_NB - 1) / BT_NB;   // blocks of the n - 1 reflectors
     const size_t nn = (size_t) n * n;
-    bool ok = ealloc(E, &E->A, nn) && ealloc(E, &E->Vh, nn) && ealloc(E, &E->Q, nn) && ealloc(E, &E->Us, nn) &&
-              ealloc(E, &E->Wp, (size_t) n * TRD_NB) && ealloc(E, &E->Y, (size_t) n * TRD_NB) &&
-              ealloc(E, &E->Y2, (size_t) n * TRD_NB) && ealloc(E, &E->d, n) && ealloc(E, &E->e, n) &&
-              ealloc(E, &E->tau, n) && ealloc(E, &E->col, n) && ealloc(E, &E->y, n) &&
+    bool ok = ealloc(E, &E->A, nn) && ealloc(E, &E->VT, nn) && ealloc(E, &E->Qb, nn) && ealloc(E, &E->Us, nn) &&
+              ealloc(E, &E->PVW, (size_t) 2 * TRD_NB * n) && ealloc(E, &E->PWV, (size_t) 2 * TRD_NB * n) &&
+              ealloc(E, &E->Y, (size_t) n * BT_NB) && ealloc(E, &E->Y2, (size_t) n * BT_NB) && ealloc(E, &E->d, n) &&
+              ealloc(E, &E->e, n) && ealloc(E, &E->tau, n) && ealloc(E, &E->col, n) && ealloc(E, &E->y, n) &&
               ealloc(E, &E->part, 2 * (size_t) E->G + TRD_NG * 2 * TRD_NB) &&
-              ealloc(E, &E->Tf, (size_t) E->npanels * TRD_NB * TRD_NB) && ealloc(E, &E->bar, 2) &&
+              ealloc(E, &E->Gb, (size_t) std::max(E->nblk, 1) * BT_NB * BT_NB) &&
+              ealloc(E, &E->Tf, (size_t) std::max(E->nblk, 1) * BT_NB * BT_NB) && ealloc(E, &E->bar, 2) &&
               ealloc(E, &E->err, 1) && ealloc(E, &E->acc, 1);
     DcPos &P = E->pos;
     ok = ok && ealloc(E, &P.lam, n) && ealloc(E, &P.ds, n) && ealloc(E, &P.dK, n) && ealloc(E, &P.zK, n) &&
@@ -983,7 +999,7 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
     const int n = E->n;
     const size_t nn = (size_t) n * n;
     TSCF_CUDA_CHECK(cudaMemcpyAsync(E->A, d_A, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
-    TSCF_CUDA_CHECK(cudaMemsetAsync(E->Vh, 0, sizeof(double) * nn, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->VT, 0, sizeof(double) * nn, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->tau, 0, sizeof(double) * n, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->e, 0, sizeof(double) * n, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->bar, 0, 2 * sizeof(unsigned), s));
@@ -991,8 +1007,9 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
     for (int P = 0; P < E->npanels; P++) {
         TrdArgs a;
         a.A = E->A;
-        a.Vh = E->Vh;
-        a.Wp = E->Wp;
+        a.VT = E->VT;
+        a.PVW = E->PVW;
+        a.PWV = E->PWV;
         a.d = E->d;
         a.e = E->e;
         a.tau = E->tau;
@@ -1012,63 +1029,70 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
                                                     dyn, s));
         const int q = a.p + a.cols, mt = n - q;
         if (mt > 0) {
-            // A22 -= V W^T + W V^T
-            const double *V = E->Vh + (size_t) q * n + a.p;
-            const double *W = E->Wp + (size_t) q * TRD_NB;
-            double *A22 = E->A + (size_t) q * n + q;
-            dgemm_untuned(false, true, mt, mt, a.cols, -1.0, V, n, W, TRD_NB, 1.0, A22, n, s);
-            dgemm_untuned(false, true, mt, mt, a.cols, -1.0, W, TRD_NB, V, n, 1.0, A22, n, s);
-            g_eig_launches += 2;
+            // A22 -= V W^T + W V^T = PVW^T PWV over the trailing columns (a full panel: cols = TRD_NB)
+            dgemm_untuned(true, false, mt, mt, 2 * TRD_NB, -1.0, E->PVW + q, n, E->PWV + q, n, 1.0,
+                          E->A + (size_t) q * n + q, n, s);
+            g_eig_launches++;
         }
     }
     return cuda_launch_rc("tridiagonalisation");
 }
 
-int divide_conquer(Eig *E, cudaStream_t s)
+// Eigenvectors of T into the columns of the returned buffer (E->A or E->Qb).
+int divide_conquer(Eig *E, cudaStream_t s, double **out)
 {
     const int n = E->n;
     const size_t nn = (size_t) n * n;
-    TSCF_CUDA_CHECK(cudaMemsetAsync(E->Q, 0, sizeof(double) * nn, s));
+    double *buf[2] = {E->A, E->Qb};   // level of depth L writes buf[L % 2], reads its children from the other
+    TSCF_CUDA_CHECK(cudaMemsetAsync(buf[0], 0, sizeof(double) * nn, s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(buf[1], 0, sizeof(double) * nn, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->Us, 0, sizeof(double) * nn, s));
-    TSCF_CUDA_CHECK(cudaMemsetAsync(E->A, 0, sizeof(double) * nn, s));   // Qg
     g_launches++;
     g_eig_launches++;
-    k_dc_init<<<(n + 255) / 256, 256, 0, s>>>(E->d, E->e, E->pos.lam, E->Q, n);
-    double *Qg = E->A;
+    k_dc_init<<<(n + 255) / 256, 256, 0, s>>>(E->d, E->e, E->pos.lam, buf[0], buf[1], n);
     for (const auto &L : E->levels) {
         const size_t m = (size_t) L.maxm;
-        k_dc_deflate<<<L.nnodes, 512, 20 * m, s>>>(E->nodes, E->pos, E->Q, E->e, n, L.node0);
+        const double *Qin = buf[(L.depth + 1) % 2];
+        double *Qout = buf[L.depth % 2];
+        k_dc_deflate<<<L.nnodes, 512, 20 * m, s>>>(E->nodes, E->pos, Qin, E->e, n, L.node0);
         k_dc_secular<<<L.nw, 256, 16 * m, s>>>(E->nodes, E->pos, E->tab_w + L.w0);
         k_dc_zhat<<<L.nw, 256, 24 * m, s>>>(E->nodes, E->pos, E->tab_w + L.w0);
         k_dc_norms<<<L.nw, 256, 16 * m, s>>>(E->nodes, E->pos, E->tab_w + L.w0);
         k_dc_order<<<L.nc, DC_CHUNK, 8 * m, s>>>(E->nodes, E->pos, E->tab_c + L.c0);
         k_dc_build<<<L.nw, 256, 0, s>>>(E->nodes, E->pos, E->tab_w + L.w0, E->Us, n);
         k_dc_rotate<<<L.nc, DC_CHUNK, 0, s>>>(E->nodes, E->pos, E->tab_c + L.c0, E->Us, n);
-        k_dc_gather<<<L.nw, 256, 0, s>>>(E->nodes, E->pos, E->tab_w + L.w0, E->Q, Qg, n);
         k_dc_commit_lam<<<L.nc, DC_CHUNK, 0, s>>>(E->nodes, E->pos, E->tab_c + L.c0);
-        k_dc_gemm<<<L.nt, 128, 0, s>>>(E->nodes, E->tiles + L.t0, Qg, E->Us, E->Q, n);
-        g_launches += 10;
-        g_eig_launches += 10;
+        k_dc_gemm<<<L.nt, 128, 0, s>>>(E->nodes, E->tiles + L.t0, Qin, E->Us, Qout, n);
+        g_launches += 9;
+        g_eig_launches += 9;
     }
+    *out = buf[0];   // the root has depth 0
     return cuda_launch_rc("divide and conquer");
 }
 
-int back_transform(Eig *E, double *d_V, cudaStream_t s)
+// Vout = Z^T Q^T, Z (the tridiagonal's eigenvectors, columns of Zc), Q the
+// product of the reflectors, in blocks of BT_NB reflectors from the last:
+// Vout <- Vout - (Vout V) T^T V^T.
+int back_transform(Eig *E, const double *Zc, double *d_V, cudaStream_t s)
 {
-    const int n = E->n;
+    const int n = E->n, nref = n - 1;
+    for (int B = 0; B < E->nblk; B++) {
+        const int p0 = B * BT_NB, bb = std::min(BT_NB, nref - p0);
+        const double *V = E->VT + (size_t) p0 * n + p0 + 1;   // bb x (n - p0 - 1), ld n
+        dgemm_untuned(false, true, bb, bb, n - p0 - 1, 1.0, V, n, V, n, 0.0, E->Gb + (size_t) B * BT_NB * BT_NB, BT_NB,
+                      s);
+    }
     g_launches += 2;
-    g_eig_launches += 2;
-    k_wy_tfactor<<<E->npanels, 256, 0, s>>>(E->Vh, E->tau, E->Tf, n);
-    k_transpose<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(E->Q, d_V, n);
-    for (int P = E->npanels - 1; P >= 0; P--) {
-        const int p = P * TRD_NB, cols = std::min(TRD_NB, n - p), mv = n - p - 1;
-        if (mv <= 0) continue;
-        const double *V = E->Vh + (size_t) (p + 1) * n + p;
-        // Y = Vout[:, p+1:] V;  Y2 = Y T^T;  Vout[:, p+1:] -= Y2 V^T
-        dgemm_untuned(false, false, n, cols, mv, 1.0, d_V + p + 1, n, V, n, 0.0, E->Y, TRD_NB, s);
-        dgemm_untuned(false, true, n, cols, cols, 1.0, E->Y, TRD_NB, E->Tf + (size_t) P * TRD_NB * TRD_NB, TRD_NB, 0.0,
-                      E->Y2, TRD_NB, s);
-        dgemm_untuned(false, true, n, mv, cols, -1.0, E->Y2, TRD_NB, V, n, 1.0, d_V + p + 1, n, s);
+    g_eig_launches += 2 + E->nblk;
+    k_wy_tfactor<<<E->nblk, 256, sizeof(double) * BT_NB * (BT_NB + 1), s>>>(E->Gb, E->tau, E->Tf, nref);
+    k_transpose<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(Zc, d_V, n);
+    for (int B = E->nblk - 1; B >= 0; B--) {
+        const int p0 = B * BT_NB, bb = std::min(BT_NB, nref - p0), mv = n - p0 - 1;
+        const double *V = E->VT + (size_t) p0 * n + p0 + 1;
+        dgemm_untuned(false, true, n, bb, mv, 1.0, d_V + p0 + 1, n, V, n, 0.0, E->Y, BT_NB, s);
+        dgemm_untuned(false, true, n, bb, bb, 1.0, E->Y, BT_NB, E->Tf + (size_t) B * BT_NB * BT_NB, BT_NB, 0.0, E->Y2,
+                      BT_NB, s);
+        dgemm_untuned(false, false, n, mv, bb, -1.0, E->Y2, BT_NB, V, n, 1.0, d_V + p0 + 1, n, s);
         g_eig_launches += 3;
     }
     return cuda_launch_rc("back-transformation");
@@ -1089,8 +1113,9 @@ int eig_run(Eig *E, const double *d_A, double *d_w, double *d_V, cudaStream_t s)
         return cuda_launch_rc("eigensolve (n = 1)");
     }
     RC_(tridiagonalize(E, d_A, s));
-    RC_(divide_conquer(E, s));
-    RC_(back_transform(E, d_V, s));
+    double *Z = nullptr;
+    RC_(divide_conquer(E, s, &Z));
+    RC_(back_transform(E, Z, d_V, s));
     TSCF_CUDA_CHECK(cudaMemcpyAsync(d_w, E->pos.lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     return OK;
 }
