@@ -39,7 +39,8 @@ namespace {
 
 constexpr int TRD_THREADS = 512;
 constexpr int TRD_NB = 32;        // columns per panel
-constexpr int TRD_NG = 8;         // CTAs that form the panel's dot products
+constexpr int TRD_SEG = 256;     // columns per item of the symmetric matrix-vector product
+constexpr int GR_KS = 8;          // row slices of the reflector blocks' Gram matrices
 constexpr int BT_NB = 128;        // reflectors per block of the back-transformation
 constexpr int DC_CHUNK = 256;     // items per CTA of the thread-per-item D&C kernels
 constexpr int DC_WCHUNK = 8;      // items per CTA of the warp-per-item D&C kernels (256 threads)
@@ -145,8 +146,9 @@ struct TrdArgs {
     double *VT;     // n x n reflectors as rows
     double *PVW, *PWV;   // 2 TRD_NB x n each
     double *d, *e, *tau;
-    double *col, *y;
-    double *part;   // [G] norms | [TRD_NG][2 TRD_NB] panel dots | [G] w.v
+    double *col;
+    double *y;      // [segment][row] partial sums of A v
+    double *part;   // [G] norms | [2 TRD_NB][G] panel dots | [G] w.v
     unsigned *bar;
     int *err;
     int n, p, cols, G;
@@ -161,8 +163,10 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
     const int n = a.n, p = a.p, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int gtid = blockIdx.x * TRD_THREADS + tid, GT = a.G * TRD_THREADS;
     const int gw = blockIdx.x * (TRD_THREADS / 32) + wid, GW = a.G * (TRD_THREADS / 32);
-    double *part_n = a.part, *part_d = a.part + a.G, *part_w = part_d + TRD_NG * 2 * TRD_NB;
-    const int NG = min(a.G, TRD_NG);   // CTAs that form the panel dot products
+    // row work: groups of 8 lanes per row, the panel columns split over the 8 lanes
+    const int l8 = lane & 7, grp = gtid >> 3, NGRP = GT >> 3;
+    const int nseg = (n + TRD_SEG - 1) / TRD_SEG;
+    double *part_n = a.part, *part_d = a.part + a.G, *part_w = part_d + (size_t) a.G * 2 * TRD_NB;
     const double *A = a.A;
     const double *PV = a.PVW;          // row cc: v of panel column cc
     double *PW = a.PWV;                // row cc: w of panel column cc (before its a2 v term)
@@ -176,16 +180,28 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
         }
         __syncthreads();
         double ss = 0.0;
-        for (int r = j + gtid; r < n; r += GT) {
-            double v = A[(size_t) j * n + r];
-#pragma unroll 8
-            for (int cc = 0; cc < c; cc++) {
-                const double vr = PV[(size_t) cc * n + r];
-                const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
-                v -= vr * s_wj[cc] + wr * s_vj[cc];
+        for (int r0 = j + (grp & ~3); r0 < n; r0 += NGRP) {   // warp-uniform trip count
+            const int r = r0 + (grp & 3);
+            double v = 0.0;
+            if (r < n) {
+                if (l8 == 0) v = A[(size_t) j * n + r];
+#pragma unroll
+                for (int q = 0; q < TRD_NB / 8; q++) {
+                    const int cc = l8 + 8 * q;
+                    if (cc < c) {
+                        const double vr = PV[(size_t) cc * n + r];
+                        const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
+                        v -= vr * s_wj[cc] + wr * s_vj[cc];
+                    }
+                }
             }
-            a.col[r] = v;
-            if (r >= j + 2) ss += v * v;
+            v += __shfl_xor_sync(0xffffffff, v, 1);
+            v += __shfl_xor_sync(0xffffffff, v, 2);
+            v += __shfl_xor_sync(0xffffffff, v, 4);
+            if (r < n && l8 == 0) {
+                a.col[r] = v;
+                if (r >= j + 2) ss += v * v;
+            }
         }
         ss = block_sum_all<TRD_THREADS>(ss, s_red);
         if (tid == 0) part_n[blockIdx.x] = ss;
@@ -194,7 +210,7 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             if (gtid == 0) a.d[j] = a.col[j];
             break;
         }
-        // ---- phase 2: reflector (every CTA forms the same one), v, y = A v, panel dots
+        // ---- phase 2: reflector (every CTA forms the same one), v, y = A v by segments, panel dots
         if (wid == 0) {
             double s = 0.0;
             for (int b = lane; b < a.G; b += 32) s += part_n[b];
@@ -229,23 +245,30 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             a.PVW[(size_t) c * n + r] = vr;
             a.PWV[(size_t) (TRD_NB + c) * n + r] = vr;
         }
-        for (int r = j + 1 + gw; r < n; r += GW) {
-            const double *row = A + (size_t) r * n;
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-            int c2 = j + 1 + lane;
-            for (; c2 + 96 < n; c2 += 128) {
-                a0 += row[c2] * sv[c2];
-                a1 += row[c2 + 32] * sv[c2 + 32];
-                a2 += row[c2 + 64] * sv[c2 + 64];
-                a3 += row[c2 + 96] * sv[c2 + 96];
+        {
+            // items (row r, segment s) over rows j+1..n-1 and the segments holding columns j+1..n-1
+            const int s0 = (j + 1) / TRD_SEG, ns = nseg - s0, m = n - j - 1;
+            const long long nitems = (long long) m * ns;
+            for (long long it = gw; it < nitems; it += GW) {
+                const int r = j + 1 + (int) (it / ns), sg = s0 + (int) (it % ns);
+                const double *row = A + (size_t) r * n;
+                double acc[TRD_SEG / 32];
+#pragma unroll
+                for (int k = 0; k < TRD_SEG / 32; k++) {
+                    const int c2 = sg * TRD_SEG + lane + 32 * k;
+                    acc[k] = (c2 > j && c2 < n) ? row[c2] * sv[c2] : 0.0;
+                }
+#pragma unroll
+                for (int k = TRD_SEG / 64; k > 0; k >>= 1)
+#pragma unroll
+                    for (int q = 0; q < k; q++) acc[q] += acc[q + k];
+                const double y = warp_sum_bcast(acc[0]);
+                if (lane == 0) a.y[(size_t) sg * n + r] = y;
             }
-            for (; c2 < n; c2 += 32) a0 += row[c2] * sv[c2];
-            const double acc = warp_sum_bcast((a0 + a1) + (a2 + a3));
-            if (lane == 0) a.y[r] = acc;
         }
-        if (c > 0 && (int) blockIdx.x < NG) {
+        if (c > 0) {
             // this CTA's rows; warp w forms the dots of panel columns w and w + 16
-            const int m = n - j - 1, chunk = (m + NG - 1) / NG;
+            const int m = n - j - 1, chunk = (m + a.G - 1) / a.G;
             const int r0 = j + 1 + blockIdx.x * chunk, r1 = min(n, r0 + chunk);
             for (int cc = wid; cc < c; cc += TRD_THREADS / 32) {
                 double aw = 0.0, av = 0.0;
@@ -257,35 +280,52 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
                 aw = warp_sum_bcast(aw);
                 av = warp_sum_bcast(av);
                 if (lane == 0) {
-                    part_d[blockIdx.x * 2 * TRD_NB + cc] = aw;
-                    part_d[blockIdx.x * 2 * TRD_NB + TRD_NB + cc] = av;
+                    part_d[(size_t) cc * a.G + blockIdx.x] = aw;
+                    part_d[(size_t) (TRD_NB + cc) * a.G + blockIdx.x] = av;
                 }
             }
         }
         if (!grid_barrier(a.bar, a.err, a.G)) return;
         // ---- phase 3: w = tau (y - V (W^T v) - W (V^T v)), partial w.v
-        if (tid < c) {
+        for (int cc = wid; cc < c; cc += TRD_THREADS / 32) {
             double sw = 0.0, sx = 0.0;
-            for (int b = 0; b < NG; b++) {
-                sw += part_d[b * 2 * TRD_NB + tid];
-                sx += part_d[b * 2 * TRD_NB + TRD_NB + tid];
+            for (int b = lane; b < a.G; b += 32) {
+                sw += part_d[(size_t) cc * a.G + b];
+                sx += part_d[(size_t) (TRD_NB + cc) * a.G + b];
             }
-            s_wv[tid] = sw;
-            s_vv[tid] = sx;
+            sw = warp_sum_bcast(sw);
+            sx = warp_sum_bcast(sx);
+            if (lane == 0) {
+                s_wv[cc] = sw;
+                s_vv[cc] = sx;
+            }
         }
         __syncthreads();
         double wd = 0.0;
-        for (int r = j + 1 + gtid; r < n; r += GT) {
-            double t = a.y[r];
-#pragma unroll 8
-            for (int cc = 0; cc < c; cc++) {
-                const double vr = PV[(size_t) cc * n + r];
-                const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
-                t -= vr * s_wv[cc] + wr * s_vv[cc];
+        const int s0 = (j + 1) / TRD_SEG;
+        for (int r0 = j + 1 + (grp & ~3); r0 < n; r0 += NGRP) {
+            const int r = r0 + (grp & 3);
+            double t = 0.0;
+            if (r < n) {
+                for (int sg = s0 + l8; sg < nseg; sg += 8) t += a.y[(size_t) sg * n + r];
+#pragma unroll
+                for (int q = 0; q < TRD_NB / 8; q++) {
+                    const int cc = l8 + 8 * q;
+                    if (cc < c) {
+                        const double vr = PV[(size_t) cc * n + r];
+                        const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
+                        t -= vr * s_wv[cc] + wr * s_vv[cc];
+                    }
+                }
             }
-            const double w = tau * t;
-            PW[(size_t) c * n + r] = w;
-            wd += w * sv[r];
+            t += __shfl_xor_sync(0xffffffff, t, 1);
+            t += __shfl_xor_sync(0xffffffff, t, 2);
+            t += __shfl_xor_sync(0xffffffff, t, 4);
+            if (r < n && l8 == 0) {
+                const double w = tau * t;
+                PW[(size_t) c * n + r] = w;
+                wd += w * sv[r];
+            }
         }
         wd = block_sum_all<TRD_THREADS>(wd, s_red);
         if (tid == 0) part_w[blockIdx.x] = wd;
@@ -309,24 +349,70 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
         }
 }
 
+// Partial Gram matrices V_B^T V_B of the reflector blocks (the reflectors of
+// block B are rows p0..p0+bb-1 of VT, zero before column p0 + 1): CTA (B,
+// 32 x 32 tile, slice ks of the columns) writes its slice's sum to Gp[B][ks].
+__global__ void __launch_bounds__(256) k_wy_gram(const double *VT, double *Gp, int n, int nref)
+{
+    __shared__ double As[32][65], Bs[32][65];
+    const int B = blockIdx.x, tile = blockIdx.y, ks = blockIdx.z;
+    const int p0 = B * BT_NB, bb = min(BT_NB, nref - p0);
+    const int ta = tile / (BT_NB / 32), tb = tile % (BT_NB / 32);
+    const int K0 = p0 + 1, K = n - K0, kper = (K + GR_KS - 1) / GR_KS;
+    const int k0 = K0 + ks * kper, k1 = min(n, k0 + kper);
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[2][2] = {};
+    for (int kc = k0; kc < k1; kc += 64) {
+        for (int l = threadIdx.x; l < 32 * 64; l += 256) {
+            const int rr = l / 64, kk = l % 64, k = kc + kk;
+            const int ra = ta * 32 + rr, rb = tb * 32 + rr;
+            As[rr][kk] = (ra < bb && k < k1) ? VT[(size_t) (p0 + ra) * n + k] : 0.0;
+            Bs[rr][kk] = (rb < bb && k < k1) ? VT[(size_t) (p0 + rb) * n + k] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 64; kk++) {
+            const double a0 = As[ty][kk], a1 = As[ty + 16][kk], b0 = Bs[tx][kk], b1 = Bs[tx + 16][kk];
+            acc[0][0] += a0 * b0;
+            acc[0][1] += a0 * b1;
+            acc[1][0] += a1 * b0;
+            acc[1][1] += a1 * b1;
+        }
+        __syncthreads();
+    }
+    double *G = Gp + (size_t) (B * GR_KS + ks) * BT_NB * BT_NB;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++) G[(size_t) (ta * 32 + ty + 16 * i) * BT_NB + tb * 32 + tx + 16 * jj] = acc[i][jj];
+}
+
 // T of the compact WY form of each block of BT_NB reflectors:
 // H_p0 ... H_(p0+bb-1) = I - V T V^T, T upper triangular (LAPACK dlarft,
-// forward, columnwise), from the block's Gram matrix G = V^T V. One CTA per block.
-__global__ void __launch_bounds__(256) k_wy_tfactor(const double *Gall, const double *tau, double *Tf, int nref)
+// forward, columnwise), from the block's Gram matrix (the sum of its
+// GR_KS slices). One CTA per block.
+__global__ void __launch_bounds__(256) k_wy_tfactor(const double *Gp, const double *tau, double *Tf, int nref)
 {
     extern __shared__ double tsm[];
-    double *T = tsm;                       // BT_NB x (BT_NB + 1)
-    const int B = blockIdx.x, p0 = B * BT_NB, bb = min(BT_NB, nref - p0), tid = threadIdx.x;
-    const double *G = Gall + (size_t) B * BT_NB * BT_NB;
     constexpr int LD = BT_NB + 1;
+    double *T = tsm;                       // BT_NB x LD
+    double *Gc = tsm + BT_NB * LD;         // column c of the Gram matrix
+    const int B = blockIdx.x, p0 = B * BT_NB, bb = min(BT_NB, nref - p0), tid = threadIdx.x;
+    const double *G = Gp + (size_t) B * GR_KS * BT_NB * BT_NB;
     for (int l = tid; l < BT_NB * LD; l += blockDim.x) T[l] = 0.0;
     __syncthreads();
     for (int c = 0; c < bb; c++) {
         const double tc = tau[p0 + c];
         if (tid < c) {
-            double s = 0.0;
-            for (int l = tid; l < c; l++) s += T[tid * LD + l] * G[(size_t) l * BT_NB + c];
-            T[tid * LD + c] = -tc * s;
+            double g = 0.0;
+            for (int ks = 0; ks < GR_KS; ks++) g += G[(size_t) ks * BT_NB * BT_NB + (size_t) tid * BT_NB + c];
+            Gc[tid] = g;
+        }
+        __syncthreads();
+        if (tid < c) {
+            double sacc = 0.0;
+            for (int l = tid; l < c; l++) sacc += T[tid * LD + l] * Gc[l];
+            T[tid * LD + c] = -tc * sacc;
         }
         if (tid == 0) T[c * LD + c] = tc;
         __syncthreads();
@@ -941,16 +1027,17 @@ Eig *eig_create(int n, cudaStream_t s)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const size_t dyn = sizeof(double) * (size_t) n;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sytrd_panel, TRD_THREADS, dyn);
-    E->G = std::max(1, std::min({nsm * std::max(per, 1), nsm, (n + 31) / 32}));
+    E->G = std::max(1, std::min({nsm * std::max(per, 1), nsm, (n + 7) / 8}));
     E->npanels = (n + TRD_NB - 1) / TRD_NB;
     E->nblk = (n - 1 + BT_NB - 1) / BT_NB;   // blocks of the n - 1 reflectors
     const size_t nn = (size_t) n * n;
     bool ok = ealloc(E, &E->A, nn) && ealloc(E, &E->VT, nn) && ealloc(E, &E->Qb, nn) && ealloc(E, &E->Us, nn) &&
               ealloc(E, &E->PVW, (size_t) 2 * TRD_NB * n) && ealloc(E, &E->PWV, (size_t) 2 * TRD_NB * n) &&
               ealloc(E, &E->Y, (size_t) n * BT_NB) && ealloc(E, &E->Y2, (size_t) n * BT_NB) && ealloc(E, &E->d, n) &&
-              ealloc(E, &E->e, n) && ealloc(E, &E->tau, n) && ealloc(E, &E->col, n) && ealloc(E, &E->y, n) &&
-              ealloc(E, &E->part, 2 * (size_t) E->G + TRD_NG * 2 * TRD_NB) &&
-              ealloc(E, &E->Gb, (size_t) std::max(E->nblk, 1) * BT_NB * BT_NB) &&
+              ealloc(E, &E->e, n) && ealloc(E, &E->tau, n) && ealloc(E, &E->col, n) &&
+              ealloc(E, &E->y, (size_t) ((n + TRD_SEG - 1) / TRD_SEG) * n) &&
+              ealloc(E, &E->part, (size_t) E->G * (2 + 2 * TRD_NB)) &&
+              ealloc(E, &E->Gb, (size_t) std::max(E->nblk, 1) * GR_KS * BT_NB * BT_NB) &&
               ealloc(E, &E->Tf, (size_t) std::max(E->nblk, 1) * BT_NB * BT_NB) && ealloc(E, &E->bar, 2) &&
               ealloc(E, &E->err, 1) && ealloc(E, &E->acc, 1);
     DcPos &P = E->pos;
@@ -1076,15 +1163,10 @@ int divide_conquer(Eig *E, cudaStream_t s, double **out)
 int back_transform(Eig *E, const double *Zc, double *d_V, cudaStream_t s)
 {
     const int n = E->n, nref = n - 1;
-    for (int B = 0; B < E->nblk; B++) {
-        const int p0 = B * BT_NB, bb = std::min(BT_NB, nref - p0);
-        const double *V = E->VT + (size_t) p0 * n + p0 + 1;   // bb x (n - p0 - 1), ld n
-        dgemm_untuned(false, true, bb, bb, n - p0 - 1, 1.0, V, n, V, n, 0.0, E->Gb + (size_t) B * BT_NB * BT_NB, BT_NB,
-                      s);
-    }
-    g_launches += 2;
-    g_eig_launches += 2 + E->nblk;
-    k_wy_tfactor<<<E->nblk, 256, sizeof(double) * BT_NB * (BT_NB + 1), s>>>(E->Gb, E->tau, E->Tf, nref);
+    g_launches += 3;
+    g_eig_launches += 3;
+    k_wy_gram<<<dim3(E->nblk, (BT_NB / 32) * (BT_NB / 32), GR_KS), 256, 0, s>>>(E->VT, E->Gb, n, nref);
+    k_wy_tfactor<<<E->nblk, 256, sizeof(double) * (BT_NB * (BT_NB + 1) + BT_NB), s>>>(E->Gb, E->tau, E->Tf, nref);
     k_transpose<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(Zc, d_V, n);
     for (int B = E->nblk - 1; B >= 0; B--) {
         const int p0 = B * BT_NB, bb = std::min(BT_NB, nref - p0), mv = n - p0 - 1;

@@ -240,14 +240,15 @@ void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
 
 // Tile shape from the call shape alone, for the many distinct shapes of the
 // eigensolver's panel updates (tuning each one would cost more than it saves):
-// the K-split tile for narrow outputs with a long K, the 128 x 128 DMMA tile
+// the K-split tile for outputs of few 64 x 64 tiles with a long K, the 128 x 128 DMMA tile
 // for large outputs, the 64 x 64 DMMA tile otherwise.
 void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda, const double *B,
                    int ldb, double beta, double *C, int ldc, cudaStream_t s)
 {
     if (m <= 0 || n <= 0) return;
     int v = 4;
-    if ((m <= 64 || n <= 64) && k >= 128) v = 5;
+    const double tiles64 = std::ceil(m / 64.0) * std::ceil(n / 64.0);
+    if (k >= 256 && tiles64 < 2.0 * 148) v = 5;
     else if ((double) m * n >= 4.0 * 148 * 128 * 128) v = 3;
     dgemm_variant(v, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
