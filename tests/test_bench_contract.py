@@ -40,6 +40,10 @@ class Engine:
     def counters(self): return [1000, 8 << 20, 100 << 20, 1, 16, 12345]
     def timing_stats(self): return {k: (4.0 * 45, 45) for k in TIMERS}
     def guess_used(self): return self.g
+    def build_FockMat(self): pass
+    def mat(self, name):
+        import numpy as np
+        return np.zeros((1010, 1010))
     def free(self): pass
 
 
@@ -83,3 +87,9 @@ def test_bench_line_has_the_contract_keys():
     assert d["gpu_launches"] == 0   # the stand-in's launch counter does not move
     assert set(d["clocks"]) >= {"sm_mhz", "sm_max_mhz", "reasons"}
     assert d["config"]["e2e_split"]["setup_device_ms"]["DFGEMM"] == 100.0
+    # errors against the reference's own results (tests/golden/c40h82_ref.npz) are stated
+    v = d["config"]["errors_vs_reference"]
+    for k in ("J_it0_maxabs", "K_it0_maxabs", "E_it0", "E_mixed_minus_reference_limit",
+              "E_plain_minus_reference_limit", "reference_limit"):
+        assert isinstance(v[k], float), k
+    assert abs(v["E_mixed_minus_reference_limit"] - (-1562.6 - v["reference_limit"])) < 1e-9
