@@ -89,7 +89,10 @@ TINYSCF_API int TinySCF_reset_timing_stats(TinySCF_t t);
  * host->device, [2] bytes copied device->host by this engine instance,
  * [3] full eigensolves and [4] occupied-subspace refinement steps taken by
  * the density builds of this instance, [5] (shell pair, aux shell) tuples the
- * last 3-centre integral build launched (before screening). */
+ * last 3-centre integral build launched (before screening), [6] restarts of
+ * TinySCF_do_SCF from the SAD guess by its divergence guard (an energy that is
+ * not finite, or one rising by more than 1e-6 Eh four iterations in a row;
+ * a second divergence in the same solve returns TINYSCF_ERR_NUMERIC). */
 TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
 /* Coulomb matrix J from a density D without allocating anything: for callers
  * that cannot call cudaMalloc (a host framework that owns all device memory

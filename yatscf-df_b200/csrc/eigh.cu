@@ -44,7 +44,7 @@ constexpr int GR_KS = 8;          // row slices of the reflector blocks' Gram ma
 constexpr int BT_NB = 128;        // reflectors per block of the back-transformation
 constexpr int DC_CHUNK = 256;     // items per CTA of the thread-per-item D&C kernels
 constexpr int DC_WCHUNK = 8;      // items per CTA of the warp-per-item D&C kernels (256 threads)
-constexpr long long kBarrierSpins = 1LL << 22;
+constexpr long long kBarrierSpins = 1LL << 22;   // acquire polls before a barrier gives up (~ 2 s)
 
 __device__ __forceinline__ double warp_sum_bcast(double v)
 {
@@ -102,34 +102,43 @@ __device__ double block_max_all(double v, double *sh)
     return r;
 }
 
-// Grid barrier for a cooperative launch (all CTAs co-resident): an arrival
-// counter and a generation word. The wait is bounded; on time-out the error
-// flag is set. Returns false (in every thread of the CTA) once the flag is
-// set, and the caller returns.
-__device__ bool grid_barrier(unsigned *bar, int *err, unsigned nblk)
+// Grid barrier for a cooperative launch (all CTAs co-resident): a 64-bit
+// ticket counter that only grows (zeroed before each solve). Thread 0 of each
+// CTA arrives with a release add and spins with acquire loads until the
+// counter reaches the end of its episode (the next multiple of nblk). The
+// wait is bounded: a CTA whose wait runs out sets the error flag and returns
+// false, and the caller returns; CTAs still waiting for it run out in turn.
+__device__ __forceinline__ unsigned long long atom_add_release(unsigned long long *p, unsigned long long v)
+{
+    unsigned long long old;
+    asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool grid_barrier(unsigned long long *bar, int *err, unsigned nblk)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
-        const unsigned g = *gen;
-        __threadfence();
-        if (atomicAdd(bar, 1u) == nblk - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            long long spins = 0;
-            while (*gen == g) {
-                if (++spins > kBarrierSpins) {
-                    atomicExch(err, 1);
-                    break;
-                }
-                __nanosleep(32);
+        const unsigned long long ticket = atom_add_release(bar, 1ull);
+        const unsigned long long target = (ticket / nblk + 1) * nblk;
+        long long spins = 0;
+        bool ok = true;
+        while (ld_acquire(bar) < target) {
+            if (++spins > kBarrierSpins) {
+                atomicExch(err, 1);
+                ok = false;
+                break;
             }
         }
-        __threadfence();
-        s_ok = (*(volatile int *) err == 0);
+        s_ok = ok;
     }
     __syncthreads();
     return s_ok != 0;
@@ -149,7 +158,7 @@ struct TrdArgs {
     double *col;
     double *y;      // [segment][row] partial sums of A v
     double *part;   // [G] norms | [2 TRD_NB][G] panel dots | [G] w.v
-    unsigned *bar;
+    unsigned long long *bar;
     int *err;
     int n, p, cols, G;
 };
@@ -873,7 +882,7 @@ struct Eig {
     // tridiagonalisation and back-transformation
     double *A = nullptr, *VT = nullptr, *PVW = nullptr, *PWV = nullptr, *d = nullptr, *e = nullptr, *tau = nullptr,
            *col = nullptr, *y = nullptr, *part = nullptr, *Gb = nullptr, *Tf = nullptr, *Y = nullptr, *Y2 = nullptr;
-    unsigned *bar = nullptr;
+    unsigned long long *bar = nullptr;
     int *err = nullptr;
     // divide and conquer: eigenvector buffers of alternate tree levels (Qa reuses A) and the merge's U
     double *Qb = nullptr, *Us = nullptr;
@@ -1053,7 +1062,7 @@ Eig *eig_create(int n, cudaStream_t s)
     }
     cudaMemset(P.colsrc, 0, sizeof(int) * n);
     cudaMemset(P.perm, 0, sizeof(int) * n);
-    cudaMemset(E->bar, 0, 2 * sizeof(unsigned));
+    cudaMemset(E->bar, 0, sizeof(unsigned long long));
     cudaMemset(E->err, 0, sizeof(int));
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
@@ -1089,7 +1098,7 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->VT, 0, sizeof(double) * nn, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->tau, 0, sizeof(double) * n, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->e, 0, sizeof(double) * n, s));
-    TSCF_CUDA_CHECK(cudaMemsetAsync(E->bar, 0, 2 * sizeof(unsigned), s));
+    TSCF_CUDA_CHECK(cudaMemsetAsync(E->bar, 0, sizeof(unsigned long long), s));
     const size_t dyn = sizeof(double) * (size_t) n;
     for (int P = 0; P < E->npanels; P++) {
         TrdArgs a;

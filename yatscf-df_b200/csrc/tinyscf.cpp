@@ -300,6 +300,7 @@ struct Engine {
     int dmode = TINYSCF_DENSITY_EIG;
     double *U = nullptr;          // occupied rows (nocc x nbf) in the orthogonal basis
     bool have_eig = false;        // V, w hold a full eigensolve of an earlier F'
+    long long guard_restarts = 0; // SCF restarts from the SAD guess by the divergence guard
     SubspaceWork sw{};
     long long n_eig = 0, n_refine = 0;
     long long n3c_quartets = 0;   // (shell pair, aux shell) tuples of the last DF build
@@ -1322,6 +1323,27 @@ int graph_iteration(TinySCF_t t, double *E)
 }
 
 // ------------------------------------------------------------------ SCF loop (TinySCF.c:378-435)
+// Divergence guard of the SCF loop: an energy that is not finite, or that
+// rises by more than kGuardRise Eh kGuardRises iterations in a row (from
+// iteration 2, where DIIS starts), restarts the solve once from the SAD guess
+// with an empty DIIS history; a second divergence in the same solve ends it
+// with ERR_NUMERIC. A converging SCF never triggers it (rises there are
+// rounding, far below kGuardRise), so it leaves the reference's iteration
+// sequence untouched.
+constexpr int kGuardRises = 4;
+constexpr double kGuardRise = 1e-6;
+
+int restart_from_sad(TinySCF_t t)
+{
+    Engine *e = E_(t);
+    const int mode = e->guess_mode;
+    e->guess_mode = TINYSCF_GUESS_SAD;
+    const int rc = TinySCF_reset_scf(t);
+    e->guess_mode = mode;
+    e->guard_restarts++;
+    return rc;
+}
+
 int scf_impl(TinySCF_t t)
 {
     Engine *e = E_(t);
@@ -1336,6 +1358,7 @@ int scf_impl(TinySCF_t t)
     cudaEventRecord(scf0, e->s);
     t->iter = 0;
     double prev_energy = 0, energy_delta = 223;
+    int rises = 0, restarts = 0;
     while ((t->iter < t->niters) && (energy_delta >= t->ene_tol)) {
         if (t->verbose) printf("--------------- Iteration %d ---------------\n", t->iter);
         double E = 0.0;
@@ -1353,12 +1376,25 @@ int scf_impl(TinySCF_t t)
         }
         tcollect(e);
         t->HF_energy = E;
+        rises = (t->iter >= 2 && E > prev_energy + kGuardRise) ? rises + 1 : 0;
+        if (!std::isfinite(E) || rises >= kGuardRises) {
+            if (restarts > 0) {
+                fprintf(stderr, "[tinyscf] SCF diverged again at iteration %d (energy %.10g): giving up\n", t->iter,
+                        E + t->nuc_energy);
+                return ERR_NUMERIC;
+            }
+            fprintf(stderr, "[tinyscf] SCF diverging at iteration %d (energy %.10g): restarting from the SAD guess\n",
+                    t->iter, E + t->nuc_energy);
+            RC(restart_from_sad(t));
+            restarts++;
+            rises = 0;
+            prev_energy = 0;
+            energy_delta = 223;
+            t->iter = 0;
+            continue;
+        }
         energy_delta = fabs(t->HF_energy - prev_energy);
         prev_energy = t->HF_energy;
-        if (!std::isfinite(E)) {
-            fprintf(stderr, "[tinyscf] SCF energy is not finite at iteration %d\n", t->iter);
-            return ERR_NUMERIC;
-        }
         if (t->verbose) {
             const double *tm = e->timers;
             printf("* Build Fock matrix     : %.3lf (s)\n", (tm[TINYSCF_T_J] + tm[TINYSCF_T_K_HT] + tm[TINYSCF_T_K_SYRK] + tm[TINYSCF_T_FOCK]) * 1e-3);
@@ -1781,8 +1817,8 @@ int TinySCF_get_counters(TinySCF_t t, long long *out, int n)
 {
     if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
-    long long v[6] = {g_launches, e->h2d, e->d2h, e->n_eig, e->n_refine, e->n3c_quartets};
-    for (int k = 0; k < n && k < 6; k++) out[k] = v[k];
+    long long v[7] = {g_launches, e->h2d, e->d2h, e->n_eig, e->n_refine, e->n3c_quartets, e->guard_restarts};
+    for (int k = 0; k < n && k < 7; k++) out[k] = v[k];
     return TINYSCF_OK;
 }
 

@@ -338,9 +338,10 @@ class TinySCF:
 
     def counters(self):
         """(engine kernel launches in this process, bytes host->device, bytes device->host,
-        full eigensolves, subspace refinement steps, 3-centre (shell pair, aux shell) tuples)."""
-        out = (ctypes.c_longlong * 6)()
-        self.lib.TinySCF_get_counters(self.t, out, 6)
+        full eigensolves, subspace refinement steps, 3-centre (shell pair, aux shell) tuples,
+        restarts from the SAD guess by the divergence guard)."""
+        out = (ctypes.c_longlong * 7)()
+        self.lib.TinySCF_get_counters(self.t, out, 7)
         return tuple(int(v) for v in out)
 
     def timings(self):
