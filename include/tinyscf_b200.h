@@ -238,6 +238,14 @@ TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iter
  * of the molecules set to TINYSCF_K_MIXED; min(n, 6) values. */
 TINYSCF_API int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n);
 TINYSCF_API int TinySCF_batch_free(TinySCF_batch_t b);
+/* Checks the tensor-core exchange kernels' bounded waits (no counterpart in
+ * the reference, which has no device code): runs one CTA of the G GEMM kernel
+ * of a handle set to TINYSCF_K_MIXED with no copies issued, so that its MMA
+ * and epilogue waits, limited to wait_cycles clock cycles, run out with
+ * nothing in flight; the kernel records the wait's code, frees its tensor
+ * memory and returns. *code receives that code (0 if no wait gave up); the
+ * flag is cleared afterwards and the handle stays usable. */
+TINYSCF_API int TinySCF_kmix_wait_probe(TinySCF_t t, long long wait_cycles, int *code);
 /* The engine's FP64 symmetric eigensolver on host buffers: A (n x n,
  * row-major, symmetric) -> w (n eigenvalues, ascending) and V (n x n, row k =
  * eigenvector k). It is what replaces the reference's LAPACKE_dsyev calls

@@ -54,8 +54,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
                  : "memory");
 }
 
-// Bounded wait on an mbarrier phase. Returns false (and records code) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, int code)
+// Bounded wait on an mbarrier phase (at most `limit` clock cycles). Returns
+// false (and records code) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, int code, long long limit = WAIT_CYCLES)
 {
     const uint32_t addr = smem_u32(bar);
     const long long t0 = clock64();
@@ -69,7 +70,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, int cod
             : "r"(addr), "r"(phase)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > WAIT_CYCLES) {
+        if (clock64() - t0 > limit) {
             atomicExch(&g_umma_error, code);
             return false;
         }
@@ -150,6 +151,10 @@ struct GArgs {               // split-K partial of dT S^T
     int nbf;
     int chunks_per_split;
     int total_chunks;
+    // Bounded-wait check (kmix_wait_probe): probe != 0 issues no copies, so the
+    // MMA and epilogue waits run out after wait_cycles with nothing in flight.
+    int probe = 0;
+    long long wait_cycles = WAIT_CYCLES;
 };
 
 constexpr int EPI_WARPS = 8;                  // two warps per TMEM lane quadrant
@@ -409,11 +414,11 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
+    if (warp == 0 && lane == 0 && !ga.probe) {
         bool ok = true;
         for (int kb = 0; kb < nk && ok; kb++) {
             const int s = kb % STAGES;
-            if (kb >= STAGES) ok = mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, 11);
+            if (kb >= STAGES) ok = mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, 11, ga.wait_cycles);
             if (!ok) break;
             unsigned char *st = smem + s * STAGE_BYTES;
             mbar_expect_tx(&full[s], STAGE_BYTES);
@@ -424,21 +429,21 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
             tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, &full[s], kx, n0);
         }
         for (int kb = (nk > STAGES ? nk - STAGES : 0); kb < nk; kb++)
-            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, 12);
+            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, 12, ga.wait_cycles);
     } else if (warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16(BN);
         bool ok = true;
         int kb = 0;
         for (int seg = 0; seg < nseg && ok; seg++) {
             const int b = seg & 1;
-            if (seg >= 2) ok = mbar_wait(&tempty[b], ((seg >> 1) - 1) & 1, 13);
+            if (seg >= 2) ok = mbar_wait(&tempty[b], ((seg >> 1) - 1) & 1, 13, ga.wait_cycles);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t acc_main = tmem + b * 256;
             const int kend = min(nk, (seg + 1) * SEG_CHUNKS);
             for (; kb < kend && ok; kb++) {
                 const int s = kb % STAGES;
-                ok = mbar_wait(&full[s], (kb / STAGES) & 1, 14);
+                ok = mbar_wait(&full[s], (kb / STAGES) & 1, 14, ga.wait_cycles);
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
@@ -465,7 +470,7 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
         bool ok = true;
         for (int seg = 0; seg < nseg && ok; seg++) {
             const int b = seg & 1;
-            ok = mbar_wait(&tfull[b], (seg >> 1) & 1, 15);
+            ok = mbar_wait(&tfull[b], (seg >> 1) & 1, 15, ga.wait_cycles);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
@@ -894,6 +899,33 @@ int kmix_error_flag()
     int v = 0;
     cudaMemcpyFromSymbol(&v, g_umma_error, sizeof(int));
     return v;
+}
+
+// The bounded-wait path of the G GEMM kernel, run on purpose: one CTA with
+// no copies issued, so its MMA warp waits on a stage that nothing fills and
+// its epilogue on an accumulator that nothing completes. Both waits give up
+// after wait_cycles, record their code, and the CTA frees its TMEM and
+// returns; nothing is in flight. Returns the recorded code (0 if no wait gave
+// up) and clears the flag again.
+int kmix_wait_probe(KMix *k, long long wait_cycles, int *code, cudaStream_t s)
+{
+    if (!k || !code || wait_cycles < 0) return ERR_INPUT;
+    const int zero = 0;
+    TSCF_CUDA_CHECK(cudaMemcpyToSymbolAsync(g_umma_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+    GArgs ga{k->G, k->nbf, k->chunks_per_split, k->total_chunks};
+    ga.probe = 1;
+    ga.wait_cycles = wait_cycles;
+    constexpr int STAGES = 3;
+    constexpr int SMEM = gemm_smem_bytes<128, STAGES>();
+    if (cudaFuncSetAttribute(k_gemm<STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+        return ERR_CUDA;
+    k_gemm<STAGES><<<dim3(1, 1, 1), THREADS, SMEM, s>>>(k->mdTh, k->mdTl, k->mSh, k->mSl, ga);
+    g_launches++;
+    TSCF_CUDA_CHECK(cudaGetLastError());
+    TSCF_CUDA_CHECK(cudaStreamSynchronize(s));
+    TSCF_CUDA_CHECK(cudaMemcpyFromSymbol(code, g_umma_error, sizeof(int)));
+    TSCF_CUDA_CHECK(cudaMemcpyToSymbol(g_umma_error, &zero, sizeof(int)));
+    return OK;
 }
 
 }  // namespace tscf

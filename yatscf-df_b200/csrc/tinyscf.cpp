@@ -2321,6 +2321,14 @@ int TinySCF_batch_free(TinySCF_batch_t b)
     return TINYSCF_OK;
 }
 
+int TinySCF_kmix_wait_probe(TinySCF_t t, long long wait_cycles, int *code)
+{
+    if (!t || !t->dev || !code) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (!e->kmix) return TINYSCF_ERR_STATE;
+    return kmix_wait_probe(e->kmix, wait_cycles, code, e->s);
+}
+
 int TinySCF_eigh(int device, int n, const double *A, double *w, double *V)
 {
     if (n < 1 || n > EIG_MAX_N || !A || !w || !V) return TINYSCF_ERR_INPUT;

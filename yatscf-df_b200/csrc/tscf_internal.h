@@ -193,6 +193,9 @@ void kmix_reset(KMix *k, cudaStream_t s);
 int  kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s,
                 const std::function<void(int)> &mark = nullptr);
 int  kmix_error_flag();
+// Runs the G GEMM kernel's bounded waits out on purpose (no copies issued,
+// waits of wait_cycles clock cycles); *code receives the recorded wait code.
+int  kmix_wait_probe(KMix *k, long long wait_cycles, int *code, cudaStream_t s);
 
 // ---------------------------------------------------------------- DIIS / density (scf.cu)
 struct DiisState {            // device-resident DIIS bookkeeping (DIIS.c:12-123)

@@ -128,6 +128,7 @@ def load_library(path=LIBPATH):
                                  ctypes.c_longlong], ctypes.c_longlong),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
         "TinySCF_eigh": ([ip, ip, dp, dp, dp], ip),
+        "TinySCF_kmix_wait_probe": ([T, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -320,6 +321,15 @@ class TinySCF:
         if got != n:
             raise TinySCFError("guess_dataset: %d" % got)
         return feat, tgt, typ
+
+    def kmix_wait_probe(self, wait_cycles):
+        """Code recorded by the tensor-core G GEMM kernel when its waits are run
+        out on purpose (wait_cycles clock cycles, no copies issued); 0 if none gave up."""
+        code = ctypes.c_int(0)
+        rc = self.lib.TinySCF_kmix_wait_probe(self.t, int(wait_cycles), ctypes.byref(code))
+        if rc:
+            raise TinySCFError("kmix_wait_probe: " + STATUS.get(rc, str(rc)))
+        return code.value
 
     def reset_scf(self):
         rc = self.lib.TinySCF_reset_scf(self.t)
