@@ -96,16 +96,20 @@ TINYSCF_API int TinySCF_reset_timing_stats(TinySCF_t t);
 TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
 /* Coulomb matrix J from a density D without allocating anything: for callers
  * that cannot call cudaMalloc (a host framework that owns all device memory
- * through its own pool, or code inside a CUDA-graph stream capture). No
- * counterpart in the reference. All pointers are device pointers: B holds one
+ * through its own pool, which an allocation made behind its back would
+ * escape). No counterpart in the reference. All pointers are device pointers: B holds one
  * DF-tensor row of naux doubles per pair, up_i/up_j/up_u list the nup upper
  * pairs (i <= j) and the B row of each, D and J are nbf x nbf row-major;
  * stream is a cudaStream_t (NULL = default stream). The call is asynchronous.
  * Scratch is a fixed 13.9 MB __device__ array inside the library (held on
  * every GPU that loads it until exit), so naux <= 4096 and nup <= 524288;
  * larger sizes return TINYSCF_ERR_UNSUPPORTED. The first call on a device
- * looks the array up (make it before any stream capture); calls that overlap
- * on the GPU share the array and race. */
+ * looks the array up and caches its address for the process (make it before
+ * any stream capture; not valid after cudaDeviceReset of that device); calls
+ * that overlap on the GPU share the array and race. The return code covers
+ * the arguments, that look-up and the launches (an error already pending on
+ * the calling thread is left pending and not reported); faults while the
+ * kernels run surface at the caller's next synchronisation. */
 TINYSCF_API int TinySCF_build_J_noalloc(const double *B, int naux, const int *up_i, const int *up_j,
                                         const int *up_u, int nup, int nbf, const double *D, double *J,
                                         void *stream);

@@ -1,8 +1,9 @@
 // A Coulomb (J) build that allocates nothing, for callers that cannot call
 // cudaMalloc: a host framework that owns every byte of device memory through
-// its own pool, or code running while a stream is being captured into a CUDA
-// graph (where a cudaMalloc is not allowed and would synchronise the device).
-// The caller passes all inputs and the output as device pointers; the
+// its own pool (an allocation made behind its back is memory its pool cannot
+// see or reclaim, and cudaMalloc can synchronise the device in the middle of
+// the framework's own pipeline). The caller passes all inputs and the output
+// as device pointers; the
 // per-block partial sums, the fitted vector t(P) and the pair weights that the
 // J build needs live in the file-scope array below instead of in buffers the
 // engine allocates.
@@ -12,8 +13,10 @@
 // loads this library, held until the process exits.
 //
 // The first call on a device looks up the array's device address with that
-// device current (cudaGetSymbolAddress) and caches it; make that first call
-// before any stream capture. Every call shares the one array, which keeps the
+// device current (cudaGetSymbolAddress) and caches it for the life of the
+// process; make that first call before any stream capture. The cached address
+// does not survive cudaDeviceReset: do not call this entry point on a device
+// after resetting it. Every call shares the one array, which keeps the
 // previous call's contents: calls that overlap on the GPU (other streams,
 // other host threads) race on it and must be serialised by the caller. No
 // part of the array has to start at zero: each call overwrites everything it
@@ -51,6 +54,8 @@ extern "C" int TinySCF_build_J_noalloc(const double *B, int naux, const int *up_
                         "fixed scratch of this entry point\n", naux, kMaxNaux, nup, kMaxPairs);
         return TINYSCF_ERR_UNSUPPORTED;
     }
+    // an error already pending on this thread is the caller's: left pending and not reported
+    const cudaError_t pending = cudaPeekAtLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TINYSCF_ERR_CUDA;
     double *scratch = nullptr;
@@ -85,5 +90,6 @@ extern "C" int TinySCF_build_J_noalloc(const double *B, int naux, const int *up_
     // J entries of screened pairs are never written by the J kernels: clear the output.
     if (cudaMemsetAsync(J, 0, sizeof(double) * (size_t) nbf * nbf, s) != cudaSuccess) return TINYSCF_ERR_CUDA;
     tscf::build_J(p, D, J, t, part, nblk, w, s);
-    return cudaGetLastError() == cudaSuccess ? TINYSCF_OK : TINYSCF_ERR_CUDA;
+    const cudaError_t launched = cudaPeekAtLastError();
+    return (launched == cudaSuccess || launched == pending) ? TINYSCF_OK : TINYSCF_ERR_CUDA;
 }

@@ -33,7 +33,7 @@
 
 namespace tscf {
 
-long long g_eig_launches = 0;
+std::atomic<long long> g_eig_launches{0};
 
 namespace {
 

@@ -15,7 +15,7 @@
 
 namespace tscf {
 
-long long g_launches = 0;
+std::atomic<long long> g_launches{0};
 
 // ------------------------------------------------------------------ DGEMM
 // Five tile shapes: FFMA 64x64 (default), 32x32 (more blocks for small

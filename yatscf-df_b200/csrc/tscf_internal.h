@@ -6,15 +6,17 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <functional>
 
 namespace tscf {
 
 // Number of engine kernels launched by this process (host-side count, read by
-// the benchmark; library kernels such as cuSOLVER's are not included).
-extern long long g_launches;
+// the benchmark); atomic, since the allocation-free J entry point may run on
+// other host threads than an engine instance.
+extern std::atomic<long long> g_launches;
 // The part of g_launches that the eigensolver (eigh.cu) launched.
-extern long long g_eig_launches;
+extern std::atomic<long long> g_eig_launches;
 
 // ---------------------------------------------------------------- limits
 constexpr int MAX_L_ORB = 2;           // orbital shells up to d
