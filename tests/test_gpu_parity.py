@@ -198,3 +198,27 @@ def test_small_molecules_against_restatement(tmp_path, name):
     f.do_SCF()
     assert abs(f.energy - Eo[-1]) < 1e-8, (f.energy, Eo[-1])
     f.free()
+
+
+def test_device_screening_structures_against_restatement():
+    """The unique shell pairs and the bf-pair CSR, built on the device
+    (TinySCF.c:183-280), equal the restatement's: same pairs in the same
+    order, same mask, columns, row starts and diagonal entries."""
+    o = oracle.OracleSCF(BAS, DFBAS, xyz("c10h22"), 30)
+    o.compute_Hcore_Ovlp_mat()
+    o.compute_sq_Schwarz_scrvals()
+    o.prepare_sparsity()
+    e = engine("c10h22")
+    e.compute_Hcore_Ovlp_mat()
+    e.compute_sq_Schwarz_scrvals()
+    e.prepare_sparsity()
+    k = e.s.num_uniq_sp
+    pairs = np.stack([e._mat("uniq_sp_lid", (k,)), e._mat("uniq_sp_rid", (k,))], axis=1)
+    assert np.array_equal(pairs, o.uniq_sp)
+    mask, cols, displs = e.csr()
+    assert np.array_equal(mask, o.bf_pair_mask)
+    assert np.array_equal(cols, o.bf_pair_j)
+    assert np.array_equal(displs, o.bf_mask_displs)
+    n = e.s.nbasfuncs
+    assert np.array_equal(e._mat("bf_pair_diag", (n,)), np.diag(o.bf_pair_mask))
+    e.free()

@@ -668,28 +668,34 @@ int schwarz_impl(TinySCF_t t)
     RC(cuda_rc("Schwarz quartets"));
     RC(sync_rc(e, "Schwarz"));
     tcollect(e);
+    // maxima and the unique shell pairs on the device (TinySCF.c:112-226); host mirrors of the results
+    double *mx_d = nullptr;
+    int *wk = nullptr, *first = nullptr, *second = nullptr;
+    RC(dalloc(e, &mx_d, 2));
+    RC(dalloc(e, &wk, (size_t) nsh * nsh + 2 * nsh + 1));
+    RC(dalloc(e, &first, (size_t) nsh * (nsh + 1) / 2));
+    RC(dalloc(e, &second, (size_t) nsh * (nsh + 1) / 2));
+    RC(device_max(e->sp_scr, (long long) nsh * nsh, mx_d, e->s));
+    RC(device_max(e->df_scr, t->df_nshells, mx_d + 1, e->s));
+    double mx[2] = {0.0, 0.0};
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(mx, mx_d, sizeof(mx), cudaMemcpyDeviceToHost, e->s));
+    RC(sync_rc(e, "screening maxima"));
+    t->max_scrval = mx[0];
+    t->max_df_scrval = mx[1];
+    const double eta = t->shell_scrtol2 / t->max_df_scrval;
+    int npairs = 0;
+    RC(device_unique_shell_pairs(e->sp_scr, e->dsh.am, nsh, eta, wk, first, second, &npairs, e->s));
+    RC(sync_rc(e, "unique shell pairs"));
+    t->num_uniq_sp = npairs;
+    d2h(e, t->uniq_sp_lid, first, sizeof(int) * npairs);
+    d2h(e, t->uniq_sp_rid, second, sizeof(int) * npairs);
     d2h(e, t->sp_scrval, e->sp_scr, sizeof(double) * nsh * nsh);
     d2h(e, t->bf_pair_scrval, e->bf_scr, sizeof(double) * e->nn);
     d2h(e, t->df_sp_scrval, e->df_scr, sizeof(double) * t->df_nshells);
-    double mx = 0.0, dmx = 0.0;
-    for (int i = 0; i < nsh * nsh; i++) mx = std::max(mx, t->sp_scrval[i]);
-    for (int i = 0; i < t->df_nshells; i++) dmx = std::max(dmx, t->df_sp_scrval[i]);
-    t->max_scrval = mx;
-    t->max_df_scrval = dmx;
-    const double eta = t->shell_scrtol2 / t->max_df_scrval;
-    std::vector<std::pair<int, int>> pairs;
-    for (int M = 0; M < nsh; M++)
-        for (int N = M; N < nsh; N++)
-            if (t->sp_scrval[M * nsh + N] > eta) {
-                int mn = e->sh.am[M] * 5 + e->sh.am[N], nm = e->sh.am[N] * 5 + e->sh.am[M];   // CMS_Simint.c:308-312
-                pairs.push_back(mn > nm ? std::make_pair(M, N) : std::make_pair(N, M));
-            }
-    std::sort(pairs.begin(), pairs.end());
-    t->num_uniq_sp = (int) pairs.size();
-    for (size_t k = 0; k < pairs.size(); k++) {
-        t->uniq_sp_lid[k] = pairs[k].first;
-        t->uniq_sp_rid[k] = pairs[k].second;
-    }
+    dfree(e, mx_d);
+    dfree(e, wk);
+    dfree(e, first);
+    dfree(e, second);
     t->shell_scr_time = e->timers[TINYSCF_T_SCHWARZ] * 1e-3;
     if (t->verbose)
         printf("TinySCF precompute shell screening info over,      elapsed time = %.3lf (s)\n", t->shell_scr_time);
@@ -704,55 +710,35 @@ int sparsity_impl(TinySCF_t t)
     if (!e || e->stage < 2) return ERR_STATE;
     const int nbf = t->nbasfuncs, naux = t->df_nbf, nocc = t->n_occ;
     const double eta = t->shell_scrtol2 / t->max_df_scrval;
-    int nnz = 0;
-    t->bf_mask_displs[0] = 0;
-    for (int i = 0; i < nbf; i++) {
-        for (int j = 0; j < nbf; j++) {
-            if (t->bf_pair_scrval[(size_t) i * nbf + j] > eta) {
-                t->bf_pair_mask[(size_t) i * nbf + j] = nnz;
-                t->bf_pair_j[nnz] = j;
-                nnz++;
-            } else {
-                t->bf_pair_mask[(size_t) i * nbf + j] = -1;
-            }
-        }
-        t->bf_pair_diag[i] = t->bf_pair_mask[(size_t) i * nbf + i];
-        t->bf_mask_displs[i + 1] = nnz;
-    }
+    // the bf-pair CSR (TinySCF.c:228-258), the unique pairs and the upper lists on the device
+    int *wk = nullptr, *mask = nullptr, *diag = nullptr;
+    RC(dalloc(e, &wk, (size_t) 5 * nbf + 2));
+    RC(dalloc(e, &mask, e->nn));
+    RC(dalloc(e, &diag, nbf));
+    RC(dalloc(e, &e->csr_displs, nbf + 1));
+    RC(dalloc(e, &e->upair, e->nn));
+    int totals[3] = {0, 0, 0};
+    RC(device_bf_counts(e->bf_scr, nbf, eta, wk, e->csr_displs, totals, e->s));
+    const int nnz = totals[0], nu = totals[1], nup = totals[2];
+    RC(dalloc(e, &e->csr_j, nnz));
+    RC(dalloc(e, &e->csr_u, nnz));
+    RC(dalloc(e, &e->up_i, nup));
+    RC(dalloc(e, &e->up_j, nup));
+    RC(dalloc(e, &e->up_u, nup));
+    RC(device_bf_fill(e->bf_scr, nbf, eta, wk, e->csr_displs, mask, diag, e->upair, e->csr_j, e->csr_u, e->up_i,
+                      e->up_j, e->up_u, e->s));
+    RC(sync_rc(e, "sparsity"));
+    d2h(e, t->bf_pair_mask, mask, sizeof(int) * e->nn);
+    d2h(e, t->bf_pair_j, e->csr_j, sizeof(int) * nnz);
+    d2h(e, t->bf_mask_displs, e->csr_displs, sizeof(int) * (nbf + 1));
+    d2h(e, t->bf_pair_diag, diag, sizeof(int) * nbf);
+    dfree(e, wk);
+    dfree(e, mask);
+    dfree(e, diag);
     t->num_bf_pair_scr = nnz;
     e->nnz = nnz;
-    // one DF-tensor row per unordered pair that survives in either order
-    std::vector<int> upair((size_t) nbf * nbf, -1);
-    int nu = 0;
-    for (int i = 0; i < nbf; i++)
-        for (int j = i; j < nbf; j++)
-            if (t->bf_pair_mask[(size_t) i * nbf + j] >= 0 || t->bf_pair_mask[(size_t) j * nbf + i] >= 0) {
-                upair[(size_t) i * nbf + j] = nu;
-                upair[(size_t) j * nbf + i] = nu;
-                nu++;
-            }
     e->nu = nu;
-    std::vector<int> csr_j(t->bf_pair_j, t->bf_pair_j + nnz), csr_u(nnz), displs(t->bf_mask_displs,
-                                                                               t->bf_mask_displs + nbf + 1);
-    std::vector<int> up_i, up_j, up_u;
-    for (int i = 0; i < nbf; i++)
-        for (int r = displs[i]; r < displs[i + 1]; r++) {
-            int j = csr_j[r];
-            csr_u[r] = upair[(size_t) i * nbf + j];
-            if (j >= i) {
-                up_i.push_back(i);
-                up_j.push_back(j);
-                up_u.push_back(csr_u[r]);
-            }
-        }
-    e->nup = (int) up_i.size();
-    RC(upload(e, &e->csr_j, csr_j));
-    RC(upload(e, &e->csr_u, csr_u));
-    RC(upload(e, &e->csr_displs, displs));
-    RC(upload(e, &e->up_i, up_i));
-    RC(upload(e, &e->up_j, up_j));
-    RC(upload(e, &e->up_u, up_u));
-    RC(upload(e, &e->upair, upair));
+    e->nup = nup;
     // 3-centre work list: unique shell pairs grouped by (am(M), am(N)) class
     std::vector<int2> pl;
     e->cls_start.clear();

@@ -98,6 +98,23 @@ void launch_three_center(const DevShells &sh, const DevShells &aux, const ThreeC
 void launch_two_center_grouped(const DevShells &aux, const int *d_ids, const int *h_start, const double *d_df_scr,
                                double scrtol2, double *d_Jpq, int naux, cudaStream_t s);
 
+// ---------------------------------------------------------------- screening structures (sparsity.cu)
+// *d_out = max of n doubles.
+int device_max(const double *d_x, long long n, double *d_out, cudaStream_t s);
+// Unique shell pairs of TinySCF.c:183-226 (sp_scr > eta, oriented by the
+// am(.)*5 + am(.) index, sorted) into d_first / d_second; *count (host) is
+// written once the stream reaches it. d_work: nsh^2 + 2 nsh + 1 ints.
+int device_unique_shell_pairs(const double *d_sp_scr, const int *d_am, int nsh, double eta, int *d_work,
+                              int *d_first, int *d_second, int *count, cudaStream_t s);
+// The bf-pair CSR of TinySCF.c:228-258 (bf_scr > eta) in two passes; d_work:
+// 5 n + 2 ints, d_displs: n + 1. Pass 1 returns the totals {ordered pairs,
+// unique pairs, upper CSR entries}; pass 2 fills the lists sized from them.
+int device_bf_counts(const double *d_bf_scr, int n, double eta, int *d_work, int *d_displs, int totals[3],
+                     cudaStream_t s);
+int device_bf_fill(const double *d_bf_scr, int n, double eta, const int *d_work, const int *d_displs, int *d_mask,
+                   int *d_diag, int *d_upair, int *d_csr_j, int *d_csr_u, int *d_up_i, int *d_up_j, int *d_up_u,
+                   cudaStream_t s);
+
 // ---------------------------------------------------------------- dense FP64 (linalg.cu)
 // C = alpha * op(A) * op(B) + beta * C, row-major, op = transpose if ta/tb.
 void dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, int lda,
