@@ -242,6 +242,20 @@ TINYSCF_API int TinySCF_batch_stats(TinySCF_batch_t b, double *scf_ms, int *iter
  * of the molecules set to TINYSCF_K_MIXED; min(n, 6) values. */
 TINYSCF_API int TinySCF_batch_phase_ms(TinySCF_batch_t b, double *ms, int n);
 TINYSCF_API int TinySCF_batch_free(TinySCF_batch_t b);
+/* Aux-partitioned Fock builds: one molecule over several GPUs, one process
+ * and handle per GPU (no counterpart in the reference, which runs on one
+ * node's cores). Called before TinySCF_build_DF_tensor, TinySCF_set_aux_slice
+ * makes the handle build and hold only the DF tensor's aux columns [p0, p1)
+ * (B = pqA (P|Q)^-1/2 restricted to those columns); TinySCF_build_FockMat then
+ * gives the slice's partial J and K, whose sums over a partition of
+ * [0, naux) are the full J and K (both are sums over the aux index).
+ * TinySCF_set_JK takes the summed J and K (host, nbf x nbf) and recomputes F
+ * and the energy as TinySCF_build_FockMat does; TinySCF_DIIS and
+ * TinySCF_build_DenMat follow unchanged. TinySCF_do_SCF refuses a sliced
+ * handle: the caller runs the loop with one reduction of [J | K] per
+ * iteration (yatscf-df_b200/auxsplit.py does, over torch.distributed). */
+TINYSCF_API int TinySCF_set_aux_slice(TinySCF_t t, int p0, int p1);
+TINYSCF_API int TinySCF_set_JK(TinySCF_t t, const double *J, const double *K);
 /* Checks the tensor-core exchange kernels' bounded waits (no counterpart in
  * the reference, which has no device code): runs one CTA of the G GEMM kernel
  * of a handle set to TINYSCF_K_MIXED with no copies issued, so that its MMA

@@ -288,6 +288,7 @@ struct Engine {
     int2 *pairs3c = nullptr;
     std::vector<int> cls_start, cls_la, cls_lb;
     double *B = nullptr;
+    int aux_p0 = 0, aux_ns = 0;   // aux columns [aux_p0, aux_p0 + aux_ns) of the DF tensor held (0: all)
     double *T = nullptr, *Kpart = nullptr;
     int2 *tiles = nullptr;
     int ksplit = 1, ksplit_max = 1, ksplit64 = 1, ktile = 64, khwide = 0;
@@ -331,7 +332,7 @@ struct Engine {
     {
         FockPlan p;
         p.nbf = sh.nbf;
-        p.naux = ash.nbf;
+        p.naux = aux_ns > 0 ? aux_ns : ash.nbf;
         p.nocc = 0;
         p.nnz = nnz;
         p.nup = nup;
@@ -1022,7 +1023,9 @@ int df_impl(TinySCF_t t)
     tstop(e, TINYSCF_T_INVSQRT);
     if (erc) { eig_destroy(eg); return erc; }
     tstart(e, TINYSCF_T_DFGEMM);
-    dgemm(false, false, e->nu, naux, naux, 1.0, pqA, naux, Jinv, naux, 0.0, e->B, naux, e->s);
+    // B = pqA (P|Q)^-1/2, or its aux columns [aux_p0, aux_p0 + aux_ns) for an aux-partitioned handle
+    const int ncol = e->aux_ns > 0 ? e->aux_ns : naux;
+    dgemm(false, false, e->nu, ncol, naux, 1.0, pqA, naux, Jinv + e->aux_p0, naux, 0.0, e->B, ncol, e->s);
     tstop(e, TINYSCF_T_DFGEMM);
     RC(cuda_rc("DF tensor GEMM"));
     int rc = sync_rc(e, "DF tensor");
@@ -1334,6 +1337,11 @@ int scf_impl(TinySCF_t t)
 {
     Engine *e = E_(t);
     if (!e || e->stage < 5) return ERR_STATE;
+    if (e->aux_ns > 0) {
+        fprintf(stderr, "[tinyscf] TinySCF_do_SCF: this handle holds a slice of the aux index; run the loop with a "
+                        "reduction of J and K over the slices (TinySCF_set_JK)\n");
+        return ERR_STATE;
+    }
     if (t->verbose) {
         printf("TinySCF SCF iteration started...\n");
         printf("Nuclear energy = %.10lf\n", t->nuc_energy);
@@ -1560,7 +1568,7 @@ int TinySCF_get_df_tensor(TinySCF_t t, double *out)
     if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
     if (e->stage < 5) return TINYSCF_ERR_STATE;
-    const int naux = t->df_nbf;
+    const int naux = e->aux_ns > 0 ? e->aux_ns : t->df_nbf;
     // one row per ordered CSR entry, gathered from the unique-pair tensor
     std::vector<int> cu(e->nnz);
     d2h(e, cu.data(), e->csr_u, sizeof(int) * e->nnz);
@@ -1585,9 +1593,9 @@ int TinySCF_set_k_precision(TinySCF_t t, int mode)
             if (rc) return rc;
             rc = dalloc(e, &e->Kmix, e->nn);
             if (rc) return rc;
-            rc = dalloc(e, &e->B32, (size_t) e->nu * t->df_nbf);
+            rc = dalloc(e, &e->B32, (size_t) e->nu * p.naux);
             if (rc) return rc;
-            convert_f32(e->B, e->B32, (size_t) e->nu * t->df_nbf, e->s);
+            convert_f32(e->B, e->B32, (size_t) e->nu * p.naux, e->s);
         }
         kmix_reset(e->kmix, e->s);
         if (sync_rc(e, "mixed K set-up")) return TINYSCF_ERR_CUDA;
@@ -2304,6 +2312,41 @@ int TinySCF_batch_free(TinySCF_batch_t b)
     if (!b) return TINYSCF_ERR_STATE;
     batch_free_impl(b);
     delete b;
+    return TINYSCF_OK;
+}
+
+int TinySCF_set_aux_slice(TinySCF_t t, int p0, int p1)
+{
+    if (!t || !t->dev) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (e->stage >= 5) return TINYSCF_ERR_STATE;   // before the DF tensor is built
+    if (p0 < 0 || p1 <= p0 || p1 > t->df_nbf) return TINYSCF_ERR_INPUT;
+    e->aux_p0 = p0;
+    e->aux_ns = (p0 == 0 && p1 == t->df_nbf) ? 0 : p1 - p0;
+    return TINYSCF_OK;
+}
+
+int TinySCF_set_JK(TinySCF_t t, const double *J, const double *K)
+{
+    if (!t || !t->dev || !J || !K) return TINYSCF_ERR_STATE;
+    Engine *e = E_(t);
+    if (e->stage < 5) return TINYSCF_ERR_STATE;
+    const size_t bytes = sizeof(double) * e->nn;
+    if (cudaMemcpyAsync(e->J, J, bytes, cudaMemcpyHostToDevice, e->s) != cudaSuccess ||
+        cudaMemcpyAsync(e->K, K, bytes, cudaMemcpyHostToDevice, e->s) != cudaSuccess)
+        return TINYSCF_ERR_CUDA;
+    e->h2d += (long long) (2 * bytes);
+    tstart(e, TINYSCF_T_FOCK);
+    build_F_energy(e->H, e->J, e->K, e->D, e->F, e->epart, t->nbasfuncs, e->s);
+    energy_reduce(e->epart, e->E, e->s);
+    tstop(e, TINYSCF_T_FOCK);
+    e->F_is_orth = false;
+    if (cuda_rc("Fock assembly") || sync_rc(e, "Fock assembly")) return TINYSCF_ERR_CUDA;
+    tcollect(e);
+    memcpy(t->J_mat, J, bytes);
+    memcpy(t->K_mat, K, bytes);
+    d2h(e, t->F_mat, e->F, bytes);
+    d2h(e, &t->HF_energy, e->E, sizeof(double));
     return TINYSCF_OK;
 }
 

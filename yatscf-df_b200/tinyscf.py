@@ -129,6 +129,8 @@ def load_library(path=LIBPATH):
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
         "TinySCF_eigh": ([ip, ip, dp, dp, dp], ip),
         "TinySCF_kmix_wait_probe": ([T, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)], ip),
+        "TinySCF_set_aux_slice": ([T, ip, ip], ip),
+        "TinySCF_set_JK": ([T, dp, dp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -321,6 +323,20 @@ class TinySCF:
         if got != n:
             raise TinySCFError("guess_dataset: %d" % got)
         return feat, tgt, typ
+
+    def set_aux_slice(self, p0, p1):
+        """Hold and use only the DF tensor's aux columns [p0, p1) (before build_DF_tensor)."""
+        rc = self.lib.TinySCF_set_aux_slice(self.t, int(p0), int(p1))
+        if rc:
+            raise TinySCFError("set_aux_slice: " + STATUS.get(rc, str(rc)))
+
+    def set_JK(self, J, K):
+        """Set the (reduced) J and K and recompute F and the energy."""
+        J = np.ascontiguousarray(J, dtype=np.float64)
+        K = np.ascontiguousarray(K, dtype=np.float64)
+        rc = self.lib.TinySCF_set_JK(self.t, _dptr(J), _dptr(K))
+        if rc:
+            raise TinySCFError("set_JK: " + STATUS.get(rc, str(rc)))
 
     def kmix_wait_probe(self, wait_cycles):
         """Code recorded by the tensor-core G GEMM kernel when its waits are run
