@@ -588,16 +588,36 @@ __global__ void __launch_bounds__(512) k_dc_deflate(DcNodes nd, DcPos ps, const 
 }
 
 // Block tables: entry b = (node, first item) for the items [first, first + chunk) of that node.
-__device__ double secular_f(const double *sd, const double *sz, int k, double rho, double dorg, double t, int lane)
+__device__ __forceinline__ void secular_parts(const double *sd, const double *sz, int k, int j, double rho,
+                                              double dorg, double t, int lane, double &p1, double &dp1, double &p2,
+                                              double &dp2)
 {
-    double s = 0.0;
-    for (int i = lane; i < k; i += 32) s += sz[i] * sz[i] / ((sd[i] - dorg) - t);
-    return 1.0 + rho * warp_sum_bcast(s);
+    double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+    for (int i = lane; i < k; i += 32) {
+        const double q = sz[i] / ((sd[i] - dorg) - t);
+        if (i <= j) {
+            a += sz[i] * q;
+            b += q * q;
+        } else {
+            c += sz[i] * q;
+            d += q * q;
+        }
+    }
+    p1 = rho * warp_sum_bcast(a);
+    dp1 = rho * warp_sum_bcast(b);
+    p2 = rho * warp_sum_bcast(c);
+    dp2 = rho * warp_sum_bcast(d);
 }
 
-// Roots of 1 + rho sum_i z_i^2 / (d_i - lambda) = 0, one warp per root:
-// lambda_j = pole + tau, pole the nearer of d_j, d_(j+1), tau found by
-// bisection (geometric while the bracket spans more than a factor 4).
+// Roots of f(l) = 1 + rho sum_i z_i^2 / (d_i - l) = 0, one warp per root:
+// l_j = pole + tau, the pole the nearer of d_j, d_(j+1) (its position is the
+// origin of tau, so tau keeps full relative accuracy), tau bracketed by the
+// signs of f. Each step fits psi1 + psi2 on either side of the root by
+// c + s / (pole - t) matched to value and slope at the current tau (the two
+// poles around the root) and takes the model's root inside the bracket;
+// a bisection step (geometric while the bracket spans more than a factor 4)
+// when it falls outside. Stops when the step is below 2 eps |tau| or the
+// bracket closes.
 __global__ void __launch_bounds__(256) k_dc_secular(DcNodes nd, DcPos ps, const int2 *tab)
 {
     extern __shared__ double dsm[];
@@ -619,33 +639,68 @@ __global__ void __launch_bounds__(256) k_dc_secular(DcNodes nd, DcPos ps, const 
         org = 0;
         tau = rho * sz[0] * sz[0];
     } else {
-        bool pos;
-        double hi;
-        if (j == k - 1) {
+        const bool last = j == k - 1;
+        double a, b;   // bracket in tau: f(a) < 0 < f(b)
+        if (last) {
             double s = 0.0;
             for (int i = lane; i < k; i += 32) s += sz[i] * sz[i];
-            hi = rho * warp_sum_bcast(s);
             org = j;
-            pos = true;
+            a = 0.0;
+            b = rho * warp_sum_bcast(s);
         } else {
             const double delta = sd[j + 1] - sd[j];
-            const double fm = secular_f(sd, sz, k, rho, sd[j], 0.5 * delta, lane);
-            pos = fm > 0.0;
-            org = pos ? j : j + 1;
-            hi = 0.5 * delta;
+            double p1, dp1, p2, dp2;
+            secular_parts(sd, sz, k, j, rho, sd[j], 0.5 * delta, lane, p1, dp1, p2, dp2);
+            if (1.0 + p1 + p2 > 0.0) {
+                org = j;
+                a = 0.0;
+                b = 0.5 * delta;
+            } else {
+                org = j + 1;
+                a = -0.5 * delta;
+                b = 0.0;
+            }
         }
-        const double sgn = pos ? 1.0 : -1.0, dorg = sd[org];
-        double lo_ = 0.0;
-        const double tiny = hi * 0x1p-200;
-        const double ft = secular_f(sd, sz, k, rho, dorg, sgn * tiny, lane);
-        if (pos ? (ft < 0.0) : (ft > 0.0)) lo_ = tiny;
-        for (int it = 0; it < 400; it++) {
-            const double midv = (lo_ > 0.0 && hi > 4.0 * lo_) ? sqrt(lo_ * hi) : 0.5 * (lo_ + hi);
-            if (!(midv > lo_ && midv < hi)) break;
-            const double fm = secular_f(sd, sz, k, rho, dorg, sgn * midv, lane);
-            if (pos ? (fm < 0.0) : (fm > 0.0)) lo_ = midv; else hi = midv;
+        const double dorg = sd[org];
+        const double del1 = sd[j] - dorg;                       // lower pole, relative
+        const double del2 = last ? 0.0 : sd[j + 1] - dorg;      // upper pole, relative
+        tau = 0.5 * (a + b);
+        for (int it = 0; it < 200; it++) {
+            double p1, dp1, p2, dp2;
+            secular_parts(sd, sz, k, j, rho, dorg, tau, lane, p1, dp1, p2, dp2);
+            const double f = 1.0 + p1 + p2;
+            if (f == 0.0) break;
+            if (f < 0.0) a = tau; else b = tau;
+            if (!(b - a > 4.0 * DBL_EPSILON * fmax(fabs(a), fabs(b)))) break;
+            // two-pole model: C + s1 / (del1 - x) + s2 / (del2 - x) = 0
+            const double e1 = del1 - tau, s1 = dp1 * e1 * e1, c1 = p1 - s1 / e1;
+            double x = NAN;
+            if (last) {
+                const double C = 1.0 + c1 + p2;
+                if (C > 0.0) x = del1 + s1 / C;
+            } else {
+                const double e2 = del2 - tau, s2 = dp2 * e2 * e2, c2 = p2 - s2 / e2;
+                const double C = 1.0 + c1 + c2;
+                const double qa = C, qb = -(C * (del1 + del2) + s1 + s2), qc = C * del1 * del2 + s1 * del2 + s2 * del1;
+                const double disc = qb * qb - 4.0 * qa * qc;
+                if (disc >= 0.0) {
+                    const double q = -0.5 * (qb + copysign(sqrt(disc), qb));
+                    const double r1 = q / qa, r2 = qc / q;
+                    const bool in1 = r1 > a && r1 < b, in2 = r2 > a && r2 < b;
+                    x = in1 && (!in2 || fabs(r1 - tau) < fabs(r2 - tau)) ? r1 : (in2 ? r2 : NAN);
+                }
+            }
+            if (!(x > a && x < b)) {   // bisection, geometric on the side of the origin while the bracket is wide
+                const double lo_ = fmin(fabs(a), fabs(b)), hi_ = fmax(fabs(a), fabs(b));
+                const double sg = (a + b) >= 0.0 ? 1.0 : -1.0;
+                x = (lo_ > 0.0 && hi_ > 4.0 * lo_ && a * b > 0.0) ? sg * sqrt(lo_ * hi_) : 0.5 * (a + b);
+                if (x == 0.0) x = 0.5 * (a + b);
+                if (!(x > a && x < b)) break;
+            }
+            const bool done = fabs(x - tau) <= 2.0 * DBL_EPSILON * fabs(x);
+            tau = x;
+            if (done) break;
         }
-        tau = sgn * 0.5 * (lo_ + hi);
     }
     if (lane == 0) {
         ps.lamb[lo + j] = sd[org];
