@@ -118,6 +118,23 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar)
                  : "memory");
 }
 
+// 32 lanes x 32 columns of FP32 from TMEM without waiting; tmem_wait_ld()
+// completes every load issued before it (so several loads overlap).
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r)
 {
     asm volatile(
@@ -475,13 +492,13 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
             for (int c0 = 0; c0 < WC; c0 += 32) {
-                tmem_ld32(tq + b * 256 + c0, r);
-                float t[32];
+                // main and correction columns in flight together, one wait
+                uint32_t r2[32];
+                tmem_ld32_nowait(tq + b * 256 + c0, r);
+                tmem_ld32_nowait(tq + b * 256 + 128 + c0, r2);
+                tmem_wait_ld();
 #pragma unroll
-                for (int q = 0; q < 32; q++) t[q] = __uint_as_float(r[q]);
-                tmem_ld32(tq + b * 256 + 128 + c0, r);
-#pragma unroll
-                for (int q = 0; q < 32; q++) acc[c0 + q] += t[q] + __uint_as_float(r[q]);
+                for (int q = 0; q < 32; q++) acc[c0 + q] += __uint_as_float(r[q]) + __uint_as_float(r2[q]);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
