@@ -63,7 +63,7 @@ __device__ __forceinline__ double warp_prod_bcast(double v)
 // Sum over the block in a fixed order (warp trees, then warp 0 over the
 // warps); the result is returned to every thread.
 template <int NT>
-__device__ double block_sum_all(double v, double *sh)
+__device__ __forceinline__ double block_sum_all(double v, double *sh)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -83,7 +83,7 @@ __device__ double block_sum_all(double v, double *sh)
 }
 
 template <int NT>
-__device__ double block_max_all(double v, double *sh)
+__device__ __forceinline__ double block_max_all(double v, double *sh)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -122,7 +122,7 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
     return v;
 }
 
-__device__ bool grid_barrier(unsigned long long *bar, int *err, unsigned nblk)
+__device__ __forceinline__ bool grid_barrier(unsigned long long *bar, int *err, unsigned nblk)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -168,49 +168,44 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
     extern __shared__ double sv[];   // v of the current column, by absolute row
     __shared__ double s_a2[TRD_NB], s_wv[TRD_NB], s_vv[TRD_NB], s_vj[TRD_NB], s_wj[TRD_NB];
     __shared__ double s_red[33];
+    __shared__ double s_dot[TRD_THREADS / 32][2 * TRD_NB];
     __shared__ double s_tau, s_scal, s_beta;
     const int n = a.n, p = a.p, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int gtid = blockIdx.x * TRD_THREADS + tid, GT = a.G * TRD_THREADS;
     const int gw = blockIdx.x * (TRD_THREADS / 32) + wid, GW = a.G * (TRD_THREADS / 32);
-    // row work: groups of 8 lanes per row, the panel columns split over the 8 lanes
-    const int l8 = lane & 7, grp = gtid >> 3, NGRP = GT >> 3;
+    // Row r of the matrix belongs to the 8-lane group r for the whole panel
+    // (G * TRD_THREADS / 8 >= n); lane l8 of the group keeps the row's entries
+    // of panel columns l8, l8 + 8, l8 + 16, l8 + 24 of V and W in registers.
+    const int l8 = lane & 7, r = gtid >> 3;
+    const bool own = r < n;
+    constexpr int NQ = TRD_NB / 8;
+    double pv[NQ], pw[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) pv[q] = pw[q] = 0.0;
     const int nseg = (n + TRD_SEG - 1) / TRD_SEG;
     double *part_n = a.part, *part_d = a.part + a.G, *part_w = part_d + (size_t) a.G * 2 * TRD_NB;
     const double *A = a.A;
-    const double *PV = a.PVW;          // row cc: v of panel column cc
-    double *PW = a.PWV;                // row cc: w of panel column cc (before its a2 v term)
+    // row p of the symmetric matrix: column p of the first step
+    double arow = (own && r >= p && l8 == 0) ? A[(size_t) p * n + r] : 0.0;
     for (int c = 0; c < a.cols; c++) {
         const int j = p + c;
-        // ---- phase 1: column j (rows j..n-1; row j of the symmetric matrix) minus the panel's corrections
-        if (tid < c) {
-            const double vj = PV[(size_t) tid * n + j];
-            s_vj[tid] = vj;
-            s_wj[tid] = PW[(size_t) tid * n + j] + s_a2[tid] * vj;
-        }
-        __syncthreads();
-        double ss = 0.0;
-        for (int r0 = j + (grp & ~3); r0 < n; r0 += NGRP) {   // warp-uniform trip count
-            const int r = r0 + (grp & 3);
-            double v = 0.0;
-            if (r < n) {
-                if (l8 == 0) v = A[(size_t) j * n + r];
+        // ---- phase 1: column j of the panel-corrected matrix, rows j..n-1 (s_vj, s_wj: row j's V and W)
+        double v = 0.0;
+        if (own && r >= j) {
+            v = arow;
 #pragma unroll
-                for (int q = 0; q < TRD_NB / 8; q++) {
-                    const int cc = l8 + 8 * q;
-                    if (cc < c) {
-                        const double vr = PV[(size_t) cc * n + r];
-                        const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
-                        v -= vr * s_wj[cc] + wr * s_vj[cc];
-                    }
-                }
+            for (int q = 0; q < NQ; q++) {
+                const int cc = l8 + 8 * q;
+                if (cc < c) v -= pv[q] * s_wj[cc] + pw[q] * s_vj[cc];
             }
-            v += __shfl_xor_sync(0xffffffff, v, 1);
-            v += __shfl_xor_sync(0xffffffff, v, 2);
-            v += __shfl_xor_sync(0xffffffff, v, 4);
-            if (r < n && l8 == 0) {
-                a.col[r] = v;
-                if (r >= j + 2) ss += v * v;
-            }
+        }
+        v += __shfl_xor_sync(0xffffffff, v, 1);
+        v += __shfl_xor_sync(0xffffffff, v, 2);
+        v += __shfl_xor_sync(0xffffffff, v, 4);
+        double ss = 0.0;
+        if (own && r >= j && l8 == 0) {
+            a.col[r] = v;
+            if (r >= j + 2) ss = v * v;
         }
         ss = block_sum_all<TRD_THREADS>(ss, s_red);
         if (tid == 0) part_n[blockIdx.x] = ss;
@@ -220,6 +215,7 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             break;
         }
         // ---- phase 2: reflector (every CTA forms the same one), v, y = A v by segments, panel dots
+        for (int rr = j + 1 + tid; rr < n; rr += TRD_THREADS) sv[rr] = a.col[rr];   // issued with part_n's loads
         if (wid == 0) {
             double s = 0.0;
             for (int b = lane; b < a.G; b += 32) s += part_n[b];
@@ -240,62 +236,78 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             }
         }
         __syncthreads();
-        const double tau = s_tau;
-        for (int r = j + 1 + tid; r < n; r += TRD_THREADS) sv[r] = (r == j + 1) ? 1.0 : a.col[r] * s_scal;
+        const double tau = s_tau, scal = s_scal;
+        for (int rr = j + 1 + tid; rr < n; rr += TRD_THREADS) sv[rr] = (rr == j + 1) ? 1.0 : sv[rr] * scal;
         __syncthreads();
         if (gtid == 0) {
             a.d[j] = a.col[j];
             a.e[j] = s_beta;
             a.tau[j] = tau;
         }
-        for (int r = j + 1 + gtid; r < n; r += GT) {
-            const double vr = sv[r];
-            a.VT[(size_t) j * n + r] = vr;
-            a.PVW[(size_t) c * n + r] = vr;
-            a.PWV[(size_t) (TRD_NB + c) * n + r] = vr;
+        for (int rr = j + 1 + gtid; rr < n; rr += GT) {
+            const double vr = sv[rr];
+            a.VT[(size_t) j * n + rr] = vr;
+            a.PVW[(size_t) c * n + rr] = vr;
+            a.PWV[(size_t) (TRD_NB + c) * n + rr] = vr;
+        }
+        const double vr_own = (own && r > j) ? sv[r] : 0.0;
+        if (l8 == (c & 7)) {   // this row's entry of the new reflector (static register indexing)
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+                if (q == (c >> 3)) pv[q] = vr_own;
         }
         {
-            // items (row r, segment s) over rows j+1..n-1 and the segments holding columns j+1..n-1
+            // items (row rr, segment sg) over rows j+1..n-1 and the segments holding columns j+1..n-1
             const int s0 = (j + 1) / TRD_SEG, ns = nseg - s0, m = n - j - 1;
             const long long nitems = (long long) m * ns;
             for (long long it = gw; it < nitems; it += GW) {
-                const int r = j + 1 + (int) (it / ns), sg = s0 + (int) (it % ns);
-                const double *row = A + (size_t) r * n;
+                const int rr = j + 1 + (int) (it / ns), sg = s0 + (int) (it % ns);
+                const double *row = A + (size_t) rr * n;
                 double acc[TRD_SEG / 32];
 #pragma unroll
                 for (int k = 0; k < TRD_SEG / 32; k++) {
                     const int c2 = sg * TRD_SEG + lane + 32 * k;
                     acc[k] = (c2 > j && c2 < n) ? row[c2] * sv[c2] : 0.0;
                 }
-#pragma unroll
-                for (int k = TRD_SEG / 64; k > 0; k >>= 1)
-#pragma unroll
-                    for (int q = 0; q < k; q++) acc[q] += acc[q + k];
-                const double y = warp_sum_bcast(acc[0]);
-                if (lane == 0) a.y[(size_t) sg * n + r] = y;
+                static_assert(TRD_SEG == 256, "the pairwise sum below is written for 8 values per lane");
+                const double y = warp_sum_bcast(((acc[0] + acc[4]) + (acc[2] + acc[6])) +
+                                                ((acc[1] + acc[5]) + (acc[3] + acc[7])));
+                if (lane == 0) a.y[(size_t) sg * n + rr] = y;
             }
         }
         if (c > 0) {
-            // this CTA's rows; warp w forms the dots of panel columns w and w + 16
-            const int m = n - j - 1, chunk = (m + a.G - 1) / a.G;
-            const int r0 = j + 1 + blockIdx.x * chunk, r1 = min(n, r0 + chunk);
-            for (int cc = wid; cc < c; cc += TRD_THREADS / 32) {
-                double aw = 0.0, av = 0.0;
-                for (int r = r0 + lane; r < r1; r += 32) {
-                    const double vr = sv[r], pv = PV[(size_t) cc * n + r];
-                    aw += (PW[(size_t) cc * n + r] + s_a2[cc] * pv) * vr;
-                    av += pv * vr;
+            // panel dots W^T v and V^T v over this CTA's rows, from the registers: groups of a warp
+            // (lanes with equal l8) summed by shuffles, then the warps in shared memory
+            double dw[NQ], dv[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                dw[q] = pw[q] * vr_own;
+                dv[q] = pv[q] * vr_own;
+                dw[q] += __shfl_xor_sync(0xffffffff, dw[q], 8);
+                dw[q] += __shfl_xor_sync(0xffffffff, dw[q], 16);
+                dv[q] += __shfl_xor_sync(0xffffffff, dv[q], 8);
+                dv[q] += __shfl_xor_sync(0xffffffff, dv[q], 16);
+            }
+            if (lane < 8) {
+#pragma unroll
+                for (int q = 0; q < NQ; q++) {
+                    s_dot[wid][lane + 8 * q] = dw[q];
+                    s_dot[wid][TRD_NB + lane + 8 * q] = dv[q];
                 }
-                aw = warp_sum_bcast(aw);
-                av = warp_sum_bcast(av);
-                if (lane == 0) {
-                    part_d[(size_t) cc * a.G + blockIdx.x] = aw;
-                    part_d[(size_t) (TRD_NB + cc) * a.G + blockIdx.x] = av;
-                }
+            }
+            __syncthreads();
+            if (tid < 2 * TRD_NB) {
+                double sacc = 0.0;
+                for (int w = 0; w < TRD_THREADS / 32; w++) sacc += s_dot[w][tid];
+                part_d[(size_t) tid * a.G + blockIdx.x] = sacc;
             }
         }
         if (!grid_barrier(a.bar, a.err, a.G)) return;
-        // ---- phase 3: w = tau (y - V (W^T v) - W (V^T v)), partial w.v
+        // ---- phase 3: w = tau (y - V (W^T v) - W (V^T v)) for this row, partial w.v
+        double ypart = 0.0;
+        const int s0 = (j + 1) / TRD_SEG;
+        if (own && r > j)
+            for (int sg = s0 + l8; sg < nseg; sg += 8) ypart += a.y[(size_t) sg * n + r];
         for (int cc = wid; cc < c; cc += TRD_THREADS / 32) {
             double sw = 0.0, sx = 0.0;
             for (int b = lane; b < a.G; b += 32) {
@@ -309,53 +321,65 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
                 s_vv[cc] = sx;
             }
         }
+        // the next column's row of A (issued here, used after the next two barriers)
+        const bool nxt = c + 1 < a.cols;
+        arow = (nxt && own && r >= j + 1 && l8 == 0) ? A[(size_t) (j + 1) * n + r] : 0.0;
         __syncthreads();
-        double wd = 0.0;
-        const int s0 = (j + 1) / TRD_SEG;
-        for (int r0 = j + 1 + (grp & ~3); r0 < n; r0 += NGRP) {
-            const int r = r0 + (grp & 3);
-            double t = 0.0;
-            if (r < n) {
-                for (int sg = s0 + l8; sg < nseg; sg += 8) t += a.y[(size_t) sg * n + r];
+        double t = ypart;
+        if (own && r > j) {
 #pragma unroll
-                for (int q = 0; q < TRD_NB / 8; q++) {
-                    const int cc = l8 + 8 * q;
-                    if (cc < c) {
-                        const double vr = PV[(size_t) cc * n + r];
-                        const double wr = PW[(size_t) cc * n + r] + s_a2[cc] * vr;
-                        t -= vr * s_wv[cc] + wr * s_vv[cc];
-                    }
-                }
+            for (int q = 0; q < NQ; q++) {
+                const int cc = l8 + 8 * q;
+                if (cc < c) t -= pv[q] * s_wv[cc] + pw[q] * s_vv[cc];
             }
-            t += __shfl_xor_sync(0xffffffff, t, 1);
-            t += __shfl_xor_sync(0xffffffff, t, 2);
-            t += __shfl_xor_sync(0xffffffff, t, 4);
-            if (r < n && l8 == 0) {
-                const double w = tau * t;
-                PW[(size_t) c * n + r] = w;
-                wd += w * sv[r];
-            }
+        }
+        t += __shfl_xor_sync(0xffffffff, t, 1);
+        t += __shfl_xor_sync(0xffffffff, t, 2);
+        t += __shfl_xor_sync(0xffffffff, t, 4);
+        const double w = (own && r > j) ? tau * t : 0.0;
+        if (l8 == (c & 7)) {
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+                if (q == (c >> 3)) pw[q] = w;
+        }
+        double wd = 0.0;
+        if (own && r > j && l8 == 0) {
+            a.PWV[(size_t) c * n + r] = w;   // before its a2 v term; row j+1's entry is read by every CTA
+            wd = w * vr_own;
         }
         wd = block_sum_all<TRD_THREADS>(wd, s_red);
         if (tid == 0) part_w[blockIdx.x] = wd;
         if (!grid_barrier(a.bar, a.err, a.G)) return;
-        // ---- phase 4: w += a2 v with a2 = -tau/2 (w.v); kept as s_a2 and folded in lazily
+        // ---- phase 4: a2 = -tau/2 (w.v), w += a2 v; row j+1's V and W for the next column
         if (wid == 0) {
             double s = 0.0;
             for (int b = lane; b < a.G; b += 32) s += part_w[b];
             s = warp_sum_bcast(s);
             if (lane == 0) s_a2[c] = -0.5 * tau * s;
+        } else if (nxt && wid == 1 && lane <= c) {
+            s_vj[lane] = a.PVW[(size_t) lane * n + j + 1];
+            s_wj[lane] = a.PWV[(size_t) lane * n + j + 1];   // before a2 v; completed below
         }
         __syncthreads();
-    }
-    // final w of the rows the trailing update reads, in both stacked panels
-    const int q = p + a.cols;
-    for (int r = q + gtid; r < n; r += GT)
-        for (int cc = 0; cc < a.cols; cc++) {
-            const double w = PW[(size_t) cc * n + r] + s_a2[cc] * PV[(size_t) cc * n + r];
-            PW[(size_t) cc * n + r] = w;
-            a.PVW[(size_t) (TRD_NB + cc) * n + r] = w;
+        if (l8 == (c & 7)) {
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+                if (q == (c >> 3)) pw[q] += s_a2[c] * pv[q];
         }
+        if (nxt && tid <= c) s_wj[tid] += s_a2[tid] * s_vj[tid];   // global W holds the values before a2 v
+        __syncthreads();
+    }
+    // final W of this panel's rows, into both stacked panels for the trailing update
+    if (own && r >= p + a.cols) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const int cc = l8 + 8 * q;
+            if (cc < a.cols) {
+                a.PWV[(size_t) cc * n + r] = pw[q];
+                a.PVW[(size_t) (TRD_NB + cc) * n + r] = pw[q];
+            }
+        }
+    }
 }
 
 // Partial Gram matrices V_B^T V_B of the reflector blocks (the reflectors of
@@ -1092,6 +1116,11 @@ Eig *eig_create(int n, cudaStream_t s)
     const size_t dyn = sizeof(double) * (size_t) n;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sytrd_panel, TRD_THREADS, dyn);
     E->G = std::max(1, std::min({nsm * std::max(per, 1), nsm, (n + 7) / 8}));
+    if ((long long) E->G * TRD_THREADS / 8 < n) {   // the panel kernel gives every row its own 8 lanes
+        fprintf(stderr, "[tinyscf] eigensolver: %d CTAs cannot hold %d rows\n", E->G, n);
+        delete E;
+        return nullptr;
+    }
     E->npanels = (n + TRD_NB - 1) / TRD_NB;
     E->nblk = (n - 1 + BT_NB - 1) / BT_NB;   // blocks of the n - 1 reflectors
     const size_t nn = (size_t) n * n;
