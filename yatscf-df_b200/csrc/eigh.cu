@@ -155,80 +155,22 @@ struct TrdArgs {
     double *VT;     // n x n reflectors as rows
     double *PVW, *PWV;   // 2 TRD_NB x n each
     double *d, *e, *tau;
-    double *col;    // the next column before the a2 term of the current one (b)
+    double *col;
     double *y;      // [segment][row] partial sums of A v
-    double *part;   // [2 TRD_NB][G] panel dots | [G] w.v
+    double *part;   // [G] norms | [2 TRD_NB][G] panel dots | [G] w.v
     unsigned long long *bar;
     int *err;
     int n, p, cols, G;
 };
 
-// w (before its a2 term) of one row, by the row's 8-lane group: tau (y_row -
-// V_row . (W^T v) - W_row . (V^T v)); ypart is this lane's share of the row's
-// segment sums of y, pvq / pwq the row's V and W of panel columns l8 + 8q.
-// The owner of the row and every CTA's replica of row j+1 run this same code
-// on the same numbers, so they get the same bits.
-template <int NQ>
-__device__ __forceinline__ double row_wpre(double ypart, const double *pvq, const double *pwq, int l8, int c,
-                                           double tau, const double *wv, const double *vv)
-{
-    double t = ypart;
-#pragma unroll
-    for (int q = 0; q < NQ; q++) {
-        const int cc = l8 + 8 * q;
-        if (cc < c) t = __fma_rn(-pvq[q], wv[cc], __fma_rn(-pwq[q], vv[cc], t));   // explicit: the same bits in every copy
-    }
-    t += __shfl_xor_sync(0xffffffff, t, 1);
-    t += __shfl_xor_sync(0xffffffff, t, 2);
-    t += __shfl_xor_sync(0xffffffff, t, 4);
-    return tau * t;
-}
-
-// Householder reflector of column jj (rows jj..n-1 in scol), formed the same
-// way by every CTA: sigma = sum_(r >= jj+2) scol[r]^2 summed in a fixed order,
-// v into sv (v[jj+1] = 1), tau into *s_tau; CTA 0 writes d, e, tau.
-__device__ __forceinline__ void form_reflector(const double *scol, double *sv, int jj, int n, double *s_red,
-                                               double *s_tau, double *s_scal, double *s_beta, double *d, double *e,
-                                               double *tauv)
-{
-    double ss = 0.0;
-    for (int rr = jj + 2 + threadIdx.x; rr < n; rr += blockDim.x) ss += scol[rr] * scol[rr];
-    ss = block_sum_all<TRD_THREADS>(ss, s_red);
-    if (threadIdx.x == 0) {
-        const double alpha = scol[jj + 1];
-        if (ss == 0.0) {
-            *s_tau = 0.0;
-            *s_beta = alpha;
-            *s_scal = 0.0;
-        } else {
-            const double nrm = sqrt(alpha * alpha + ss);
-            const double beta = alpha >= 0.0 ? -nrm : nrm;
-            *s_tau = (beta - alpha) / beta;
-            *s_beta = beta;
-            *s_scal = 1.0 / (alpha - beta);
-        }
-    }
-    __syncthreads();
-    const double scal = *s_scal;
-    for (int rr = jj + 1 + threadIdx.x; rr < n; rr += blockDim.x) sv[rr] = (rr == jj + 1) ? 1.0 : scol[rr] * scal;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        d[jj] = scol[jj];
-        e[jj] = *s_beta;
-        tauv[jj] = *s_tau;
-    }
-    __syncthreads();
-}
-
 __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
 {
-    extern __shared__ double smx[];
-    const int n = a.n, p = a.p, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    double *sv = smx;          // v of the current column, by absolute row
-    double *scol = smx + n;    // the next column of the panel-corrected matrix, by absolute row
+    extern __shared__ double sv[];   // v of the current column, by absolute row
     __shared__ double s_a2[TRD_NB], s_wv[TRD_NB], s_vv[TRD_NB], s_vj[TRD_NB], s_wj[TRD_NB];
     __shared__ double s_red[33];
     __shared__ double s_dot[TRD_THREADS / 32][2 * TRD_NB];
-    __shared__ double s_tau, s_scal, s_beta, s_wn;
+    __shared__ double s_tau, s_scal, s_beta;
+    const int n = a.n, p = a.p, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int gtid = blockIdx.x * TRD_THREADS + tid, GT = a.G * TRD_THREADS;
     const int gw = blockIdx.x * (TRD_THREADS / 32) + wid, GW = a.G * (TRD_THREADS / 32);
     // Row r of the matrix belongs to the 8-lane group r for the whole panel
@@ -241,21 +183,67 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
 #pragma unroll
     for (int q = 0; q < NQ; q++) pv[q] = pw[q] = 0.0;
     const int nseg = (n + TRD_SEG - 1) / TRD_SEG;
-    double *part_d = a.part, *part_w = part_d + (size_t) a.G * 2 * TRD_NB;
+    double *part_n = a.part, *part_d = a.part + a.G, *part_w = part_d + (size_t) a.G * 2 * TRD_NB;
     const double *A = a.A;
-    // the panel's first column: row p of the (symmetric) trailing matrix, read by every CTA
-    for (int rr = p + tid; rr < n; rr += TRD_THREADS) scol[rr] = A[(size_t) p * n + rr];
-    __syncthreads();
-    if (p == n - 1) {
-        if (gtid == 0) a.d[p] = scol[p];
-        return;
-    }
-    form_reflector(scol, sv, p, n, s_red, &s_tau, &s_scal, &s_beta, a.d, a.e, a.tau);
+    // row p of the symmetric matrix: column p of the first step
+    double arow = (own && r >= p && l8 == 0) ? A[(size_t) p * n + r] : 0.0;
     for (int c = 0; c < a.cols; c++) {
-        const int j = p + c;                        // sv holds v_j, s_tau tau_j
-        const bool more = c + 1 < a.cols;           // this launch forms column j + 1 too
-        const double tau = s_tau;
-        // ---- phase A: store v, y = A v by segments, panel dots; prefetch row j+1's data
+        const int j = p + c;
+        // ---- phase 1: column j of the panel-corrected matrix, rows j..n-1 (s_vj, s_wj: row j's V and W)
+        double v = 0.0;
+        if (own && r >= j) {
+            v = arow;
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const int cc = l8 + 8 * q;
+                if (cc < c) v -= pv[q] * s_wj[cc] + pw[q] * s_vj[cc];
+            }
+        }
+        v += __shfl_xor_sync(0xffffffff, v, 1);
+        v += __shfl_xor_sync(0xffffffff, v, 2);
+        v += __shfl_xor_sync(0xffffffff, v, 4);
+        double ss = 0.0;
+        if (own && r >= j && l8 == 0) {
+            a.col[r] = v;
+            if (r >= j + 2) ss = v * v;
+        }
+        ss = block_sum_all<TRD_THREADS>(ss, s_red);
+        if (tid == 0) part_n[blockIdx.x] = ss;
+        if (!grid_barrier(a.bar, a.err, a.G)) return;
+        if (j == n - 1) {
+            if (gtid == 0) a.d[j] = a.col[j];
+            break;
+        }
+        // ---- phase 2: reflector (every CTA forms the same one), v, y = A v by segments, panel dots
+        for (int rr = j + 1 + tid; rr < n; rr += TRD_THREADS) sv[rr] = a.col[rr];   // issued with part_n's loads
+        if (wid == 0) {
+            double s = 0.0;
+            for (int b = lane; b < a.G; b += 32) s += part_n[b];
+            s = warp_sum_bcast(s);
+            if (lane == 0) {
+                const double alpha = a.col[j + 1];
+                if (s == 0.0) {
+                    s_tau = 0.0;
+                    s_beta = alpha;
+                    s_scal = 0.0;
+                } else {
+                    const double nrm = sqrt(alpha * alpha + s);
+                    const double beta = alpha >= 0.0 ? -nrm : nrm;
+                    s_tau = (beta - alpha) / beta;
+                    s_beta = beta;
+                    s_scal = 1.0 / (alpha - beta);
+                }
+            }
+        }
+        __syncthreads();
+        const double tau = s_tau, scal = s_scal;
+        for (int rr = j + 1 + tid; rr < n; rr += TRD_THREADS) sv[rr] = (rr == j + 1) ? 1.0 : sv[rr] * scal;
+        __syncthreads();
+        if (gtid == 0) {
+            a.d[j] = a.col[j];
+            a.e[j] = s_beta;
+            a.tau[j] = tau;
+        }
         for (int rr = j + 1 + gtid; rr < n; rr += GT) {
             const double vr = sv[rr];
             a.VT[(size_t) j * n + rr] = vr;
@@ -263,18 +251,13 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             a.PWV[(size_t) (TRD_NB + c) * n + rr] = vr;
         }
         const double vr_own = (own && r > j) ? sv[r] : 0.0;
-        if (l8 == (c & 7)) {
+        if (l8 == (c & 7)) {   // this row's entry of the new reflector (static register indexing)
 #pragma unroll
             for (int q = 0; q < NQ; q++)
                 if (q == (c >> 3)) pv[q] = vr_own;
         }
-        const double arow = (more && own && r >= j + 1 && l8 == 0) ? A[(size_t) (j + 1) * n + r] : 0.0;
-        if (more && tid < c) {                      // row j+1's V and final W of the earlier panel columns
-            const double vj = a.PVW[(size_t) tid * n + j + 1];
-            s_vj[tid] = vj;
-            s_wj[tid] = __fma_rn(s_a2[tid], vj, a.PWV[(size_t) tid * n + j + 1]);
-        }
         {
+            // items (row rr, segment sg) over rows j+1..n-1 and the segments holding columns j+1..n-1
             const int s0 = (j + 1) / TRD_SEG, ns = nseg - s0, m = n - j - 1;
             const long long nitems = (long long) m * ns;
             for (long long it = gw; it < nitems; it += GW) {
@@ -293,6 +276,8 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             }
         }
         if (c > 0) {
+            // panel dots W^T v and V^T v over this CTA's rows, from the registers: groups of a warp
+            // (lanes with equal l8) summed by shuffles, then the warps in shared memory
             double dw[NQ], dv[NQ];
 #pragma unroll
             for (int q = 0; q < NQ; q++) {
@@ -318,9 +303,9 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
             }
         }
         if (!grid_barrier(a.bar, a.err, a.G)) return;
-        // ---- phase B: w of this CTA's rows (before a2), row j+1's w in every CTA, the next column's b
-        const int s0 = (j + 1) / TRD_SEG;
+        // ---- phase 3: w = tau (y - V (W^T v) - W (V^T v)) for this row, partial w.v
         double ypart = 0.0;
+        const int s0 = (j + 1) / TRD_SEG;
         if (own && r > j)
             for (int sg = s0 + l8; sg < nseg; sg += 8) ypart += a.y[(size_t) sg * n + r];
         for (int cc = wid; cc < c; cc += TRD_THREADS / 32) {
@@ -336,73 +321,53 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) k_sytrd_panel(TrdArgs a)
                 s_vv[cc] = sx;
             }
         }
+        // the next column's row of A (issued here, used after the next two barriers)
+        const bool nxt = c + 1 < a.cols;
+        arow = (nxt && own && r >= j + 1 && l8 == 0) ? A[(size_t) (j + 1) * n + r] : 0.0;
         __syncthreads();
-        const double wpre = row_wpre<NQ>(ypart, pv, pw, l8, c, tau, s_wv, s_vv);
-        const double w_own = (own && r > j) ? wpre : 0.0;
+        double t = ypart;
+        if (own && r > j) {
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const int cc = l8 + 8 * q;
+                if (cc < c) t -= pv[q] * s_wv[cc] + pw[q] * s_vv[cc];
+            }
+        }
+        t += __shfl_xor_sync(0xffffffff, t, 1);
+        t += __shfl_xor_sync(0xffffffff, t, 2);
+        t += __shfl_xor_sync(0xffffffff, t, 4);
+        const double w = (own && r > j) ? tau * t : 0.0;
         if (l8 == (c & 7)) {
 #pragma unroll
             for (int q = 0; q < NQ; q++)
-                if (q == (c >> 3)) pw[q] = w_own;
+                if (q == (c >> 3)) pw[q] = w;
         }
-        if (more && wid == 0) {                      // replica of row j+1's group
-            double yp = 0.0;
-            for (int sg = s0 + l8; sg < nseg; sg += 8) yp += a.y[(size_t) sg * n + j + 1];
-            double pvq[NQ], pwq[NQ];
-#pragma unroll
-            for (int q = 0; q < NQ; q++) {
-                const int cc = l8 + 8 * q;
-                pvq[q] = cc < c ? s_vj[cc] : 0.0;
-                pwq[q] = cc < c ? s_wj[cc] : 0.0;
-            }
-            const double wn = row_wpre<NQ>(yp, pvq, pwq, l8, c, tau, s_wv, s_vv);
-            if (lane == 0) s_wn = wn;
-        }
-        __syncthreads();
-        double bsum = 0.0;
-        if (more && own && r >= j + 1) {             // b = column j+1 before the a2 term of column j
-            bsum = arow;
-#pragma unroll
-            for (int q = 0; q < NQ; q++) {
-                const int cc = l8 + 8 * q;
-                if (cc < c) bsum -= pv[q] * s_wj[cc] + pw[q] * s_vj[cc];
-            }
-        }
-        bsum += __shfl_xor_sync(0xffffffff, bsum, 1);
-        bsum += __shfl_xor_sync(0xffffffff, bsum, 2);
-        bsum += __shfl_xor_sync(0xffffffff, bsum, 4);
         double wd = 0.0;
-        if (own && l8 == 0) {
-            if (r > j) {
-                a.PWV[(size_t) c * n + r] = w_own;   // before its a2 v term
-                wd = w_own * vr_own;
-            }
-            if (more && r >= j + 1) a.col[r] = bsum - ((r == j + 1 ? 1.0 : vr_own) * s_wn + w_own);
+        if (own && r > j && l8 == 0) {
+            a.PWV[(size_t) c * n + r] = w;   // before its a2 v term; row j+1's entry is read by every CTA
+            wd = w * vr_own;
         }
         wd = block_sum_all<TRD_THREADS>(wd, s_red);
         if (tid == 0) part_w[blockIdx.x] = wd;
         if (!grid_barrier(a.bar, a.err, a.G)) return;
-        // ---- phase C: a2 = -tau/2 (w.v), w += a2 v; column j+1 = b - 2 a2 v and its reflector, in every CTA
+        // ---- phase 4: a2 = -tau/2 (w.v), w += a2 v; row j+1's V and W for the next column
         if (wid == 0) {
             double s = 0.0;
             for (int b = lane; b < a.G; b += 32) s += part_w[b];
             s = warp_sum_bcast(s);
             if (lane == 0) s_a2[c] = -0.5 * tau * s;
+        } else if (nxt && wid == 1 && lane <= c) {
+            s_vj[lane] = a.PVW[(size_t) lane * n + j + 1];
+            s_wj[lane] = a.PWV[(size_t) lane * n + j + 1];   // before a2 v; completed below
         }
         __syncthreads();
-        const double a2 = s_a2[c];
         if (l8 == (c & 7)) {
 #pragma unroll
             for (int q = 0; q < NQ; q++)
-                if (q == (c >> 3)) pw[q] = __fma_rn(a2, pv[q], pw[q]);
+                if (q == (c >> 3)) pw[q] += s_a2[c] * pv[q];
         }
-        if (!more) break;
-        for (int rr = j + 1 + tid; rr < n; rr += TRD_THREADS) scol[rr] = a.col[rr] - 2.0 * a2 * sv[rr];
+        if (nxt && tid <= c) s_wj[tid] += s_a2[tid] * s_vj[tid];   // global W holds the values before a2 v
         __syncthreads();
-        if (j + 1 == n - 1) {
-            if (gtid == 0) a.d[j + 1] = scol[j + 1];
-            break;
-        }
-        form_reflector(scol, sv, j + 1, n, s_red, &s_tau, &s_scal, &s_beta, a.d, a.e, a.tau);
     }
     // final W of this panel's rows, into both stacked panels for the trailing update
     if (own && r >= p + a.cols) {
@@ -1148,7 +1113,7 @@ Eig *eig_create(int n, cudaStream_t s)
     int dev = 0, nsm = 1, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const size_t dyn = 2 * sizeof(double) * (size_t) n;
+    const size_t dyn = sizeof(double) * (size_t) n;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sytrd_panel, TRD_THREADS, dyn);
     E->G = std::max(1, std::min({nsm * std::max(per, 1), nsm, (n + 7) / 8}));
     if ((long long) E->G * TRD_THREADS / 8 < n) {   // the panel kernel gives every row its own 8 lanes
@@ -1218,7 +1183,7 @@ int tridiagonalize(Eig *E, const double *d_A, cudaStream_t s)
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->tau, 0, sizeof(double) * n, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->e, 0, sizeof(double) * n, s));
     TSCF_CUDA_CHECK(cudaMemsetAsync(E->bar, 0, sizeof(unsigned long long), s));
-    const size_t dyn = 2 * sizeof(double) * (size_t) n;   // v and the next column
+    const size_t dyn = sizeof(double) * (size_t) n;
     for (int P = 0; P < E->npanels; P++) {
         TrdArgs a;
         a.A = E->A;
