@@ -92,7 +92,11 @@ TINYSCF_API int TinySCF_reset_timing_stats(TinySCF_t t);
  * last 3-centre integral build launched (before screening), [6] restarts of
  * TinySCF_do_SCF from the SAD guess by its divergence guard (an energy that is
  * not finite, or one rising by more than 1e-6 Eh four iterations in a row;
- * a second divergence in the same solve returns TINYSCF_ERR_NUMERIC). */
+ * a second divergence in the same solve returns TINYSCF_ERR_NUMERIC), [7] FP64
+ * exchange products K = T T^T this instance ran on the integer tensor cores
+ * (Ozaki scheme II: int8 residues of T modulo 15 coprime moduli, exact int32
+ * products, Chinese-remainder reconstruction; chosen by the autotuner when
+ * faster, forced on or off by the environment variable TINYSCF_OZAKI=1 / 0). */
 TINYSCF_API int TinySCF_get_counters(TinySCF_t t, long long *out, int n);
 /* Coulomb matrix J from a density D without allocating anything: for callers
  * that cannot call cudaMalloc (a host framework that owns all device memory
@@ -274,6 +278,14 @@ TINYSCF_API int TinySCF_kmix_wait_probe(TinySCF_t t, long long wait_cycles, int 
  * device; synchronous. TINYSCF_ERR_CUDA if a grid barrier of the
  * tridiagonalisation gave up waiting. */
 TINYSCF_API int TinySCF_eigh(int device, int n, const double *A, double *w, double *V);
+/* K = T T^T (T: n x q, row-major; K: n x n, both triangles) on host buffers,
+ * by the integer-tensor-core product the engine's FP64 exchange uses when
+ * TINYSCF_OZAKI selects it (the rank-k step of build_Fock.c:317-341): each row
+ * of T scaled by a power of two and rounded to a 49-bit integer, its residues
+ * modulo 15 coprime moduli <= 256 multiplied as int8 with exact int32 sums,
+ * the sums rebuilt by the Chinese remainder theorem and rounded once to FP64.
+ * Allocates and frees its own workspace (about 15 n q bytes); synchronous. */
+TINYSCF_API int TinySCF_syrk_int8(int device, int n, long long q, const double *T, double *K);
 /* Back to the state right after TinySCF_get_initial_guess (SAD density, its
  * factor, empty DIIS history), keeping integrals and the DF tensor. */
 TINYSCF_API int TinySCF_reset_scf(TinySCF_t t);

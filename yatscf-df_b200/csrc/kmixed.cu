@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "tscf_internal.h"
+#include "umma.cuh"
 
 namespace tscf {
 
@@ -41,60 +42,13 @@ constexpr long long WAIT_CYCLES = 4000000000LL;   // ~2 s at 2 GHz
 
 __device__ int g_umma_error;     // set to a nonzero code when a bounded wait times out
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
+using namespace umma;
 
 // Bounded wait on an mbarrier phase (at most `limit` clock cycles). Returns
-// false (and records code) on timeout.
+// false (and records code in g_umma_error) on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, int code, long long limit = WAIT_CYCLES)
 {
-    const uint32_t addr = smem_u32(bar);
-    const long long t0 = clock64();
-    while (true) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(phase)
-            : "memory");
-        if (done) return true;
-        if (clock64() - t0 > limit) {
-            atomicExch(&g_umma_error, code);
-            return false;
-        }
-    }
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-        ::"r"(smem_u32(dst)), "l"((uint64_t) map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-        : "memory");
-}
-
-// K-major operand tile, 128-byte swizzle: rows of 128 B, 8-row atoms 1024 B apart.
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr)
-{
-    uint64_t d = 0;
-    d |= (uint64_t) ((addr >> 4) & 0x3FFF);   // start address
-    d |= (uint64_t) 1 << 16;                  // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t) (1024 >> 4) << 32;        // stride byte offset: next 8-row atom
-    d |= (uint64_t) 1 << 46;                  // descriptor version (sm_100)
-    d |= (uint64_t) 2 << 61;                  // SWIZZLE_128B
-    return d;
+    return mbar_wait_bounded(bar, phase, &g_umma_error, code, limit);
 }
 
 // kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = n.
@@ -110,43 +64,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t 
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t *bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-// 32 lanes x 32 columns of FP32 from TMEM without waiting; tmem_wait_ld()
-// completes every load issued before it (so several loads overlap).
-__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t *r)
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r)
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
@@ -197,12 +114,6 @@ __device__ __forceinline__ void mma_chunk(uint32_t a_hi, uint32_t a_lo, uint32_t
         umma_bf16(acc_corr, dal, dbh, idesc, 1u);
         if (LOLO) umma_bf16(acc_corr, dal, dbl, idesc, 1u);
     }
-}
-
-__device__ __forceinline__ void tmem_alloc_warp(uint32_t *slot, uint32_t cols)
-{
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(cols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
 }
 
 // ------------------------------------------------------------------ half-transform
@@ -530,36 +441,10 @@ constexpr int gemm_smem_bytes()
 }
 
 // ---------------------------------------------------------------- TMA descriptors
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn()
-{
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn) p;
-    }
-    return fn;
-}
-
 // 2D BF16 matrix rows x cols (cols contiguous, pitch in elements), box 64 cols x box_rows.
 int make_map(CUtensorMap *m, const void *base, long long rows, long long cols, long long pitch, int box_rows)
 {
-    EncodeTiledFn fn = encode_fn();
-    if (!fn) return ERR_CUDA;
-    cuuint64_t dims[2] = {(cuuint64_t) cols, (cuuint64_t) rows};
-    cuuint64_t strides[1] = {(cuuint64_t) pitch * 2};
-    cuuint32_t box[2] = {(cuuint32_t) BK, (cuuint32_t) box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? OK : ERR_CUDA;
+    return make_map_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, rows, cols, pitch, BK, box_rows) ? OK : ERR_CUDA;
 }
 
 }  // namespace
@@ -848,8 +733,35 @@ static int launch_gemm(const KMix *k, const GArgs &ga, cudaStream_t s)
         attr_set = true;
     }
     const int mt = (k->nbf + UM - 1) / UM;
-    k_gemm<STAGES><<<dim3(mt, mt, k->ksplit), THREADS, SMEM, s>>>(k->mdTh, k->mdTl, k->mSh, k->mSl, ga);
+    // Clusters of CTAs along the row tiles: the CTAs that read the same S tile
+    // (and, cluster after cluster, the same dT tiles) run at the same time on
+    // one GPC, so their TMA loads of the shared tiles meet in L2 instead of
+    // each going to DRAM. No cluster feature is used inside the kernel.
+    static const int cl_max = [] {
+        const char *v = getenv("TINYSCF_GEMM_CLUSTER");
+        const int c = v ? atoi(v) : 2;
+        return (c == 1 || c == 2 || c == 4 || c == 8) ? c : 2;
+    }();
+    int cl = 1;
+    for (int c = cl_max; c >= 2; c >>= 1)
+        if (mt % c == 0) {
+            cl = c;
+            break;
+        }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(mt, mt, k->ksplit);
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     g_launches++;
+    if (cudaLaunchKernelEx(&cfg, k_gemm<STAGES>, k->mdTh, k->mdTl, k->mSh, k->mSl, ga) != cudaSuccess) return ERR_CUDA;
     return OK;
 }
 

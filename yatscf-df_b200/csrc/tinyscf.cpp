@@ -293,6 +293,9 @@ struct Engine {
     int2 *tiles = nullptr;
     int ksplit = 1, ksplit_max = 1, ksplit64 = 1, ktile = 64, khwide = 0;
     int2 *tiles128 = nullptr;
+    OzSyrk *oz = nullptr;   // K = T T^T on the integer tensor cores (used when kozaki)
+    bool kozaki = false;
+    long long n_ozaki = 0;  // K = T T^T builds that ran on the integer tensor cores
     double *Jt = nullptr, *Jpart = nullptr, *Jw = nullptr;
     int jblk = 1, jblk_max = 1;
     double *epart = nullptr, *E = nullptr;
@@ -926,9 +929,32 @@ int guess_impl(TinySCF_t t)
 // blocks of the J first pass are timed on this molecule's buffers (their
 // contents do not matter for the timing; the first Fock build rewrites J and
 // K) and the fastest kept; later molecules of the same sizes reuse the choice.
+// K = T T^T on the integer tensor cores (ozaki.cu): TINYSCF_OZAKI=1 always,
+// 0 never, otherwise when the autotuner times it faster than the FP64 kernels.
+static int ozaki_mode()
+{
+    const char *v = getenv("TINYSCF_OZAKI");
+    if (v && v[0] == '0') return 0;
+    if (v && v[0] == '1') return 1;
+    return -1;
+}
+
+static int ensure_oz(Engine *e, TinySCF_t t)
+{
+    if (e->oz) return OK;
+    return oz_create(&e->oz, t->nbasfuncs, (long long) t->n_occ * e->plan().naux, e->s);
+}
+
+static bool use_oz(const Engine *e)
+{
+    const int om = ozaki_mode();
+    return e->oz && (om == 1 || (om < 0 && e->kozaki));
+}
+
 int autotune_fock(TinySCF_t t)
 {
     Engine *e = E_(t);
+    if (ozaki_mode() == 1) RC(ensure_oz(e, t));
     if (!tune_enabled()) return OK;
     FockPlan p = e->plan();
     p.nocc = t->n_occ;
@@ -956,6 +982,28 @@ int autotune_fock(TinySCF_t t)
         e->ktile = c / 1000;
         e->ksplit = c % 1000;
         if (e->ktile == 64) e->ksplit64 = e->ksplit;
+    }
+    if (ozaki_mode() < 0 && t->nbasfuncs >= 128) {
+        snprintf(key, sizeof(key), "ksyrk_oz:%d:%d:%d", t->nbasfuncs, t->n_occ, p.naux);
+        c = tune_lookup(key);
+        if (c != 0) {
+            if (ensure_oz(e, t) != OK) {
+                cudaGetLastError();
+                c = 0;
+            } else if (c < 0) {
+                c = tune_run(key, {0, 1}, [&](int v) {
+                    if (v) oz_syrk(e->oz, e->T, e->K, e->s);
+                    else build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 64 ? e->tiles : e->tiles128,
+                                      e->s, e->ktile);
+                }, e->s);
+            }
+        }
+        e->kozaki = c == 1;
+        if (!e->kozaki && e->oz) {
+            RC(sync_rc(e, "autotuning"));
+            oz_destroy(e->oz);
+            e->oz = nullptr;
+        }
     }
     snprintf(key, sizeof(key), "khalf:%d:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf, e->nnz);
     c = tune_lookup(key);
@@ -1079,7 +1127,12 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
         build_K_halftransform(p, e->Cocc, e->T, e->s, e->khwide);
         tstop(e, TINYSCF_T_K_HT);
         tstart(e, TINYSCF_T_K_SYRK);
-        build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 64 ? e->tiles : e->tiles128, e->s, e->ktile);
+        if (use_oz(e)) {
+            RC(oz_syrk(e->oz, e->T, e->K, e->s));
+            e->n_ozaki++;
+        } else
+            build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 64 ? e->tiles : e->tiles128, e->s,
+                         e->ktile);
         tstop(e, TINYSCF_T_K_SYRK);
     }
     if (Kuse != e->K)
@@ -1425,6 +1478,13 @@ int scf_impl(TinySCF_t t)
             return ERR_CUDA;
         }
     }
+    if (e->oz) {
+        const int fl = oz_error_flag();
+        if (fl) {
+            fprintf(stderr, "[tinyscf] integer tensor-core K: a bounded wait timed out (code %d)\n", fl);
+            return ERR_CUDA;
+        }
+    }
     cudaEventRecord(scf1, e->s);
     cudaEventSynchronize(scf1);
     float ms = 0;
@@ -1448,6 +1508,7 @@ void free_impl(TinySCF_t t)
         guessnet_free(e->gnet);
         eig_destroy(e->eig);
         kmix_destroy(e->kmix);
+        oz_destroy(e->oz);
         for (void *p : e->allocs) cudaFree(p);
         e->allocs.clear();
         if (e->s) {
@@ -1811,8 +1872,9 @@ int TinySCF_get_counters(TinySCF_t t, long long *out, int n)
 {
     if (!t || !t->dev || !out) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
-    long long v[7] = {g_launches, e->h2d, e->d2h, e->n_eig, e->n_refine, e->n3c_quartets, e->guard_restarts};
-    for (int k = 0; k < n && k < 7; k++) out[k] = v[k];
+    long long v[8] = {g_launches, e->h2d,         e->d2h,           e->n_eig,
+                      e->n_refine, e->n3c_quartets, e->guard_restarts, e->n_ozaki};
+    for (int k = 0; k < n && k < 8; k++) out[k] = v[k];
     return TINYSCF_OK;
 }
 
@@ -1829,8 +1891,8 @@ int TinySCF_get_timings(TinySCF_t t, double *ms, int n)
 // ------------------------------------------------------------------ batched SCF
 // Many molecules, each set up through the single-molecule API, iterate
 // together: every SCF phase is one launch over all molecules still iterating
-// (batch.cu), the density eigensolves are one batched cuSOLVER call per group
-// of equal basis size. Each molecule follows the reference loop
+// (batch.cu), the density eigensolves run per molecule on the engine's own
+// eigensolver. Each molecule follows the reference loop
 // (TinySCF.c:378-435) with its own ene_tol, niters and convergence.
 struct TinySCF_batch_struct {
     std::vector<TinySCF_t> mols;
@@ -2385,6 +2447,35 @@ int TinySCF_eigh(int device, int n, const double *A, double *w, double *V)
     cudaFree(dA);
     cudaFree(dw);
     cudaFree(dV);
+    cudaStreamDestroy(s);
+    return rc;
+}
+
+int TinySCF_syrk_int8(int device, int n, long long q, const double *T, double *K)
+{
+    if (n < 1 || q < 1 || !T || !K) return TINYSCF_ERR_INPUT;
+    if (cudaSetDevice(device) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    double *dT = nullptr, *dK = nullptr;
+    OzSyrk *oz = nullptr;
+    int rc = TINYSCF_OK;
+    if (cudaMalloc(&dT, sizeof(double) * (size_t) n * q) != cudaSuccess ||
+        cudaMalloc(&dK, sizeof(double) * (size_t) n * n) != cudaSuccess) {
+        cudaGetLastError();
+        rc = TINYSCF_ERR_ALLOC;
+    } else if ((rc = oz_create(&oz, n, q, s)) == OK) {
+        if (cudaMemcpyAsync(dT, T, sizeof(double) * (size_t) n * q, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            rc = TINYSCF_ERR_CUDA;
+        else if ((rc = oz_syrk(oz, dT, dK, s)) == OK &&
+                 (cudaMemcpyAsync(K, dK, sizeof(double) * (size_t) n * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                  cudaStreamSynchronize(s) != cudaSuccess))
+            rc = TINYSCF_ERR_CUDA;
+        if (rc == OK && oz_error_flag()) rc = TINYSCF_ERR_CUDA;
+    }
+    oz_destroy(oz);
+    cudaFree(dT);
+    cudaFree(dK);
     cudaStreamDestroy(s);
     return rc;
 }

@@ -216,6 +216,17 @@ int  kmix_error_flag();
 // waits of wait_cycles clock cycles); *code receives the recorded wait code.
 int  kmix_wait_probe(KMix *k, long long wait_cycles, int *code, cudaStream_t s);
 
+// ---------------------------------------------------------------- K = T T^T on the integer tensor cores (ozaki.cu)
+struct OzSyrk;
+// T is nbf x Q (row pitch Q); workspace: the residue planes (nmod x nbf x Q bytes, padded).
+int  oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s);
+void oz_destroy(OzSyrk *o);
+// K (nbf x nbf, both triangles) = T T^T to FP64 accuracy.
+int  oz_syrk(OzSyrk *o, const double *d_T, double *d_K, cudaStream_t s);
+int  oz_error_flag();
+// {moduli, beta, tiles, K ranges, chunks per range, padded rows}
+void oz_info(const OzSyrk *o, int info[6]);
+
 // ---------------------------------------------------------------- DIIS / density (scf.cu)
 struct DiisState {            // device-resident DIIS bookkeeping (DIIS.c:12-123)
     int len;

@@ -128,6 +128,7 @@ def load_library(path=LIBPATH):
                                  ctypes.c_longlong], ctypes.c_longlong),
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
         "TinySCF_eigh": ([ip, ip, dp, dp, dp], ip),
+        "TinySCF_syrk_int8": ([ip, ip, ctypes.c_longlong, dp, dp], ip),
         "TinySCF_kmix_wait_probe": ([T, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)], ip),
         "TinySCF_set_aux_slice": ([T, ip, ip], ip),
         "TinySCF_set_JK": ([T, dp, dp], ip),
@@ -365,9 +366,10 @@ class TinySCF:
     def counters(self):
         """(engine kernel launches in this process, bytes host->device, bytes device->host,
         full eigensolves, subspace refinement steps, 3-centre (shell pair, aux shell) tuples,
-        restarts from the SAD guess by the divergence guard)."""
-        out = (ctypes.c_longlong * 7)()
-        self.lib.TinySCF_get_counters(self.t, out, 7)
+        restarts from the SAD guess by the divergence guard, K = T T^T products run on the
+        integer tensor cores)."""
+        out = (ctypes.c_longlong * 8)()
+        self.lib.TinySCF_get_counters(self.t, out, 8)
         return tuple(int(v) for v in out)
 
     def timings(self):
@@ -474,6 +476,18 @@ def eigh(A, device=0):
     if rc:
         raise TinySCFError("eigh: " + STATUS.get(rc, str(rc)))
     return w, V
+
+
+def syrk_int8(T, device=0):
+    """K = T T^T (FP64 accuracy) from the engine's integer-tensor-core product."""
+    lib = load_library()
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    n, q = T.shape
+    K = np.zeros((n, n))
+    rc = lib.TinySCF_syrk_int8(int(device), n, ctypes.c_longlong(q), _dptr(T), _dptr(K))
+    if rc:
+        raise TinySCFError("syrk_int8: " + STATUS.get(rc, str(rc)))
+    return K
 
 
 def device_memory(device=0):
