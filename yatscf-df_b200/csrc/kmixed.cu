@@ -429,6 +429,172 @@ k_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensor
     }
 }
 
+// ------------------------------------------------------------------ G = dT S^T on CTA pairs
+// The product of k_gemm with 256 x 256 output tiles, each computed by a CTA
+// pair (cta_group::2, clusters of 2 along x): CTA r of the pair loads rows
+// m0 + 128 r .. + 127 of dT (hi, lo) and rows n0 + 128 r .. + 127 of S (hi, lo);
+// rank 0 issues M = 256, N = 256 MMAs that read both CTAs' tiles, and the
+// tensor memory of each CTA receives its 128 rows. Per byte staged in shared
+// memory this is twice k_gemm's MMA work (k_gemm is bound by shared-memory and
+// L2 bandwidth). The three split products share one FP32 accumulator, double
+// buffered in 2 x 256 columns. Rank 0's stage-full barrier counts both CTAs'
+// copies; its MMA commits arrive at the stage-empty and accumulator-full
+// barriers of both CTAs; both CTAs' epilogue warps arrive at rank 0's
+// accumulator-empty barrier.
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+constexpr int PAIR_N = 256;                 // output tile columns (and rows) per CTA pair
+constexpr int PAIR_STAGES = 3;
+__host__ __device__ constexpr int pair_stage_bytes() { return 2 * UM * BK * 2 + 2 * (PAIR_N / 2) * BK * 2; }
+__host__ __device__ constexpr int pair_smem_bytes() { return PAIR_STAGES * pair_stage_bytes() + 1024 + 8 * (2 * PAIR_STAGES + 4) + 16; }
+static_assert(pair_smem_bytes() <= 227 * 1024, "paired G GEMM stages exceed shared memory");
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+        const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, GArgs ga)
+{
+    constexpr int STAGES = PAIR_STAGES;
+    constexpr int BH = PAIR_N / 2;                // rows of S per CTA
+    constexpr int A_BYTES = UM * BK * 2, B_BYTES = BH * BK * 2;
+    constexpr int STAGE_BYTES = pair_stage_bytes();
+    constexpr uint32_t TMEM_COLS = 512;
+    constexpr int WC = PAIR_N / 2;                // output columns per epilogue warp
+    // kind::f16, BF16 x BF16 -> FP32, K-major, M = 256 (the pair), N = 256
+    constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (PAIR_N >> 3) << 17) |
+                               ((uint32_t) (256 >> 4) << 24);
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    uint64_t *full = (uint64_t *) (smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;    // [2] accumulator buffer ready (both CTAs)
+    uint64_t *tempty = tfull + 2;        // [2] accumulator buffer drained (rank 0's counts both CTAs)
+    uint32_t *tmem_slot = (uint32_t *) (tempty + 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int m0 = (blockIdx.x >> 1) * PAIR_N + (int) rank * UM;   // this CTA's rows of the tile
+    const int n0 = blockIdx.y * PAIR_N;                             // the tile's columns
+    const int kc0 = blockIdx.z * ga.chunks_per_split;
+    const int nk = max(0, min(ga.total_chunks, kc0 + ga.chunks_per_split) - kc0);
+    const int nseg = (nk + SEG_CHUNKS - 1) / SEG_CHUNKS;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 2 * EPI_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc_pair(tmem_slot, TMEM_COLS);
+    fence_before_sync();
+    __syncthreads();
+    cluster_sync();   // both CTAs' barriers exist before either signals the other's
+    fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0 && !ga.probe) {
+        const uint32_t full0 = mapa_shared(smem_u32(&full[0]), 0);   // rank 0's stage-full barriers
+        bool ok = true;
+        for (int kb = 0; kb < nk && ok; kb++) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES) ok = mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, 31, ga.wait_cycles);
+            if (!ok) break;
+            if (rank == 0) mbar_expect_tx(&full[s], 2 * STAGE_BYTES);
+            unsigned char *st = smem + s * STAGE_BYTES;
+            const int kx = (kc0 + kb) * BK;
+            const uint32_t bar = full0 + 8u * (uint32_t) s;
+            tma_load_2d_pair(st, &mAh, bar, kx, m0);
+            tma_load_2d_pair(st + A_BYTES, &mAl, bar, kx, m0);
+            tma_load_2d_pair(st + 2 * A_BYTES, &mBh, bar, kx, n0 + (int) rank * BH);
+            tma_load_2d_pair(st + 2 * A_BYTES + B_BYTES, &mBl, bar, kx, n0 + (int) rank * BH);
+        }
+        // the pair's MMAs have consumed (so the copies have landed in) the last stages
+        for (int kb = (nk > STAGES ? nk - STAGES : 0); kb < nk && ok; kb++)
+            mbar_wait(&empty[kb % STAGES], (kb / STAGES) & 1, 32, ga.wait_cycles);
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        bool ok = true;
+        int kb = 0;
+        for (int seg = 0; seg < nseg && ok; seg++) {
+            const int b = seg & 1;
+            if (seg >= 2) ok = mbar_wait(&tempty[b], ((seg >> 1) - 1) & 1, 33, ga.wait_cycles);
+            if (!ok) break;
+            fence_after_sync();
+            const uint32_t acc = tmem + b * PAIR_N;
+            const int kend = min(nk, (seg + 1) * SEG_CHUNKS);
+            for (; kb < kend && ok; kb++) {
+                const int s = kb % STAGES;
+                ok = mbar_wait(&full[s], (kb / STAGES) & 1, 34, ga.wait_cycles);
+                if (!ok) break;
+                fence_after_sync();
+                const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
+                const uint32_t a_lo = a_hi + A_BYTES, b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < BK / UK; kk++) {
+                    const uint32_t off = kk * UK * 2;
+                    const uint64_t dah = desc_sw128(a_hi + off), dal = desc_sw128(a_lo + off);
+                    const uint64_t dbh = desc_sw128(b_hi + off), dbl = desc_sw128(b_lo + off);
+                    umma_bf16_pair(acc, dah, dbh, idesc, (kb == seg * SEG_CHUNKS && kk == 0) ? 0u : 1u);
+                    umma_bf16_pair(acc, dah, dbl, idesc, 1u);
+                    umma_bf16_pair(acc, dal, dbh, idesc, 1u);
+                }
+                umma_commit_pair(&empty[s], 0x3);
+            }
+            umma_commit_pair(&tfull[b], 0x3);
+        }
+    } else if (warp >= 2) {
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int row = quad * 32 + lane;
+        const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16) + half * WC;
+        const uint32_t tempty0 = mapa_shared(smem_u32(&tempty[0]), 0);
+        const int gi = m0 + row;
+        const int lim = ga.nbf - (n0 + half * WC);
+        double *o = ga.part + (size_t) blockIdx.z * ga.nbf * ga.nbf + (size_t) gi * ga.nbf + n0 + half * WC;
+        const bool own = gi < ga.nbf;
+        float acc[WC];
+#pragma unroll
+        for (int c = 0; c < WC; c++) acc[c] = 0.f;
+        uint32_t r[32];
+        bool ok = true;
+        for (int seg = 0; seg < nseg && ok; seg++) {
+            const int b = seg & 1;
+            ok = mbar_wait(&tfull[b], (seg >> 1) & 1, 35, ga.wait_cycles);
+            if (!ok) break;
+            fence_after_sync();
+#pragma unroll
+            for (int c0 = 0; c0 < WC; c0 += 32) {
+                tmem_ld32(tq + b * PAIR_N + c0, r);
+#pragma unroll
+                for (int q = 0; q < 32; q++) acc[c0 + q] += __uint_as_float(r[q]);
+            }
+            fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(tempty0 + 8u * (uint32_t) b);
+        }
+        if (own) {   // zero when the split is empty or a wait gave up
+#pragma unroll
+            for (int c = 0; c < WC; c++)
+                if (c < lim) o[c] = ok ? (double) acc[c] : 0.0;
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    cluster_sync();   // the pair's MMAs, commits and remote arrivals are over
+    if (warp == 1) {
+        fence_after_sync();
+        tmem_dealloc_pair(tmem, TMEM_COLS);
+    }
+}
+
 template <int BN, int STAGES>
 constexpr int half_smem_bytes()
 {
@@ -722,8 +888,43 @@ static int launch_half(const KMix *k, HalfArgs ha, cudaStream_t s)
     return OK;
 }
 
+// The paired kernel (k_gemm2) unless TINYSCF_GEMM_PAIR=0.
+static bool use_pair_gemm()
+{
+    const char *v = getenv("TINYSCF_GEMM_PAIR");
+    return !(v && v[0] == '0');
+}
+
+static int launch_gemm2(const KMix *k, const GArgs &ga, cudaStream_t s)
+{
+    constexpr int SMEM = pair_smem_bytes();
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+            return ERR_CUDA;
+        attr_set = true;
+    }
+    const int mt = (k->nbf + PAIR_N - 1) / PAIR_N;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * mt, mt, k->ksplit);
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    g_launches++;
+    if (cudaLaunchKernelEx(&cfg, k_gemm2, k->mdTh, k->mdTl, k->mSh, k->mSl, ga) != cudaSuccess) return ERR_CUDA;
+    return OK;
+}
+
 static int launch_gemm(const KMix *k, const GArgs &ga, cudaStream_t s)
 {
+    if (use_pair_gemm()) return launch_gemm2(k, ga, s);
     constexpr int STAGES = 3;
     constexpr int SMEM = gemm_smem_bytes<128, STAGES>();
     static bool attr_set = false;
