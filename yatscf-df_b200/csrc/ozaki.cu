@@ -19,12 +19,13 @@
 // With 15 moduli M ~ 2^117.8 and beta = 49: the only rounding before the final
 // one is step 1's, 2^-50 of each row's largest element.
 //
-// k_oz_gemm: 128 x 256 output tiles over the upper triangle, one CTA per
-// (tile, K range); warp 0 issues the TMA loads of both residue tiles (128 B of
-// K per stage), warp 1 the MMAs (M = 128, N = 256, K = 32 per instruction) of
-// modulus k into TMEM buffer k & 1, warps 2-9 reduce the other buffer mod its
-// modulus and store the bytes, so the drain overlaps the next modulus' MMAs.
-// All mbarrier waits are bounded; a timeout sets an error flag instead of hanging.
+// k_oz_gemm: 256 x 256 output tiles over the upper triangle, one CTA pair
+// (tcgen05 cta_group::2) per (tile, K range); in each CTA warp 0 issues the TMA
+// loads of its halves of both residue tiles (128 B of K per stage), warp 1 of
+// rank 0 the MMAs (M = 256, N = 256, K = 32 per instruction) of modulus k into
+// TMEM buffer k & 1, warps 2-9 reduce the other buffer mod its modulus and
+// store the bytes, so the drain overlaps the next modulus' MMAs. All mbarrier
+// waits are bounded; a timeout sets an error flag instead of hanging.
 #include <cuda.h>
 #include <cstdio>
 #include <cstdlib>
@@ -44,14 +45,14 @@ typedef unsigned __int128 u128;
 
 constexpr int OZ_MODULI[] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197};
 constexpr int OZ_NMAX = 15;
-constexpr int OM = 128;                 // tile rows (UMMA M)
-constexpr int ON = 256;                 // tile columns (UMMA N)
+constexpr int OM = 128;                 // tile rows per CTA (a CTA pair's MMA has M = 256)
+constexpr int ON = 256;                 // tile columns (UMMA N); tiles are 256 x 256 per pair
 constexpr int OKB = 128;                // K bytes per pipeline stage (one 128-byte swizzle row)
 constexpr int OZ_MAX_CHUNKS = 1023;     // K range <= 1023 * 128 = 130944 terms: |sum| < 2^31
-constexpr int OZ_STAGES = 4;
+constexpr int OZ_STAGES = 6;
 constexpr int OZ_EPI_WARPS = 8;         // two warps per TMEM lane quadrant, 128 columns each
 constexpr int OZ_THREADS = 64 + 32 * OZ_EPI_WARPS;
-constexpr int OZ_A_BYTES = OM * OKB, OZ_B_BYTES = ON * OKB;
+constexpr int OZ_A_BYTES = OM * OKB, OZ_B_BYTES = (ON / 2) * OKB;   // per CTA of a pair: 128 rows each
 constexpr int OZ_STAGE_BYTES = OZ_A_BYTES + OZ_B_BYTES;
 constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE_BYTES + 1024 + 8 * (2 * OZ_STAGES + 4) + 16;
 static_assert(OZ_SMEM <= 227 * 1024, "Ozaki GEMM stages exceed shared memory");
@@ -63,18 +64,18 @@ __constant__ double c_m[OZ_NMAX], c_inv[OZ_NMAX];
 __constant__ int c_mi[OZ_NMAX], c_y[OZ_NMAX];
 __constant__ unsigned long long c_Mk[OZ_NMAX][2], c_M[2];
 
-// kind::i8 instruction descriptor: S8 x S8 -> S32 (no saturation), K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_s8(int n)
+// kind::i8 instruction descriptor: S8 x S8 -> S32 (no saturation), K-major, M = m, N = n.
+__host__ __device__ constexpr uint32_t idesc_s8(int m, int n)
 {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) | ((uint32_t) (OM >> 4) << 24);
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) | ((uint32_t) (m >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+__device__ __forceinline__ void umma_s8_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
@@ -153,26 +154,36 @@ __global__ void __launch_bounds__(256) k_oz_residues(const double *__restrict__ 
 }
 
 struct OzArgs {
-    const int2 *tiles;       // (row block of 128, column block of 256)
+    const int2 *tiles;       // upper tiles (row block, column block) of 256
     uint8_t *res;            // [ksplit][nmod][rows_pad][rows_pad] residues of the range sums
     int rows_pad, nmod, chunks_per_split, total_chunks;
     long long wait_cycles;
 };
 
+// One 256 x 256 tile per CTA pair (clusters of 2 along x): CTA r loads rows
+// 128 r .. + 127 of the tile's row block (A) and of its column block (B) of
+// residue plane k; rank 0 issues M = 256, N = 256 MMAs reading both CTAs'
+// tiles, each CTA's tensor memory receives its 128 rows. Rank 0's stage-full
+// barrier counts both CTAs' copies; its commits arrive at the stage-empty and
+// accumulator-full barriers of both CTAs; both CTAs' epilogue warps arrive at
+// rank 0's accumulator-empty barrier.
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-k_oz_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB, OzArgs a)
+k_oz_gemm(const __grid_constant__ CUtensorMap mR, OzArgs a)
 {
     constexpr uint32_t TMEM_COLS = 512;
+    constexpr uint32_t idesc = idesc_s8(2 * OM, ON);
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
     uint64_t *full = (uint64_t *) (smem + OZ_STAGES * OZ_STAGE_BYTES);
     uint64_t *empty = full + OZ_STAGES;
-    uint64_t *tfull = empty + OZ_STAGES;   // [2] accumulator buffer ready
-    uint64_t *tempty = tfull + 2;          // [2] accumulator buffer drained
+    uint64_t *tfull = empty + OZ_STAGES;   // [2] accumulator buffer ready (both CTAs)
+    uint64_t *tempty = tfull + 2;          // [2] accumulator buffer drained (rank 0's counts both CTAs)
     uint32_t *tmem_slot = (uint32_t *) (tempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int2 tile = a.tiles[blockIdx.x];
-    const int m0 = tile.x * OM, n0 = tile.y * ON, split = blockIdx.y;
+    const uint32_t rank = cluster_ctarank();
+    const int2 tile = a.tiles[blockIdx.x >> 1];
+    const int m0 = tile.x * ON + (int) rank * OM, n0 = tile.y * ON, split = blockIdx.y;
+    const int nb_own = n0 + (int) rank * OM;
     const int kc0 = split * a.chunks_per_split;
     const int nk = max(0, min(a.total_chunks, kc0 + a.chunks_per_split) - kc0);
     const int nit = nk * a.nmod;
@@ -184,34 +195,36 @@ k_oz_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtens
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], OZ_EPI_WARPS);
+            mbar_init(&tempty[b], 2 * OZ_EPI_WARPS);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 1) tmem_alloc_warp(tmem_slot, TMEM_COLS);
+    if (warp == 1) tmem_alloc_pair(tmem_slot, TMEM_COLS);
     fence_before_sync();
     __syncthreads();
+    cluster_sync();   // both CTAs' barriers exist before either signals the other's
     fence_after_sync();
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
+        const uint32_t full0 = mapa_shared(smem_u32(&full[0]), 0);   // rank 0's stage-full barriers
         bool ok = true;
         for (int it = 0; it < nit && ok; it++) {
             const int s = it % OZ_STAGES, k = it / nk, kb = it % nk;
             if (it >= OZ_STAGES) ok = mbar_wait_bounded(&empty[s], ((it / OZ_STAGES) - 1) & 1, &g_oz_error, 21,
                                                         a.wait_cycles);
             if (!ok) break;
+            if (rank == 0) mbar_expect_tx(&full[s], 2 * OZ_STAGE_BYTES);
             unsigned char *st = smem + s * OZ_STAGE_BYTES;
-            mbar_expect_tx(&full[s], OZ_STAGE_BYTES);
             const int kx = (kc0 + kb) * OKB;
-            tma_load_2d(st, &mA, &full[s], kx, k * a.rows_pad + m0);
-            tma_load_2d(st + OZ_A_BYTES, &mB, &full[s], kx, k * a.rows_pad + n0);
+            const uint32_t bar = full0 + 8u * (uint32_t) s;
+            tma_load_2d_pair(st, &mR, bar, kx, k * a.rows_pad + m0);
+            tma_load_2d_pair(st + OZ_A_BYTES, &mR, bar, kx, k * a.rows_pad + nb_own);
         }
-        // nothing may be in flight when the CTA exits
-        for (int it = (nit > OZ_STAGES ? nit - OZ_STAGES : 0); it < nit; it++)
-            mbar_wait_bounded(&full[it % OZ_STAGES], (it / OZ_STAGES) & 1, &g_oz_error, 22, a.wait_cycles);
-    } else if (warp == 1 && lane == 0) {
-        constexpr uint32_t idesc = idesc_s8(ON);
+        // the pair's MMAs have consumed (so the copies have landed in) the last stages
+        for (int it = (nit > OZ_STAGES ? nit - OZ_STAGES : 0); it < nit && ok; it++)
+            mbar_wait_bounded(&empty[it % OZ_STAGES], (it / OZ_STAGES) & 1, &g_oz_error, 22, a.wait_cycles);
+    } else if (warp == 1 && lane == 0 && rank == 0) {
         bool ok = true;
         int it = 0;
         for (int k = 0; k < a.nmod && ok && nk > 0; k++) {
@@ -228,16 +241,17 @@ k_oz_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtens
                 const uint32_t sa = smem_u32(smem + s * OZ_STAGE_BYTES), sb = sa + OZ_A_BYTES;
 #pragma unroll
                 for (int kk = 0; kk < OKB / 32; kk++)
-                    umma_s8(acc, desc_sw128(sa + kk * 32), desc_sw128(sb + kk * 32), idesc,
-                            (kb > 0 || kk > 0) ? 1u : 0u);
-                umma_commit(&empty[s]);
+                    umma_s8_pair(acc, desc_sw128(sa + kk * 32), desc_sw128(sb + kk * 32), idesc,
+                                 (kb > 0 || kk > 0) ? 1u : 0u);
+                umma_commit_pair(&empty[s], 0x3);
             }
-            umma_commit(&tfull[b]);
+            umma_commit_pair(&tfull[b], 0x3);
         }
     } else if (warp >= 2) {
         const int quad = warp & 3, half = (warp - 2) >> 2;
         const int row = quad * 32 + lane;
         const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16) + half * 128;
+        const uint32_t tempty0 = mapa_shared(smem_u32(&tempty[0]), 0);
         bool ok = true;
         for (int k = 0; k < a.nmod && ok && nk > 0; k++) {
             const int b = k & 1;
@@ -270,14 +284,15 @@ k_oz_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtens
             }
             fence_before_sync();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[b]);
+            if (lane == 0) mbar_arrive_cluster(tempty0 + 8u * (uint32_t) b);
         }
     }
     fence_before_sync();
     __syncthreads();
+    cluster_sync();   // the pair's MMAs, commits and remote arrivals are over
     if (warp == 1) {
         fence_after_sync();
-        tmem_dealloc_warp(tmem, TMEM_COLS);
+        tmem_dealloc_pair(tmem, TMEM_COLS);
     }
 }
 
@@ -334,7 +349,7 @@ struct OzSyrk {
     int8_t *R = nullptr;
     uint8_t *res = nullptr;
     int2 *tiles = nullptr;
-    CUtensorMap mA, mB;
+    CUtensorMap mR;
 };
 
 void oz_destroy(OzSyrk *o)
@@ -406,7 +421,7 @@ int oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s)
     o->total_chunks = (int) (o->Qp / OKB);
     std::vector<int2> tl;
     for (int bj = 0; bj * ON < nbf; bj++)
-        for (int bi = 0; bi * OM < nbf && bi * OM <= bj * ON + ON - 1; bi++) tl.push_back(make_int2(bi, bj));
+        for (int bi = 0; bi <= bj; bi++) tl.push_back(make_int2(bi, bj));
     o->ntiles = (int) tl.size();
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -415,7 +430,7 @@ int oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s)
     o->nsm = nsm;
     // K ranges: at most OZ_MAX_CHUNKS chunks each, and about one CTA per SM in total
     const int ks_min = (o->total_chunks + OZ_MAX_CHUNKS - 1) / OZ_MAX_CHUNKS;
-    int ks = std::max(ks_min, nsm / o->ntiles);
+    int ks = std::max(ks_min, nsm / (2 * o->ntiles));
     ks = std::max(1, std::min(ks, o->total_chunks));
     o->cps = (o->total_chunks + ks - 1) / ks;
     o->ksplit = (o->total_chunks + o->cps - 1) / o->cps;
@@ -431,8 +446,7 @@ int oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s)
     TSCF_CUDA_CHECK(cudaMemsetAsync(o->R, 0, rbytes, s));
     TSCF_CUDA_CHECK(cudaMemcpyAsync(o->tiles, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice, s));
     const long long rows = (long long) o->nmod * o->rows_pad;
-    if (!make_map_2d(&o->mA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, o->R, rows, o->Qp, o->Qp, OKB, OM) ||
-        !make_map_2d(&o->mB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, o->R, rows, o->Qp, o->Qp, OKB, ON)) {
+    if (!make_map_2d(&o->mR, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, o->R, rows, o->Qp, o->Qp, OKB, OM)) {
         oz_destroy(o);
         return ERR_CUDA;
     }
@@ -455,7 +469,19 @@ int oz_syrk(OzSyrk *o, const double *d_T, double *d_K, cudaStream_t s)
     k_oz_rowexp<<<o->nbf, 1024, 0, s>>>(d_T, o->Q, o->e);
     k_oz_residues<<<o->nsm * 8, 256, 0, s>>>(d_T, o->nbf, o->Q, o->Qp, o->rows_pad, o->e, o->beta, o->nmod, o->R);
     OzArgs a{o->tiles, o->res, o->rows_pad, o->nmod, o->cps, o->total_chunks, OZ_WAIT_CYCLES};
-    k_oz_gemm<<<dim3(o->ntiles, o->ksplit), OZ_THREADS, OZ_SMEM, s>>>(o->mA, o->mB, a);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * o->ntiles, o->ksplit);
+    cfg.blockDim = dim3(OZ_THREADS);
+    cfg.dynamicSmemBytes = OZ_SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_oz_gemm, o->mR, a) != cudaSuccess) return ERR_CUDA;
     const long long nn = (long long) o->nbf * o->nbf;
     k_oz_crt<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(o->res, o->ksplit, o->nmod, o->rows_pad, o->nbf, o->e,
                                                           o->beta, d_K);
