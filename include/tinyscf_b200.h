@@ -217,8 +217,15 @@ TINYSCF_API int TinySCF_guess_mlp_grad(int din, int hid, int dout, const float *
  * rounding in the last bits). */
 TINYSCF_API int TinySCF_set_autotune(int on);
 /* Free and total device memory in bytes (cudaMemGetInfo) of a CUDA device,
- * for callers that size batches of molecules to what fits. */
+ * for callers that size batches of molecules to what fits. Free includes the
+ * memory that freed engines left in the engines' pool (below). */
 TINYSCF_API int TinySCF_device_memory(int device, long long *free_bytes, long long *total_bytes);
+/* The engines' large device buffers come from the device's stream-ordered
+ * memory pool, which keeps memory reserved after an engine is freed so that
+ * the next engine reuses it without new mappings (TINYSCF_MEMPOOL=0 in the
+ * environment uses cudaMalloc / cudaFree instead). This returns the pool's
+ * unused memory to the device. */
+TINYSCF_API int TinySCF_trim_memory(int device);
 /* The tuner's table as text ("key -> choice (ms) [candidate: ms]..."); writes
  * at most len bytes into buf and returns the full length. */
 TINYSCF_API int TinySCF_autotune_report(char *buf, int len);

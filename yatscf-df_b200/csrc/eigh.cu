@@ -988,7 +988,7 @@ template <typename T>
 bool ealloc(Eig *e, T **p, size_t count)
 {
     void *q = nullptr;
-    if (cudaMalloc(&q, sizeof(T) * (count ? count : 1)) != cudaSuccess) return false;
+    if (dev_malloc(&q, sizeof(T) * (count ? count : 1), 0) != OK) return false;
     e->allocs.push_back(q);
     *p = (T *) q;
     return true;
@@ -1160,7 +1160,8 @@ Eig *eig_create(int n, cudaStream_t s)
 void eig_destroy(Eig *e)
 {
     if (!e) return;
-    for (void *p : e->allocs) cudaFree(p);
+    for (void *p : e->allocs) dev_free(p, 0);
+    cudaStreamSynchronize(0);
     delete e;
 }
 

@@ -203,7 +203,7 @@ template <bool VEC>
 __global__ void __launch_bounds__(256, 1)
     k_halftransform_pipe(const double *__restrict__ B, const double *__restrict__ C, const int *__restrict__ csr_j,
                          const int *__restrict__ csr_u, const int *__restrict__ displs, int nocc, int naux,
-                         double *__restrict__ T, int n_items, int stiles, int ptiles)
+                         double *__restrict__ T, int n_items, int stiles, int ptiles, unsigned long long *rowmax)
 {
     extern __shared__ __align__(16) double khsm[];
     constexpr int NBR = VEC ? 8 : 16;   // DF rows whose copies this thread issues per step
@@ -278,6 +278,7 @@ __global__ void __launch_bounds__(256, 1)
                 for (int y = 0; y < 8; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
         }
         if (++Q.step == Q.nsteps) {   // item done: write its tile, start the next
+            double amax = 0.0;        // max |T| of the tile (padding entries are zero)
 #pragma unroll
             for (int x = 0; x < 4; x++) {
                 const int sg = Q.s0 + ws + 8 * x + fr;
@@ -287,8 +288,13 @@ __global__ void __launch_bounds__(256, 1)
                     const int pg = Q.p0 + wp + 8 * y + 2 * fc;
                     if (sg < nocc && pg < naux) row[pg] = acc[x][y][0];
                     if (sg < nocc && pg + 1 < naux) row[pg + 1] = acc[x][y][1];
+                    amax = fmax(amax, fmax(fabs(acc[x][y][0]), fabs(acc[x][y][1])));
                     acc[x][y][0] = acc[x][y][1] = 0.0;
                 }
+            }
+            if (rowmax) {   // row maxima for the integer-tensor-core K (non-negative: bit order = value order)
+                for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffff, amax, o));
+                if (lane == 0 && amax > 0.0) atomicMax(rowmax + Q.i, (unsigned long long) __double_as_longlong(amax));
             }
             kh_set(Q, Q.item + gridDim.x, n_items, stiles, ptiles, displs);
         }
@@ -343,11 +349,13 @@ __global__ void k_syrk_reduce(const double *Kpart, int nsplit, int nbf, double *
 
 size_t build_K_part_elems(const FockPlan &p, int ksplit) { return (size_t) ksplit * p.nbf * p.nbf; }
 
-void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide)
+void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide,
+                           unsigned long long *d_rowmax)
 {
     if (p.nbf <= 0 || p.nocc <= 0 || p.naux <= 0) return;   // T is empty: no grid to launch
     g_launches++;
     if (wide == 3) {
+        if (d_rowmax) cudaMemsetAsync(d_rowmax, 0, sizeof(unsigned long long) * p.nbf, s);
         const int stiles = (p.nocc + KH_S - 1) / KH_S, ptiles = (p.naux + KH_P - 1) / KH_P;
         const long long items = (long long) p.nbf * stiles * ptiles;
         int dev = 0, sms = 0;
@@ -361,11 +369,11 @@ void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T,
         if (p.naux % 2 == 0)
             k_halftransform_pipe<true><<<grid, 256, KH_PIPE_SMEM, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs,
                                                                        p.nocc, p.naux, d_T, (int) items, stiles,
-                                                                       ptiles);
+                                                                       ptiles, d_rowmax);
         else
             k_halftransform_pipe<false><<<grid, 256, KH_PIPE_SMEM, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u,
                                                                         p.csr_displs, p.nocc, p.naux, d_T,
-                                                                        (int) items, stiles, ptiles);
+                                                                        (int) items, stiles, ptiles, d_rowmax);
     } else if (wide) {
         dim3 g1((p.naux + KH_P - 1) / KH_P, (p.nocc + KH_S - 1) / KH_S, p.nbf);
         if (wide == 2)

@@ -735,10 +735,7 @@ struct KMix {
 
 static int kalloc(KMix *k, void **p, size_t bytes)
 {
-    if (cudaMalloc(p, bytes ? bytes : 16) != cudaSuccess) {
-        cudaGetLastError();
-        return ERR_ALLOC;
-    }
+    if (dev_malloc(p, bytes, 0) != OK) return ERR_ALLOC;
     k->mem.push_back(*p);
     return OK;
 }
@@ -752,7 +749,8 @@ static int kalloc(KMix *k, void **p, size_t bytes)
 void kmix_destroy(KMix *k)
 {
     if (!k) return;
-    for (void *p : k->mem) cudaFree(p);
+    for (void *p : k->mem) dev_free(p, 0);
+    cudaStreamSynchronize(0);
     delete k;
 }
 

@@ -5,6 +5,9 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
 
 #include <utility>
 #include <vector>
@@ -259,6 +262,71 @@ int cuda_launch_rc(const char *what)
     if (err == cudaSuccess) return OK;
     fprintf(stderr, "[tinyscf] CUDA error in %s: %s\n", what, cudaGetErrorString(err));
     return ERR_CUDA;
+}
+
+// ---------------------------------------------------------------- device memory
+// The engine's large buffers come from the device's stream-ordered memory
+// pool, kept reserved (release threshold: unlimited), so that freeing an
+// engine hands its memory to the next one without unmapping and remapping;
+// TINYSCF_MEMPOOL=0 uses cudaMalloc / cudaFree instead. The choice is made
+// once per process. TinySCF_trim_memory returns the pool's unused memory.
+static bool pool_mode()
+{
+    static const bool on = [] {
+        const char *v = getenv("TINYSCF_MEMPOOL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
+int dev_malloc(void **p, size_t bytes, cudaStream_t s)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (pool_mode()) {
+        static std::mutex mu;
+        static bool configured[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (dev >= 0 && dev < 64 && !configured[dev]) {
+                cudaMemPool_t pool;
+                if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                    uint64_t thr = UINT64_MAX;
+                    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+                }
+                configured[dev] = true;
+            }
+        }
+        if (cudaMallocAsync(p, bytes, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return ERR_ALLOC;
+        }
+        return OK;
+    }
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return ERR_ALLOC;
+    }
+    return OK;
+}
+
+void dev_free(void *p, cudaStream_t s)
+{
+    if (!p) return;
+    if (pool_mode()) cudaFreeAsync(p, s);
+    else cudaFree(p);
+}
+
+int dev_trim(int device)
+{
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return ERR_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess) return ERR_CUDA;
+    return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? OK : ERR_CUDA;
 }
 
 __global__ void k_scale_rows_invsqrt(const double *w, const double *V, double *out, int n)

@@ -100,6 +100,17 @@ __global__ void __launch_bounds__(1024) k_oz_rowexp(const double *__restrict__ T
     }
 }
 
+// e[i] from row maxima given as double bits.
+__global__ void k_oz_exp_from_max(const unsigned long long *__restrict__ rowmax, int nbf, int *e)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nbf) return;
+    const double m = __longlong_as_double((long long) rowmax[i]);
+    int ex = 0;
+    if (m > 0.0) frexp(m, &ex);
+    e[i] = ex;
+}
+
 // Residue planes R[k][i][q] (pitch Qp, q >= Q zero) of X_iq = rint(T_iq 2^(beta - e_i)).
 // One thread per 16 consecutive q of a row; q = fma(x, 1/m, MAGIC) - MAGIC is
 // round(x / m) (|x / m| < 2^51; for odd m, x / m is at least 1/(2m) from a
@@ -346,6 +357,7 @@ struct OzSyrk {
     int nbf = 0, nmod = 0, beta = 0, rows_pad = 0, ntiles = 0, ksplit = 1, cps = 1, total_chunks = 0, nsm = 1;
     long long Q = 0, Qp = 0;
     int *e = nullptr;
+    unsigned long long *rowmax = nullptr;
     int8_t *R = nullptr;
     uint8_t *res = nullptr;
     int2 *tiles = nullptr;
@@ -355,10 +367,9 @@ struct OzSyrk {
 void oz_destroy(OzSyrk *o)
 {
     if (!o) return;
-    cudaFree(o->e);
-    cudaFree(o->R);
-    cudaFree(o->res);
-    cudaFree(o->tiles);
+    for (void *p : {(void *) o->e, (void *) o->rowmax, (void *) o->R, (void *) o->res, (void *) o->tiles})
+        dev_free(p, 0);
+    cudaStreamSynchronize(0);
     delete o;
 }
 
@@ -436,9 +447,10 @@ int oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s)
     o->ksplit = (o->total_chunks + o->cps - 1) / o->cps;
     const size_t rbytes = (size_t) o->nmod * o->rows_pad * o->Qp;
     const size_t sbytes = (size_t) o->ksplit * o->nmod * o->rows_pad * o->rows_pad;
-    if (cudaMalloc(&o->e, sizeof(int) * nbf) != cudaSuccess || cudaMalloc(&o->R, rbytes) != cudaSuccess ||
-        cudaMalloc(&o->res, sbytes) != cudaSuccess || cudaMalloc(&o->tiles, sizeof(int2) * tl.size()) != cudaSuccess) {
-        cudaGetLastError();
+    if (dev_malloc((void **) &o->e, sizeof(int) * nbf, s) != OK ||
+        dev_malloc((void **) &o->rowmax, sizeof(unsigned long long) * nbf, s) != OK ||
+        dev_malloc((void **) &o->R, rbytes, s) != OK || dev_malloc((void **) &o->res, sbytes, s) != OK ||
+        dev_malloc((void **) &o->tiles, sizeof(int2) * tl.size(), s) != OK) {
         oz_destroy(o);
         return ERR_ALLOC;
     }
@@ -463,10 +475,13 @@ int oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s)
     return OK;
 }
 
-int oz_syrk(OzSyrk *o, const double *d_T, double *d_K, cudaStream_t s)
+unsigned long long *oz_rowmax(OzSyrk *o) { return o ? o->rowmax : nullptr; }
+
+int oz_syrk(OzSyrk *o, const double *d_T, double *d_K, cudaStream_t s, const unsigned long long *d_rowmax)
 {
     if (!o) return ERR_STATE;
-    k_oz_rowexp<<<o->nbf, 1024, 0, s>>>(d_T, o->Q, o->e);
+    if (d_rowmax) k_oz_exp_from_max<<<(o->nbf + 255) / 256, 256, 0, s>>>(d_rowmax, o->nbf, o->e);
+    else k_oz_rowexp<<<o->nbf, 1024, 0, s>>>(d_T, o->Q, o->e);
     k_oz_residues<<<o->nsm * 8, 256, 0, s>>>(d_T, o->nbf, o->Q, o->Qp, o->rows_pad, o->e, o->beta, o->nmod, o->R);
     OzArgs a{o->tiles, o->res, o->rows_pad, o->nmod, o->cps, o->total_chunks, OZ_WAIT_CYCLES};
     cudaLaunchConfig_t cfg = {};

@@ -100,20 +100,37 @@ __device__ __forceinline__ void dgemm_tile_dmma(int m, int n, int k, double alph
     for (int x = 0; x < 8; x++)
 #pragma unroll
         for (int y = 0; y < 4; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
-    for (int k0 = 0; k0 < k; k0 += GB_K) {
+    // the next K step's operands are fetched into registers while the DMMAs
+    // of the current one run
+    double pa[BT / 16], pb[BT / 16];
+    auto fetch = [&](int k0) {
 #pragma unroll
         for (int r = 0; r < BT / 16; r++) {
             const int l = tid + 256 * r;
             int row, kk;
             if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / BT; row = l % BT; }
             const int gi = m0 + row, gk = k0 + kk;
-            As[row][kk] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
+            pa[r] = (gi < m && gk < k) ? (TA ? A[(size_t) gk * lda + gi] : A[(size_t) gi * lda + gk]) : 0.0;
             int col;
             if (!TB) { kk = l / BT; col = l % BT; } else { col = l / GB_K; kk = l % GB_K; }
             const int gj = n0 + col, gk2 = k0 + kk;
-            Bs[col][kk] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
+            pb[r] = (gj < n && gk2 < k) ? (TB ? B[(size_t) gj * ldb + gk2] : B[(size_t) gk2 * ldb + gj]) : 0.0;
+        }
+    };
+    if (k > 0) fetch(0);
+    for (int k0 = 0; k0 < k; k0 += GB_K) {
+#pragma unroll
+        for (int r = 0; r < BT / 16; r++) {
+            const int l = tid + 256 * r;
+            int row, kk;
+            if (!TA) { row = l / GB_K; kk = l % GB_K; } else { kk = l / BT; row = l % BT; }
+            As[row][kk] = pa[r];
+            int col;
+            if (!TB) { kk = l / BT; col = l % BT; } else { col = l / GB_K; kk = l % GB_K; }
+            Bs[col][kk] = pb[r];
         }
         __syncthreads();
+        if (k0 + GB_K < k) fetch(k0 + GB_K);
 #pragma unroll
         for (int k4 = 0; k4 < GB_K; k4 += 4) {
             double a[8], b[4];

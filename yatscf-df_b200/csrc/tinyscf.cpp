@@ -293,6 +293,7 @@ struct Engine {
     int2 *tiles = nullptr;
     int ksplit = 1, ksplit_max = 1, ksplit64 = 1, ktile = 64, khwide = 0;
     int2 *tiles128 = nullptr;
+    bool d_from_cocc = false;   // D = Cocc Cocc^T (set by the engine's density builds, cleared by SAD / set_density)
     OzSyrk *oz = nullptr;   // K = T T^T on the integer tensor cores (used when kozaki)
     bool kozaki = false;
     long long n_ozaki = 0;  // K = T T^T builds that ran on the integer tensor cores
@@ -356,8 +357,7 @@ template <typename T>
 int dalloc(Engine *e, T **p, size_t count)
 {
     void *q = nullptr;
-    if (cudaMalloc(&q, sizeof(T) * (count ? count : 1)) != cudaSuccess) {
-        cudaGetLastError();
+    if (dev_malloc(&q, sizeof(T) * (count ? count : 1), e->s) != OK) {
         fprintf(stderr, "[tinyscf] device allocation of %zu bytes failed\n", sizeof(T) * count);
         return ERR_ALLOC;
     }
@@ -369,7 +369,8 @@ int dalloc(Engine *e, T **p, size_t count)
 void dfree(Engine *e, void *p)
 {
     if (!p) return;
-    cudaFree(p);
+    cudaStreamSynchronize(e->s);
+    dev_free(p, e->s);
     auto it = std::find(e->allocs.begin(), e->allocs.end(), p);
     if (it != e->allocs.end()) e->allocs.erase(it);
 }
@@ -866,11 +867,11 @@ int learned_guess(TinySCF_t t)
         // iterations find its occupied space at a fraction of an eigensolve
         prc = dominant_subspace(e->eig, e->F, e->V, e->tmp, e->tmp2, n, o, kGuessSubspaceIters, e->s);
         if (prc != OK && prc != ERR_NUMERIC) return prc;
-        if (prc == OK) density_from_rows(e->X, e->V, e->Cocc, e->D, n, o, e->s);
+        if (prc == OK) { density_from_rows(e->X, e->V, e->Cocc, e->D, n, o, e->s); e->d_from_cocc = true; }
     }
     if (prc != OK) {   // projected SAD, or a Gram matrix that lost definiteness
         RC(eig_run(e->eig, e->F, e->w, e->V, e->s));
-        density_from_eig(e->X, e->V + (size_t) (n - o) * n, e->Cocc, e->D, n, o, e->s);
+        { density_from_eig(e->X, e->V + (size_t) (n - o) * n, e->Cocc, e->D, n, o, e->s); e->d_from_cocc = true; }
     }
     tstop(e, TINYSCF_T_GUESS);
     RC(cuda_rc("learned initial guess"));
@@ -903,6 +904,7 @@ int guess_impl(TinySCF_t t)
         if (t->verbose) printf("TinySCF learned initial guess: an atom is not covered, using SAD\n");
     }
     e->guess_used = TINYSCF_GUESS_SAD;
+    e->d_from_cocc = false;   // the SAD density is not Cocc Cocc^T
     tstart(e, TINYSCF_T_GUESS);   // the timer spans reading the SAD blocks too
     std::vector<double> D((size_t) nbf * nbf, 0.0);
     sad_blocks(e, t, D);
@@ -1123,12 +1125,15 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
         tstop(e, TINYSCF_T_K_MIXED);
         Kuse = e->Kmix;
     } else {
+        // with the pipelined half-transform and the integer-tensor-core K, the
+        // row maxima that K's scaling needs come out of the half-transform
+        unsigned long long *rm = (use_oz(e) && e->khwide == 3) ? oz_rowmax(e->oz) : nullptr;
         tstart(e, TINYSCF_T_K_HT);
-        build_K_halftransform(p, e->Cocc, e->T, e->s, e->khwide);
+        build_K_halftransform(p, e->Cocc, e->T, e->s, e->khwide, rm);
         tstop(e, TINYSCF_T_K_HT);
         tstart(e, TINYSCF_T_K_SYRK);
         if (use_oz(e)) {
-            RC(oz_syrk(e->oz, e->T, e->K, e->s));
+            RC(oz_syrk(e->oz, e->T, e->K, e->s, rm));
             e->n_ozaki++;
         } else
             build_K_syrk(p, e->T, e->K, e->Kpart, e->ksplit, e->ktile == 64 ? e->tiles : e->tiles128, e->s,
@@ -1172,7 +1177,11 @@ int diis_device(TinySCF_t t)
     } else {
         int md = t->max_diis;
         if (md < 1 || md > MAX_DIIS) md = MAX_DIIS;
-        diis_step(e->diis, md, e->F, e->D, e->S, e->X, e->Fp, e->F0, e->R, e->tmp, e->tmp2, n, e->s);
+        const int o = t->n_occ;
+        if (e->d_from_cocc && o > 0 && 2 * o <= n)
+            diis_step_cocc(e->diis, md, e->F, e->Cocc, o, e->S, e->X, e->Fp, e->F0, e->R, e->tmp, e->tmp2, n, e->s);
+        else
+            diis_step(e->diis, md, e->F, e->D, e->S, e->X, e->Fp, e->F0, e->R, e->tmp, e->tmp2, n, e->s);
     }
     tstop(e, TINYSCF_T_DIIS);
     e->F_is_orth = true;
@@ -1203,13 +1212,13 @@ int density_device(TinySCF_t t)
         RC(subspace_refine(Fo, e->V, e->w, e->U, n, o, e->sw, kRefineTol, kRefineSteps, &steps, &res, e->s));
         e->n_refine += steps;
         if (res < kRefineTol) {
-            density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, e->s);
+            { density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, e->s); e->d_from_cocc = true; }
             tstop(e, TINYSCF_T_DENSITY);
             return cuda_rc("density (subspace refinement)");
         }
     }
     RC(eig_run(e->eig, Fo, e->w, e->V, e->s));
-    density_from_eig(e->X, e->V, e->Cocc, e->D, n, o, e->s);
+    { density_from_eig(e->X, e->V, e->Cocc, e->D, n, o, e->s); e->d_from_cocc = true; }
     e->n_eig++;
     if (e->dmode == TINYSCF_DENSITY_REFINE && o > 0) {
         TSCF_CUDA_CHECK(cudaMemcpyAsync(e->U, e->V, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, e->s));
@@ -1300,7 +1309,7 @@ int graph_capture(TinySCF_t t)
         tstart(e, TINYSCF_T_DENSITY);
         rc = subspace_refine_capture(e->Fp, e->V, e->w, e->U, n, o, e->sw, e->rctl, e->s, e->s_body, &e->g_body);
         if (!rc) {
-            density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, e->s);
+            { density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, e->s); e->d_from_cocc = true; }
             cudaMemcpyAsync(e->h_rctl, e->rctl, sizeof(RefineCtl), cudaMemcpyDeviceToHost, e->s);
         }
         tstop(e, TINYSCF_T_DENSITY);
@@ -1349,7 +1358,7 @@ int graph_iteration(TinySCF_t t, double *E)
             // same as the eager solver's fallback: full eigensolve of this F'
             // (the DENSITY timer keeps the start the graph recorded)
             RC(eig_run(e->eig, e->Fp, e->w, e->V, e->s));
-            density_from_eig(e->X, e->V, e->Cocc, e->D, n, o, e->s);
+            { density_from_eig(e->X, e->V, e->Cocc, e->D, n, o, e->s); e->d_from_cocc = true; }
             TSCF_CUDA_CHECK(cudaMemcpyAsync(e->U, e->V, sizeof(double) * (size_t) o * n, cudaMemcpyDeviceToDevice, e->s));
             e->n_eig++;
             tstop(e, TINYSCF_T_DENSITY);
@@ -1509,8 +1518,9 @@ void free_impl(TinySCF_t t)
         eig_destroy(e->eig);
         kmix_destroy(e->kmix);
         oz_destroy(e->oz);
-        for (void *p : e->allocs) cudaFree(p);
+        for (void *p : e->allocs) dev_free(p, e->s);
         e->allocs.clear();
+        if (e->s) cudaStreamSynchronize(e->s);
         if (e->s) {
             for (int k = 0; k < TINYSCF_T_COUNT; k++) {
                 cudaEventDestroy(e->ev0[k]);
@@ -1600,6 +1610,7 @@ int TinySCF_set_density(TinySCF_t t, const double *D, const double *Cocc)
     if (!t || !t->dev) return TINYSCF_ERR_STATE;
     Engine *e = E_(t);
     if (D && cudaMemcpy(e->D, D, sizeof(double) * e->nn, cudaMemcpyHostToDevice) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    if (D || Cocc) e->d_from_cocc = false;   // a caller's pair need not satisfy D = Cocc Cocc^T
     if (Cocc && cudaMemcpy(e->Cocc, Cocc, sizeof(double) * t->nbasfuncs * t->n_occ, cudaMemcpyHostToDevice) != cudaSuccess)
         return TINYSCF_ERR_CUDA;
     if (D) memcpy(t->D_mat, D, sizeof(double) * e->nn);
@@ -2186,7 +2197,7 @@ int batch_scf_impl(TinySCF_batch_t b)
             RC(subspace_refine(e->Fp, e->V, e->w, e->U, n, o, e->sw, kRefineTol, kRefineSteps, &steps, &res, b->s));
             e->n_refine += steps;
             if (res < kRefineTol) {
-                density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, b->s);
+                { density_from_rows(e->X, e->U, e->Cocc, e->D, n, o, b->s); e->d_from_cocc = true; }
                 need[k] = 0;
             }
         }
@@ -2311,6 +2322,14 @@ int TinySCF_device_memory(int device, long long *free_bytes, long long *total_by
     if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return TINYSCF_ERR_CUDA;
     size_t f = 0, tot = 0;
     cudaError_t err = cudaMemGetInfo(&f, &tot);
+    cudaMemPool_t pool;   // memory the engines' pool holds but does not use is free for them too
+    if (err == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device >= 0 ? device : cur) == cudaSuccess) {
+        uint64_t reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+            f += (size_t) (reserved - used);
+    }
+    cudaGetLastError();
     cudaSetDevice(cur);
     if (err != cudaSuccess) return TINYSCF_ERR_CUDA;
     if (free_bytes) *free_bytes = (long long) f;
@@ -2449,6 +2468,19 @@ int TinySCF_eigh(int device, int n, const double *A, double *w, double *V)
     cudaFree(dV);
     cudaStreamDestroy(s);
     return rc;
+}
+
+int TinySCF_trim_memory(int device)
+{
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) {
+        cudaGetLastError();
+        return TINYSCF_ERR_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return TINYSCF_ERR_CUDA;
+    const int rc = dev_trim(device);
+    cudaSetDevice(cur);
+    return rc == OK ? TINYSCF_OK : TINYSCF_ERR_CUDA;
 }
 
 int TinySCF_syrk_int8(int device, int n, long long q, const double *T, double *K)

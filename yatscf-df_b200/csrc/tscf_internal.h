@@ -126,6 +126,14 @@ void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const do
 // ERR_CUDA (with a message) when a launch since the last check failed; the error is not cleared.
 int cuda_launch_rc(const char *what);
 
+// Device buffers of the engine (linalg.cu): from the device's stream-ordered
+// pool, kept reserved across engines, unless TINYSCF_MEMPOOL=0. dev_malloc
+// returns once the buffer is usable on any stream; dev_free is stream-ordered
+// on s (the caller synchronises before reusing the memory elsewhere).
+int  dev_malloc(void **p, size_t bytes, cudaStream_t s);
+void dev_free(void *p, cudaStream_t s);
+int  dev_trim(int device);   // return the pool's unused memory to the device
+
 // Symmetric eigen-decomposition (eigh.cu; ascending eigenvalues). A is
 // row-major n x n symmetric; on return V holds eigenvectors as ROWS (V[k*n + i]
 // = i-th entry of eigenvector k); V may alias A. Workspace (four n x n
@@ -187,7 +195,10 @@ void convert_f32(const double *in, float *out, size_t n, cudaStream_t s);
 // (k_halftransform_dmma), 3: the same DMMA tiles in persistent CTAs with a
 // cp.async pipeline over the CSR chunks (k_halftransform_pipe), 0: 64 x 64
 // FFMA tiles
-void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide = 0);
+// d_rowmax (wide = 3 only, else ignored): max_q |T(i, q)| of every row as
+// double bits, for the integer-tensor-core K.
+void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide = 0,
+                           unsigned long long *d_rowmax = nullptr);
 // ... then K = T T^T over upper 64x64 tiles (d_tiles: (bi,bj), bi <= bj), split-K, mirrored.
 // tile = 64 (k_syrk_part, FFMA), 128 (k_syrk_part128, FFMA) or KSYRK_DMMA
 // (k_syrk_dmma: 128 x 128 tiles on the FP64 tensor cores); d_tiles lists the
@@ -221,8 +232,11 @@ struct OzSyrk;
 // T is nbf x Q (row pitch Q); workspace: the residue planes (nmod x nbf x Q bytes, padded).
 int  oz_create(OzSyrk **out, int nbf, long long Q, cudaStream_t s);
 void oz_destroy(OzSyrk *o);
-// K (nbf x nbf, both triangles) = T T^T to FP64 accuracy.
-int  oz_syrk(OzSyrk *o, const double *d_T, double *d_K, cudaStream_t s);
+// K (nbf x nbf, both triangles) = T T^T to FP64 accuracy. d_rowmax: the rows'
+// max |T| as double bits when the half-transform produced them (oz_rowmax),
+// else nullptr (the rows are scanned).
+int  oz_syrk(OzSyrk *o, const double *d_T, double *d_K, cudaStream_t s, const unsigned long long *d_rowmax = nullptr);
+unsigned long long *oz_rowmax(OzSyrk *o);
 int  oz_error_flag();
 // {moduli, beta, tiles, K ranges, chunks per range, padded rows}
 void oz_info(const OzSyrk *o, int info[6]);
@@ -242,6 +256,10 @@ void diis_init(DiisState *d_st, cudaStream_t s);
 void diis_step(DiisState *d_st, int max_diis, const double *d_F, const double *d_D, const double *d_S,
                const double *d_X, double *d_Fout, double *d_F0, double *d_R, double *d_tmp, double *d_tmp2,
                int n, cudaStream_t s);
+// diis_step when D = Cocc Cocc^T: the commutator from n x n_occ products (needs 2 n_occ <= n).
+void diis_step_cocc(DiisState *d_st, int max_diis, const double *d_F, const double *d_Cocc, int o, const double *d_S,
+                    const double *d_X, double *d_Fout, double *d_F0, double *d_R, double *d_tmp, double *d_tmp2, int n,
+                    cudaStream_t s);
 void xtfx(const double *d_X, const double *d_F, double *d_out, double *d_tmp, int n, cudaStream_t s);
 void energy_reduce(const double *d_epart, double *d_E, cudaStream_t s);
 // Occupied-subspace refinement between full eigensolves (scf.cu).

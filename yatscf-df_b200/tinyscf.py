@@ -129,6 +129,7 @@ def load_library(path=LIBPATH):
         "quickSort_eigval": ([dp, ctypes.POINTER(ctypes.c_int), ip, ip], None),
         "TinySCF_eigh": ([ip, ip, dp, dp, dp], ip),
         "TinySCF_syrk_int8": ([ip, ip, ctypes.c_longlong, dp, dp], ip),
+        "TinySCF_trim_memory": ([ip], ip),
         "TinySCF_kmix_wait_probe": ([T, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)], ip),
         "TinySCF_set_aux_slice": ([T, ip, ip], ip),
         "TinySCF_set_JK": ([T, dp, dp], ip),
@@ -476,6 +477,13 @@ def eigh(A, device=0):
     if rc:
         raise TinySCFError("eigh: " + STATUS.get(rc, str(rc)))
     return w, V
+
+
+def trim_memory(device=0):
+    """Return the memory that freed engines left in the device's pool."""
+    rc = load_library().TinySCF_trim_memory(int(device))
+    if rc:
+        raise TinySCFError("trim_memory: " + STATUS.get(rc, str(rc)))
 
 
 def syrk_int8(T, device=0):
