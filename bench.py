@@ -546,12 +546,14 @@ def run_batch(args, rank, world, local_rank):
     clocks.start()
     scf_ms, guess_ms, waves, launches, iters, setup_s, phases = 0.0, 0.0, 0, 0, [], 0.0, {}
     k = 0
+    e_batched = {}
     while k < len(order):
-        wave = []
+        wave, wave_idx = [], []
         t0 = time.perf_counter()
         while k < len(order):
             e = engine(paths[order[k]], tinyscf.GUESS_LEARNED, True)
             wave.append(e)
+            wave_idx.append(order[k])
             guess_ms += e.timings()["GUESS"]
             k += 1
             if tinyscf.device_memory(local_rank)[0] < 40 * 2 ** 30:
@@ -566,6 +568,8 @@ def run_batch(args, rank, world, local_rank):
         launches += nl
         waves += 1
         iters += [e.s.iter for e in wave]
+        for kk, e in zip(wave_idx, wave):
+            e_batched[kk] = e.energy
         b.free()
         for e in wave:
             e.free()
@@ -573,6 +577,7 @@ def run_batch(args, rank, world, local_rank):
     # one by one, sampled
     sample = order[::8]
     seq_sad, seq_ml, it_sad = 0.0, 0.0, []
+    e_plain = {}
     for kk in sample:
         for guess in (None, tinyscf.GUESS_LEARNED):
             e = engine(paths[kk], guess, guess is not None)
@@ -582,9 +587,18 @@ def run_batch(args, rank, world, local_rank):
             if guess is None:
                 seq_sad += t
                 it_sad.append(e.s.iter)
+                e_plain[kk] = e.energy
             else:
                 seq_ml += t
             e.free()
+    if args.check_all:   # every remaining cluster, SAD + plain FP64, untimed
+        for kk in order:
+            if kk not in e_plain:
+                e = engine(paths[kk], None)
+                e.do_SCF()
+                e_plain[kk] = e.energy
+                e.free()
+    errs = [abs(e_batched[kk] - e_plain[kk]) for kk in e_plain]
     scale = len(order) / len(sample)
     total = (scf_ms + guess_ms) * 1e-3
     if world > 1:
@@ -613,6 +627,11 @@ def run_batch(args, rank, world, local_rank):
                        "sequential_learned_s": seq_ml * scale * 1e-3,
                        "sequential_sample": "every 8th cluster by size (%d), scaled by %.1f" % (len(sample), scale),
                        "speedup_vs_sequential_sad": seq_sad * scale * 1e-3 / total,
+                       "energy_error_vs_sad_plain_fp64": {
+                           "clusters": len(errs), "max": max(errs), "mean": statistics.mean(errs),
+                           "over_1e-8": sum(1 for x in errs if x > 1e-8),
+                           "note": "|E(batched, learned guess, tensor-core K) - E(one by one, SAD, plain FP64)| per "
+                                   "cluster, both converged to ene_tol"},
                        "setup_s": setup_s, "guess_s": guess_ms * 1e-3, "autotune": "off",
                        "batched_phase_s": {k: round(v * 1e-3, 3) for k, v in phases.items()}},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
@@ -633,6 +652,9 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--no-graph", action="store_true",
                     help="run the mixed form's iterations as individual launches (a profiler then sees every kernel)")
+    ap.add_argument("--check-all", action="store_true",
+                    help="waters256: also solve every cluster one by one with SAD and plain FP64 (untimed) and "
+                         "report the batched energies' errors against all of them")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
