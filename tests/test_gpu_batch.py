@@ -87,6 +87,31 @@ def test_batch_mixed_k_matches_single_molecule(tmp_path):
         e.free()
 
 
+def test_batch_mixed_k_one_launch_per_kernel(tmp_path, monkeypatch):
+    """The mixed molecules' tensor-core K of a batch runs as one half-transform
+    launch and one G GEMM launch over all of them: the same arithmetic per
+    molecule as their builds one by one (identical energies), fewer launches."""
+    paths = _molecules(tmp_path)[:6]
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("TINYSCF_BATCH_KMIX", mode)
+        engines = []
+        for p in paths:
+            e = _engine(p, tinyscf.GUESS_LEARNED)
+            e.set_k_precision(tinyscf.K_MIXED)
+            engines.append(e)
+        b = tinyscf.TinySCFBatch(engines)
+        b.do_SCF()
+        ms, iters, launches = b.stats()
+        out[mode] = ([e.energy for e in engines], [e.s.iter for e in engines], launches)
+        b.free()
+        for e in engines:
+            e.free()
+    assert out["1"][0] == out["0"][0]
+    assert out["1"][1] == out["0"][1]
+    assert out["1"][2] < out["0"][2], (out["1"][2], out["0"][2])
+
+
 def test_batch_refine_density_matches_single_molecule(tmp_path):
     """Molecules set to the subspace-refinement density solver refine in the
     batch as in their own SCF: same energies."""

@@ -28,13 +28,13 @@ __global__ void k_j_weights(const int *up_i, const int *up_j, const double *D, d
 
 // Each block streams a contiguous range of upper rows and keeps its partial
 // t(P) for every column in registers (jt_rows).
-template <typename BT>
+template <typename BT, int COLS>
 __global__ void __launch_bounds__(JT_THREADS) k_j_tpart(const BT *__restrict__ B, const int *__restrict__ up_u,
                                                         const double *__restrict__ w, int nup, int naux, int rows_per_blk,
                                                         double *__restrict__ part)
 {
     const int r0 = blockIdx.x * rows_per_blk, r1 = min(nup, r0 + rows_per_blk);
-    jt_rows<BT>(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
+    jt_rows<BT, COLS>(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
 }
 
 __global__ void k_j_treduce(const double *part, int nblk, int naux, double *t)
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) k_j_rows(const BT *__restrict__ B, const 
 
 int build_J_part_blocks(const FockPlan &p)
 {
-    int nb = 2 * 148;
+    int nb = 2 * num_sms();
     if (p.nup < nb) nb = p.nup > 0 ? p.nup : 1;
     return nb;
 }
@@ -83,9 +83,12 @@ static void build_J_t(const FockPlan &p, const BT *B, const double *d_D, double 
     g_launches += 4;
     k_j_weights<<<(p.nup + 255) / 256, 256, 0, s>>>(p.up_i, p.up_j, d_D, d_w, p.nup, p.nbf);
     int rows_per_blk = (p.nup + nblk - 1) / nblk;
-    k_j_tpart<BT><<<nblk, JT_THREADS, 0, s>>>(B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
+    if (p.naux <= 8 * JT_THREADS)
+        k_j_tpart<BT, 8><<<nblk, JT_THREADS, 0, s>>>(B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
+    else
+        k_j_tpart<BT, JT_COLS><<<nblk, JT_THREADS, 0, s>>>(B, p.up_u, d_w, p.nup, p.naux, rows_per_blk, d_part);
     k_j_treduce<<<(p.naux + 255) / 256, 256, 0, s>>>(d_part, nblk, p.naux, d_t);
-    int blocks = 148 * 4;
+    int blocks = num_sms() * 4;
     const size_t shm = sizeof(double) * p.naux;   // t(P) staged in shared memory
     if (shm > 48 * 1024) cudaFuncSetAttribute(k_j_rows<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
     k_j_rows<BT><<<blocks, 256, shm, s>>>(B, p.up_i, p.up_j, p.up_u, d_t, p.nup, p.naux, p.nbf, d_J);
@@ -112,7 +115,7 @@ __global__ void k_to_f32(const double *in, float *out, size_t n)
 void convert_f32(const double *in, float *out, size_t n, cudaStream_t s)
 {
     g_launches++;
-    k_to_f32<<<148 * 8, 256, 0, s>>>(in, out, n);
+    k_to_f32<<<num_sms() * 8, 256, 0, s>>>(in, out, n);
 }
 
 // ------------------------------------------------------------------ K, FP64
@@ -358,14 +361,12 @@ void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T,
         if (d_rowmax) cudaMemsetAsync(d_rowmax, 0, sizeof(unsigned long long) * p.nbf, s);
         const int stiles = (p.nocc + KH_S - 1) / KH_S, ptiles = (p.naux + KH_P - 1) / KH_P;
         const long long items = (long long) p.nbf * stiles * ptiles;
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int sms = num_sms();
         cudaFuncSetAttribute(k_halftransform_pipe<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int) KH_PIPE_SMEM);
         cudaFuncSetAttribute(k_halftransform_pipe<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int) KH_PIPE_SMEM);
-        const int grid = (int) std::min<long long>(items, sms > 0 ? sms : 148);
+        const int grid = (int) std::min<long long>(items, sms);
         if (p.naux % 2 == 0)
             k_halftransform_pipe<true><<<grid, 256, KH_PIPE_SMEM, s>>>(p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs,
                                                                        p.nocc, p.naux, d_T, (int) items, stiles,

@@ -172,7 +172,7 @@ __global__ void k_gather_rows(const float *src, const int *idx, int rows, int co
     dst[i] = src[(size_t) idx[r] * cols + c];
 }
 
-constexpr int LOSS_BLOCKS = 148;
+constexpr int LOSS_BLOCKS = 148;   // partial sums of the loss (a fixed count: the sum order is fixed)
 
 // Work buffers for one MLP on batches of up to `cap` rows.
 struct MlpWork {

@@ -614,6 +614,9 @@ __global__ void __launch_bounds__(64) k_one_electron(DevShells sh, const int *id
     const long long tid = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (long long) nM * nN) return;
     const int M = idsM[tid / nN], N = idsN[tid % nN];
+    // S and H are symmetric: each unordered pair once (the shell of lower AM,
+    // or the lower index within one AM class, first), its block mirrored
+    if (LM == LN && M > N) return;
     constexpr int dM = ncart(LM), dN = ncart(LN), LE = LM + LN;
     constexpr int NEa = ncum(LE) - ncum(LM - 1);
     const Sh A = load_shell(sh, M), B = load_shell(sh, N);
@@ -693,9 +696,12 @@ __global__ void __launch_bounds__(64) k_one_electron(DevShells sh, const int *id
                                 c_comp[baseB + ib][0], c_comp[baseB + ib][1], c_comp[baseB + ib][2], AB, le, lw);
             double v = 0.0;
             for (int k = 0; k < nl; k++) v += lw[k] * Vacc[le[k] - eoff];
-            size_t o = (size_t) (bfM + ia) * nbf + bfN + ib;
-            S[o] = Sv[ia * dN + ib];
-            H[o] = Tv[ia * dN + ib] + v;
+            size_t o = (size_t) (bfM + ia) * nbf + bfN + ib, ot = (size_t) (bfN + ib) * nbf + bfM + ia;
+            const double sv = Sv[ia * dN + ib], hv = Tv[ia * dN + ib] + v;
+            S[o] = sv;
+            H[o] = hv;
+            S[ot] = sv;
+            H[ot] = hv;
         }
 }
 
@@ -703,7 +709,7 @@ template <int LM>
 static void launch_1e_row(const DevShells &sh, const int *ids, const int *start, int natoms, const double *Z,
                           const double *xyz, double *S, double *H, int nbf, cudaStream_t s)
 {
-    for (int ln = 0; ln <= MAX_L_ORB; ln++) {
+    for (int ln = LM; ln <= MAX_L_ORB; ln++) {   // classes (LM, LN >= LM); the kernel mirrors each block
         int m0 = start[LM], nM = start[LM + 1] - m0, n0 = start[ln], nN = start[ln + 1] - n0;
         long long n = (long long) nM * nN;
         if (n == 0) continue;

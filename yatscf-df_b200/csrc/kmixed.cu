@@ -456,9 +456,8 @@ __host__ __device__ constexpr int pair_stage_bytes() { return 2 * UM * BK * 2 + 
 __host__ __device__ constexpr int pair_smem_bytes() { return PAIR_STAGES * pair_stage_bytes() + 1024 + 8 * (2 * PAIR_STAGES + 4) + 16; }
 static_assert(pair_smem_bytes() <= 227 * 1024, "paired G GEMM stages exceed shared memory");
 
-__global__ void __launch_bounds__(THREADS, 1)
-k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-        const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, GArgs ga)
+__device__ __forceinline__ void gemm2_body(const CUtensorMap *mAh, const CUtensorMap *mAl, const CUtensorMap *mBh,
+                                           const CUtensorMap *mBl, const GArgs &ga, int tile_x, int tile_y, int split)
 {
     constexpr int STAGES = PAIR_STAGES;
     constexpr int BH = PAIR_N / 2;                // rows of S per CTA
@@ -478,9 +477,9 @@ k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtenso
     uint32_t *tmem_slot = (uint32_t *) (tempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_ctarank();
-    const int m0 = (blockIdx.x >> 1) * PAIR_N + (int) rank * UM;   // this CTA's rows of the tile
-    const int n0 = blockIdx.y * PAIR_N;                             // the tile's columns
-    const int kc0 = blockIdx.z * ga.chunks_per_split;
+    const int m0 = tile_x * PAIR_N + (int) rank * UM;   // this CTA's rows of the tile
+    const int n0 = tile_y * PAIR_N;                      // the tile's columns
+    const int kc0 = split * ga.chunks_per_split;
     const int nk = max(0, min(ga.total_chunks, kc0 + ga.chunks_per_split) - kc0);
     const int nseg = (nk + SEG_CHUNKS - 1) / SEG_CHUNKS;
 
@@ -513,10 +512,10 @@ k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtenso
             unsigned char *st = smem + s * STAGE_BYTES;
             const int kx = (kc0 + kb) * BK;
             const uint32_t bar = full0 + 8u * (uint32_t) s;
-            tma_load_2d_pair(st, &mAh, bar, kx, m0);
-            tma_load_2d_pair(st + A_BYTES, &mAl, bar, kx, m0);
-            tma_load_2d_pair(st + 2 * A_BYTES, &mBh, bar, kx, n0 + (int) rank * BH);
-            tma_load_2d_pair(st + 2 * A_BYTES + B_BYTES, &mBl, bar, kx, n0 + (int) rank * BH);
+            tma_load_2d_pair(st, mAh, bar, kx, m0);
+            tma_load_2d_pair(st + A_BYTES, mAl, bar, kx, m0);
+            tma_load_2d_pair(st + 2 * A_BYTES, mBh, bar, kx, n0 + (int) rank * BH);
+            tma_load_2d_pair(st + 2 * A_BYTES + B_BYTES, mBl, bar, kx, n0 + (int) rank * BH);
         }
         // the pair's MMAs have consumed (so the copies have landed in) the last stages
         for (int kb = (nk > STAGES ? nk - STAGES : 0); kb < nk && ok; kb++)
@@ -558,7 +557,7 @@ k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtenso
         const uint32_t tempty0 = mapa_shared(smem_u32(&tempty[0]), 0);
         const int gi = m0 + row;
         const int lim = ga.nbf - (n0 + half * WC);
-        double *o = ga.part + (size_t) blockIdx.z * ga.nbf * ga.nbf + (size_t) gi * ga.nbf + n0 + half * WC;
+        double *o = ga.part + (size_t) split * ga.nbf * ga.nbf + (size_t) gi * ga.nbf + n0 + half * WC;
         const bool own = gi < ga.nbf;
         float acc[WC];
 #pragma unroll
@@ -593,6 +592,221 @@ k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtenso
         fence_after_sync();
         tmem_dealloc_pair(tmem, TMEM_COLS);
     }
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_gemm2(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+        const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, GArgs ga)
+{
+    gemm2_body(&mAh, &mAl, &mBh, &mBl, ga, blockIdx.x >> 1, blockIdx.y, blockIdx.z);
+}
+
+// ------------------------------------------------------------------ many molecules per launch
+// The operands of one molecule of a batched tensor-core K (a device array;
+// the TMA unit reads the tensor maps from global memory).
+struct KMixDev {
+    CUtensorMap mBh, mBl, mCh, mCl, mdTh, mdTl, mSh, mSl;
+    HalfArgs ha;
+    GArgs ga;
+    int bn, mt, ksplit;
+};
+
+// The molecule of global item g: starts[m] <= g < starts[m + 1] (molecules
+// without items have starts[m] == starts[m + 1]).
+__device__ __forceinline__ int find_mol(const int *starts, int nmol, int g)
+{
+    int lo = 0, hi = nmol - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (starts[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+constexpr int KB_STAGES = 2;
+constexpr int KB_BN = 256;   // shared-memory stages sized for the largest N
+__host__ __device__ constexpr int kb_half_smem_bytes()
+{
+    return KB_STAGES * (2 * UM * BK * 2 + 2 * KB_BN * BK * 2) + 1024 + 8 * (2 * KB_STAGES + 4) + 16;
+}
+static_assert(kb_half_smem_bytes() <= 227 * 1024, "batched half-transform stages exceed shared memory");
+
+// k_half over the items of many molecules: persistent CTAs take global items
+// blockIdx.x, + gridDim.x, ...; each item is (molecule, CSR row, 128 aux rows)
+// with the molecule's own N (padded n_occ), tensor maps and buffers.
+__global__ void __launch_bounds__(THREADS, 1)
+kb_half(const KMixDev *__restrict__ mols, const int *__restrict__ starts, int nmol)
+{
+    constexpr int STAGES = KB_STAGES;
+    constexpr int A_BYTES = UM * BK * 2;
+    constexpr int BMAX_BYTES = KB_BN * BK * 2;
+    constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * BMAX_BYTES;
+    constexpr uint32_t ACC_COLS = 256, TMEM_COLS = 512;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    uint64_t *full = (uint64_t *) (smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;   // [2]
+    uint64_t *tempty = tfull + 2;       // [2]
+    uint32_t *tmem_slot = (uint32_t *) (tempty + 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = starts[nmol];
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], EPI_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc_warp(tmem_slot, TMEM_COLS);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        bool ok = true;
+        long long g = 0;   // chunk counter across this CTA's items
+        for (int it = blockIdx.x; it < total && ok; it += gridDim.x) {
+            const int m = find_mol(starts, nmol, it);
+            const KMixDev &d = mols[m];
+            const int t = it - starts[m];
+            const int i = t / d.ha.ptiles, m0 = (t % d.ha.ptiles) * UM;
+            const int kc0 = d.ha.row_chunk0[i], nk = d.ha.row_chunk0[i + 1] - kc0;
+            const uint32_t bbytes = (uint32_t) d.bn * BK * 2;
+            for (int kb = 0; kb < nk && ok; kb++, g++) {
+                const int s = (int) (g % STAGES);
+                if (g >= STAGES) ok = mbar_wait(&empty[s], (uint32_t) (((g / STAGES) - 1) & 1), 41);
+                if (!ok) break;
+                unsigned char *st = smem + s * STAGE_BYTES;
+                mbar_expect_tx(&full[s], 2 * A_BYTES + 2 * bbytes);
+                const int kx = (kc0 + kb) * BK;
+                tma_load_2d(st, &d.mBh, &full[s], kx, m0);
+                tma_load_2d(st + A_BYTES, &d.mBl, &full[s], kx, m0);
+                tma_load_2d(st + 2 * A_BYTES, &d.mCh, &full[s], kx, 0);
+                tma_load_2d(st + 2 * A_BYTES + BMAX_BYTES, &d.mCl, &full[s], kx, 0);
+            }
+        }
+        for (long long q = (g > STAGES ? g - STAGES : 0); q < g; q++)
+            mbar_wait(&full[q % STAGES], (uint32_t) ((q / STAGES) & 1), 42);
+    } else if (warp == 1 && lane == 0) {
+        bool ok = true;
+        long long g = 0;
+        int li = 0;
+        for (int it = blockIdx.x; it < total && ok; it += gridDim.x, li++) {
+            const int m = find_mol(starts, nmol, it);
+            const KMixDev &d = mols[m];
+            const int t = it - starts[m];
+            const int i = t / d.ha.ptiles;
+            const int nk = d.ha.row_chunk0[i + 1] - d.ha.row_chunk0[i];
+            const uint32_t idesc = idesc_bf16(d.bn);
+            const int b = li & 1;
+            if (li >= 2) ok = mbar_wait(&tempty[b], (uint32_t) (((li >> 1) - 1) & 1), 43);
+            if (!ok) break;
+            fence_after_sync();
+            const uint32_t acc = tmem + b * ACC_COLS;
+            for (int kb = 0; kb < nk && ok; kb++, g++) {
+                const int s = (int) (g % STAGES);
+                ok = mbar_wait(&full[s], (uint32_t) ((g / STAGES) & 1), 44);
+                if (!ok) break;
+                fence_after_sync();
+                const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
+                if (kb == 0) mma_chunk4<true>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + BMAX_BYTES,
+                                              acc, idesc);
+                else mma_chunk4<false>(a_hi, a_hi + A_BYTES, a_hi + 2 * A_BYTES, a_hi + 2 * A_BYTES + BMAX_BYTES,
+                                       acc, idesc);
+                umma_commit(&empty[s]);
+            }
+            umma_commit(&tfull[b]);
+        }
+    } else if (warp >= 2) {
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int row = quad * 32 + lane;
+        const uint32_t tq = tmem + ((uint32_t) (quad * 32) << 16);
+        uint32_t rm[32];
+        float dtv[32];
+        bool ok = true;
+        int li = 0;
+        for (int it = blockIdx.x; it < total && ok; it += gridDim.x, li++) {
+            const int m = find_mol(starts, nmol, it);
+            const KMixDev &d = mols[m];
+            const HalfArgs &ha = d.ha;
+            const int t = it - starts[m];
+            const int i = t / ha.ptiles, m0 = (t % ha.ptiles) * UM;
+            const int nk = ha.row_chunk0[i + 1] - ha.row_chunk0[i];
+            const int b = li & 1;
+            ok = mbar_wait(&tfull[b], (uint32_t) ((li >> 1) & 1), 45);
+            if (!ok) break;
+            fence_after_sync();
+            const int P = m0 + row;
+            const size_t base = (size_t) i * ha.Qp + P;
+            for (int c0 = half * 32; c0 < d.bn; c0 += 64) {
+                if (nk > 0) {
+                    tmem_ld32(tq + b * ACC_COLS + c0, rm);
+#pragma unroll
+                    for (int q = 0; q < 32; q++) dtv[q] = __uint_as_float(rm[q]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 32; q++) dtv[q] = 0.f;
+                }
+                if (P >= ha.naux) continue;
+#pragma unroll
+                for (int h16 = 0; h16 < 32; h16 += 16) {
+                    float told[16];
+#pragma unroll
+                    for (int q = h16; q < h16 + 16; q++) {
+                        const int sq = c0 + q;
+                        told[q - h16] = (sq < ha.nocc) ? ha.Tm[base + (size_t) sq * ha.naux] : 0.f;
+                    }
+#pragma unroll
+                    for (int q = h16; q < h16 + 16; q++) {
+                        const int sq = c0 + q;
+                        if (sq < ha.nocc) {
+                            const size_t idx = base + (size_t) sq * ha.naux;
+                            const float dt = dtv[q];
+                            const float tnew = told[q - h16] + dt;
+                            ha.Tm[idx] = tnew;
+                            __nv_bfloat16 h, l;
+                            split_bf16(dt, h, l);
+                            ha.dTh[idx] = h;
+                            ha.dTl[idx] = l;
+                            split_bf16(told[q - h16] + tnew, h, l);
+                            ha.Sh[idx] = h;
+                            ha.Sl[idx] = l;
+                        }
+                    }
+                }
+            }
+            fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after_sync();
+        tmem_dealloc_warp(tmem, TMEM_COLS);
+    }
+}
+
+// k_gemm2 over the tiles of many molecules: pair item p = blockIdx.x / 2 is
+// (molecule, 256-row tile x, tile y, split) of that molecule's own G GEMM.
+__global__ void __launch_bounds__(THREADS, 1)
+kb_gemm2(const KMixDev *__restrict__ mols, const int *__restrict__ starts, int nmol)
+{
+    const int p = blockIdx.x >> 1;
+    const int m = find_mol(starts, nmol, p);
+    const KMixDev &d = mols[m];
+    const int local = p - starts[m];
+    const int tx = local % d.mt, ty = (local / d.mt) % d.mt, split = local / (d.mt * d.mt);
+    gemm2_body(&d.mdTh, &d.mdTl, &d.mSh, &d.mSl, d.ga, tx, ty, split);
 }
 
 template <int BN, int STAGES>
@@ -783,11 +997,12 @@ int kmix_create(KMix **out, const FockPlan &p, const int *h_displs, cudaStream_t
     // the CTA count rounded up to whole waves of 148 when that costs little.
     const int mt = (p.nbf + UM - 1) / UM;
     const int tiles = mt * mt;
-    int ks = std::max((4 * 148 + tiles - 1) / tiles, (k->total_chunks + SEG_CHUNKS * MAX_SEGS - 1) / (SEG_CHUNKS * MAX_SEGS));
+    const int nsm = num_sms();
+    int ks = std::max((4 * nsm + tiles - 1) / tiles, (k->total_chunks + SEG_CHUNKS * MAX_SEGS - 1) / (SEG_CHUNKS * MAX_SEGS));
     {
         int best = ks;
         for (int c = ks; c <= ks + ks / 4 + 1; c++)
-            if ((tiles * c) % 148 == 0) {
+            if ((tiles * c) % nsm == 0) {
                 best = c;
                 break;
             }
@@ -877,10 +1092,7 @@ static int launch_half(const KMix *k, HalfArgs ha, cudaStream_t s)
     }
     ha.ptiles = (k->naux + UM - 1) / UM;
     ha.n_items = k->nbf * ha.ptiles;
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = std::max(1, std::min(ha.n_items, nsm));
+    const int grid = std::max(1, std::min(ha.n_items, num_sms()));
     k_half<BN, STAGES><<<grid, THREADS, SMEM, s>>>(k->mBh, k->mBl, k->mCh, k->mCl, ha);
     g_launches++;
     return OK;
@@ -965,8 +1177,9 @@ static int launch_gemm(const KMix *k, const GArgs &ga, cudaStream_t s)
 }
 
 // One incremental K build from the new occupied factor Cocc (nbf x nocc).
-int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s,
-               const std::function<void(int)> &mark)
+// Alignment of the new occupied factor and the gathered dC operands of one
+// molecule (everything of an incremental K build before the half-transform).
+static void kmix_prepare(KMix *k, const double *Cocc, const double *S, cudaStream_t s)
 {
     const int n = k->nbf, o = k->nocc;
     // align C_n to C_{n-1}: R = polar(C_n^T S C_{n-1}) by Newton-Schulz; R = I if it does not converge
@@ -987,7 +1200,30 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     dim3 gg((unsigned) ((k->rp + 255) / 256), k->bn_half);
     k_gather_dc<<<gg, 256, 0, s>>>(k->dC, k->pad_entry, k->csr_j, o, k->rp, k->Ch, k->Cl);
     g_launches += 3;
-    HalfArgs ha{k->row_chunk0, k->Tm, k->dTh, k->dTl, k->Sh, k->Sl, o, k->naux, k->Qp, 0, 0};
+}
+
+// K += sym(sum over splits of G) (the first build of a solve sets K).
+static void kmix_finish(KMix *k, double *K, cudaStream_t s)
+{
+    const size_t nn = (size_t) k->nbf * k->nbf;
+    k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, k->ksplit, k->nbf, k->first ? 1 : 0, K);
+    g_launches++;
+    k->first = false;
+}
+
+static HalfArgs half_args(const KMix *k)
+{
+    HalfArgs ha{k->row_chunk0, k->Tm, k->dTh, k->dTl, k->Sh, k->Sl, k->nocc, k->naux, k->Qp, 0, 0};
+    ha.ptiles = (k->naux + UM - 1) / UM;
+    ha.n_items = k->nbf * ha.ptiles;
+    return ha;
+}
+
+int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s,
+               const std::function<void(int)> &mark)
+{
+    kmix_prepare(k, Cocc, S, s);
+    HalfArgs ha = half_args(k);
     int rc;
     if (mark) mark(0);
     switch (k->bn_half) {
@@ -1011,15 +1247,134 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     }
     if (rc) return rc;
     if (mark) mark(1);
-    GArgs ga{k->G, n, k->chunks_per_split, k->total_chunks};
+    GArgs ga{k->G, k->nbf, k->chunks_per_split, k->total_chunks};
     rc = launch_gemm(k, ga, s);
     if (rc) return rc;
     if (mark) mark(2);
-    const size_t nn = (size_t) n * n;
-    k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, k->ksplit, n, k->first ? 1 : 0, K);
-    g_launches++;
-    k->first = false;
+    kmix_finish(k, K, s);
     return OK;
+}
+
+// ---------------------------------------------------------------- many molecules in one launch per kernel
+struct KMixBatch {
+    std::vector<KMix *> ks;
+    KMixDev *d_mols = nullptr;
+    int *d_starts = nullptr;           // [2][nmol + 1]: half-transform items, G GEMM pair items
+    std::vector<int> h_starts;
+    int max_bn = 0;
+};
+
+void kmix_batch_destroy(KMixBatch *b)
+{
+    if (!b) return;
+    cudaFree(b->d_mols);
+    cudaFree(b->d_starts);
+    delete b;
+}
+
+int kmix_batch_create(KMixBatch **out, KMix *const *ks, int n, cudaStream_t s)
+{
+    *out = nullptr;
+    if (n <= 0) return ERR_INPUT;
+    KMixBatch *b = new KMixBatch();
+    b->ks.assign(ks, ks + n);
+    std::vector<KMixDev> h(n);
+    for (int m = 0; m < n; m++) {
+        const KMix *k = ks[m];
+        KMixDev &d = h[m];
+        memset(&d, 0, sizeof(d));
+        d.mBh = k->mBh;
+        d.mBl = k->mBl;
+        d.mCh = k->mCh;
+        d.mCl = k->mCl;
+        d.mdTh = k->mdTh;
+        d.mdTl = k->mdTl;
+        d.mSh = k->mSh;
+        d.mSl = k->mSl;
+        d.ha = half_args(k);
+        d.ga.part = k->G;
+        d.ga.nbf = k->nbf;
+        d.ga.chunks_per_split = k->chunks_per_split;
+        d.ga.total_chunks = k->total_chunks;
+        d.ga.probe = 0;
+        d.ga.wait_cycles = WAIT_CYCLES;
+        d.bn = k->bn_half;
+        d.mt = (k->nbf + PAIR_N - 1) / PAIR_N;
+        d.ksplit = k->ksplit;
+        b->max_bn = std::max(b->max_bn, d.bn);
+    }
+    b->h_starts.assign(2 * (n + 1), 0);
+    if (cudaMalloc(&b->d_mols, sizeof(KMixDev) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_starts, sizeof(int) * 2 * (n + 1)) != cudaSuccess ||
+        cudaMemcpyAsync(b->d_mols, h.data(), sizeof(KMixDev) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        kmix_batch_destroy(b);
+        return ERR_ALLOC;
+    }
+    *out = b;
+    return OK;
+}
+
+// One incremental K build of every molecule m with active[m] != 0: the
+// alignments per molecule, then one half-transform launch and one G GEMM
+// launch over all of them, then the per-molecule reductions into K[m].
+int kmix_batch_build(KMixBatch *b, const int *active, const double *const *Cocc, const double *const *S,
+                     double *const *K, cudaStream_t s)
+{
+    const int n = (int) b->ks.size();
+    int *hh = b->h_starts.data(), *hg = hh + n + 1;
+    hh[0] = hg[0] = 0;
+    for (int m = 0; m < n; m++) {
+        const KMix *k = b->ks[m];
+        const int mt = (k->nbf + PAIR_N - 1) / PAIR_N;
+        hh[m + 1] = hh[m] + (active[m] ? k->nbf * ((k->naux + UM - 1) / UM) : 0);
+        hg[m + 1] = hg[m] + (active[m] ? mt * mt * k->ksplit : 0);
+    }
+    if (hh[n] == 0) return OK;
+    for (int m = 0; m < n; m++)
+        if (active[m]) kmix_prepare(b->ks[m], Cocc[m], S[m], s);
+    TSCF_CUDA_CHECK(cudaMemcpyAsync(b->d_starts, hh, sizeof(int) * 2 * (n + 1), cudaMemcpyHostToDevice, s));
+    {
+        constexpr int SMEM = kb_half_smem_bytes();
+        static bool attr_set = false;
+        if (!attr_set) {
+            if (cudaFuncSetAttribute(kb_half, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+                return ERR_CUDA;
+            attr_set = true;
+        }
+        const int grid = std::max(1, std::min(hh[n], num_sms()));
+        kb_half<<<grid, THREADS, SMEM, s>>>(b->d_mols, b->d_starts, n);
+        g_launches++;
+    }
+    {
+        constexpr int SMEM = pair_smem_bytes();
+        static bool attr_set = false;
+        if (!attr_set) {
+            if (cudaFuncSetAttribute(kb_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+                return ERR_CUDA;
+            attr_set = true;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * hg[n]);
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        g_launches++;
+        if (cudaLaunchKernelEx(&cfg, kb_gemm2, (const KMixDev *) b->d_mols, (const int *) (b->d_starts + n + 1), n) !=
+            cudaSuccess)
+            return ERR_CUDA;
+    }
+    for (int m = 0; m < n; m++)
+        if (active[m]) kmix_finish(b->ks[m], K[m], s);
+    return cuda_launch_rc("batched tensor-core exchange");
 }
 
 int kmix_error_flag()

@@ -251,9 +251,24 @@ void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const do
     if (m <= 0 || n <= 0) return;
     int v = 4;
     const double tiles64 = std::ceil(m / 64.0) * std::ceil(n / 64.0);
-    if (k >= 256 && tiles64 < 2.0 * 148) v = 5;
-    else if ((double) m * n >= 4.0 * 148 * 128 * 128) v = 3;
+    const double nsm = num_sms();
+    if (k >= 256 && tiles64 < 2.0 * nsm) v = 5;
+    else if ((double) m * n >= 4.0 * nsm * 128 * 128) v = 3;
     dgemm_variant(v, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+}
+
+int num_sms()
+{
+    static int cached[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = v > 0 ? v : 1;
+    }
+    return cached[dev];
 }
 
 int cuda_launch_rc(const char *what)
@@ -388,7 +403,15 @@ __device__ ValIdx block_argmax(ValIdx x, ValIdx *sh)
     return r;
 }
 
-__global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, int *piv, int *rank_out, double *work)
+// blkp (nullptr: one block): the block of every position, permuted with the
+// pivots. A is block diagonal in these blocks (the SAD density: one block per
+// atom), so column j of the factor is nonzero only in the rows of the pivot's
+// block and every product with another block's entry is an exact zero: the
+// rows of other blocks are skipped and their squared-norm sums left alone,
+// which changes no bit of the result (adding +-0 is exact) but makes each
+// step cost the pivot search instead of an (n - j) x j update.
+__global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, int *piv, int *rank_out, double *work,
+                                                int *blkp)
 {
     __shared__ ValIdx sh[32];
     __shared__ int s_stop;
@@ -415,9 +438,12 @@ __global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, in
     for (int j = 0; j < n; j++) {
         if (j > 0) {
             ValIdx b{-DBL_MAX, 0x7fffffff};
+            const int bprev = blkp ? blkp[j - 1] : 0;
             for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
-                double a = AA(i, j - 1);
-                dot[i] += a * a;
+                if (!blkp || blkp[i] == bprev) {
+                    double a = AA(i, j - 1);
+                    dot[i] += a * a;
+                }
                 double c = AA(i, i) - dot[i];
                 cand[i] = c;
                 b = better(b, ValIdx{c, i});
@@ -437,6 +463,9 @@ __global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, in
                 AA(pvt, pvt) = AA(j, j);
                 double t = dot[j]; dot[j] = dot[pvt]; dot[pvt] = t;
                 int p = piv[pvt]; piv[pvt] = piv[j]; piv[j] = p;
+                if (blkp) {
+                    const int q = blkp[pvt]; blkp[pvt] = blkp[j]; blkp[j] = q;
+                }
             }
             for (int c = threadIdx.x; c < j; c += blockDim.x) {          // rows j and pvt, columns 0..j-1
                 double t = AA(j, c); AA(j, c) = AA(pvt, c); AA(pvt, c) = t;
@@ -455,9 +484,12 @@ __global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, in
         // A(j+1:n, j) = (A(j+1:n, j) - A(j+1:n, 0:j) A(j, 0:j)^T) / ajj : one warp per row
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
         const double rinv = 1.0 / ajj;
+        const int bj = blkp ? blkp[j] : 0;
         for (int r = j + 1 + wid; r < n; r += nw) {
+            if (blkp && blkp[r] != bj) continue;   // zero column entry: (0 - 0) / ajj stays +0
             double s = 0.0;
-            for (int c = lane; c < j; c += 32) s += AA(r, c) * AA(j, c);
+            for (int c = lane; c < j; c += 32)
+                if (!blkp || blkp[c] == bj) s += AA(r, c) * AA(j, c);
             for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffff, s, o);
             if (lane == 0) AA(r, j) = (AA(r, j) - s) * rinv;
         }
@@ -467,10 +499,16 @@ __global__ void __launch_bounds__(1024) k_pstf2(double *A, int n, double tol, in
 #undef AA
 }
 
-void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s)
+void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s,
+                      const int *d_blk, int *d_blk_work)
 {
     g_launches++;
-    k_pstf2<<<1, 1024, 0, s>>>(d_A, n, tol, d_piv, d_rank, d_work);
+    int *blkp = nullptr;
+    if (d_blk && d_blk_work) {
+        cudaMemcpyAsync(d_blk_work, d_blk, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
+        blkp = d_blk_work;
+    }
+    k_pstf2<<<1, 1024, 0, s>>>(d_A, n, tol, d_piv, d_rank, d_work, blkp);
 }
 
 __global__ void k_d2cocc(const double *chol, const int *rank_p, double *C, int nbf, int nocc)

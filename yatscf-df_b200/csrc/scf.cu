@@ -151,7 +151,96 @@ __device__ void diis_solve_body(DiisState *st)
     for (int i = 0; i < n; i++) st->coef[i] = b[i];
 }
 
-__global__ void k_diis_solve(DiisState *st) { diis_solve_body(st); }
+// The same update and elimination with one warp: lane i holds row i of the
+// bordered system (n <= MAXDIIS + 1 <= 32), the pivot search is a first-maximum
+// reduction over the lanes, and each lane eliminates its own row with the
+// pivot row broadcast by shuffles; the arithmetic of every element is that
+// of diis_solve_body.
+__global__ void __launch_bounds__(32) k_diis_solve(DiisState *st)
+{
+    constexpr int ld = MAXDIIS + 1;
+    const int lane = threadIdx.x;
+    const int len = st->len, idx = st->idx, n = len + 1;
+    if (lane < len) {
+        st->B[idx * ld + lane] = st->dots[lane];
+        st->B[lane * ld + idx] = st->dots[lane];
+    }
+    __syncwarp();
+    if (lane == 0)
+        for (int i = 0; i < len; i++)
+            if (st->B[i * ld + i] > st->bmax) {
+                st->bmax = st->B[i * ld + i];
+                st->bmax_id = i;
+            }
+    double a[ld], b;
+#pragma unroll
+    for (int j = 0; j < ld; j++) a[j] = (lane < n && j < n) ? st->B[lane * ld + j] : 0.0;
+    b = (lane == len) ? -1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < ld; k++) {
+        if (k >= n) break;
+        // first maximum of |a(i, k)| over rows i >= k
+        double mx = (lane >= k && lane < n) ? fabs(a[k]) : -1.0;
+        int p = lane;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double m2 = __shfl_xor_sync(0xffffffff, mx, o);
+            const int p2 = __shfl_xor_sync(0xffffffff, p, o);
+            if (m2 > mx || (m2 == mx && p2 < p)) {
+                mx = m2;
+                p = p2;
+            }
+        }
+        p = __shfl_sync(0xffffffff, p, 0);   // one pivot for the whole warp (even with NaN entries)
+        if (p != k) {   // swap rows k and p
+#pragma unroll
+            for (int j = 0; j < ld; j++) {
+                const double vk = __shfl_sync(0xffffffff, a[j], k), vp = __shfl_sync(0xffffffff, a[j], p);
+                if (lane == k) a[j] = vp;
+                if (lane == p) a[j] = vk;
+            }
+            const double bk = __shfl_sync(0xffffffff, b, k), bp = __shfl_sync(0xffffffff, b, p);
+            if (lane == k) b = bp;
+            if (lane == p) b = bk;
+        }
+        double prow[ld];
+#pragma unroll
+        for (int j = 0; j < ld; j++) prow[j] = __shfl_sync(0xffffffff, a[j], k);
+        const double bkk = __shfl_sync(0xffffffff, b, k);
+        const double piv = prow[k];
+        if (piv == 0.0) continue;
+        if (lane > k && lane < n) {
+            const double f = a[k] / piv;
+            a[k] = f;
+#pragma unroll
+            for (int j = 0; j < ld; j++)
+                if (j > k && j < n) a[j] -= f * prow[j];
+            b -= f * bkk;
+        }
+    }
+    // back substitution from the last row; each solved entry is broadcast
+    double sol[ld];
+#pragma unroll
+    for (int j = 0; j < ld; j++) sol[j] = 0.0;
+    for (int i = n - 1; i >= 0; i--) {
+        double v = 0.0;
+        if (lane == i) {
+            double s2 = b;
+#pragma unroll
+            for (int j = 0; j < ld; j++)
+                if (j > i && j < n) s2 -= a[j] * sol[j];
+            v = s2 / a[i];
+        }
+        v = __shfl_sync(0xffffffff, v, i);
+#pragma unroll
+        for (int j = 0; j < ld; j++)
+            if (j == i) sol[j] = v;
+    }
+    if (lane < n) {
+#pragma unroll
+        for (int j = 0; j < ld; j++)
+            if (j == lane) st->coef[lane] = sol[j];
+    }
+}
 
 // one thread per molecule of a batch
 __global__ void k_diis_solve_batched(const MolDev *mols, const int *active, int nmol)
@@ -194,7 +283,7 @@ void diis_step(DiisState *st, int max_diis, const double *d_F, const double *d_D
     k_diis_dots<<<MAXDIIS, 1024, 0, s>>>(d_R, st, nn);
     xtfx(d_X, d_F, d_tmp2, d_tmp, n, s);                                     // X^T F X
     k_copy_to_slot<<<nb, 256, 0, s>>>(d_tmp2, d_F0, st, nn);
-    k_diis_solve<<<1, 1, 0, s>>>(st);
+    k_diis_solve<<<1, 32, 0, s>>>(st);
     k_diis_combine<<<nb, 256, 0, s>>>(d_F0, st, d_Fout, nn);
 }
 
@@ -231,7 +320,7 @@ void diis_step_cocc(DiisState *st, int max_diis, const double *d_F, const double
     k_diis_dots<<<MAXDIIS, 1024, 0, s>>>(d_R, st, nn);
     xtfx(d_X, d_F, d_tmp2, d_tmp, n, s);                                           // X^T F X
     k_copy_to_slot<<<nb, 256, 0, s>>>(d_tmp2, d_F0, st, nn);
-    k_diis_solve<<<1, 1, 0, s>>>(st);
+    k_diis_solve<<<1, 32, 0, s>>>(st);
     k_diis_combine<<<nb, 256, 0, s>>>(d_F0, st, d_Fout, nn);
 }
 
@@ -326,7 +415,7 @@ static void refine_residual(const double *d_Fp, const double *d_U, int n, int o,
     dgemm(true, false, n, o, o, 1.0, d_U, n, w.UA, o, 0.0, w.R, o, s);         // R = U^T UA
     k_sub<<<(unsigned) (((size_t) n * o + 255) / 256), 256, 0, s>>>(w.A, w.R, (size_t) n * o);   // R = A - R
     cudaMemsetAsync(w.res, 0, sizeof(double), s);
-    k_absmax<<<148, 256, 0, s>>>(w.R, (size_t) n * o, w.res);
+    k_absmax<<<num_sms(), 256, 0, s>>>(w.R, (size_t) n * o, w.res);
     g_launches += 2;
 }
 

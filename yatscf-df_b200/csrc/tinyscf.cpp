@@ -280,6 +280,7 @@ struct Engine {
     DiisState *diis = nullptr;
     double *sp_scr = nullptr, *bf_scr = nullptr, *df_scr = nullptr;
     int *piv = nullptr, *rank = nullptr;
+    int *bf_atom = nullptr, *bf_atom_work = nullptr;   // atom of each basis function (SAD blocks)
     double *pwork = nullptr;
     // sparsity
     int nnz = 0, nu = 0, nup = 0;
@@ -766,9 +767,10 @@ int sparsity_impl(TinySCF_t t)
     RC(dalloc(e, &e->T, (size_t) nbf * nocc * naux));
     const int nt = (nbf + 63) / 64, ntiles = nt * (nt + 1) / 2;
     const int nt2 = (nbf + 127) / 128, ntiles2 = nt2 * (nt2 + 1) / 2;
-    e->ksplit = std::max(1, std::min(64, (4 * 148 + ntiles - 1) / ntiles));
+    const int nsm = num_sms();
+    e->ksplit = std::max(1, std::min(64, (4 * nsm + ntiles - 1) / ntiles));
     e->ksplit64 = e->ksplit;
-    const int h128 = std::max(1, std::min(64, (2 * 148 + ntiles2 - 1) / ntiles2));
+    const int h128 = std::max(1, std::min(64, (2 * nsm + ntiles2 - 1) / ntiles2));
     e->ksplit_max = std::min(64, 2 * std::max(e->ksplit, h128));   // room for the autotuner's candidates
     // untuned defaults by size: the larger register tiles pay off once there are enough of them
     if (nbf >= 384) {
@@ -788,7 +790,7 @@ int sparsity_impl(TinySCF_t t)
     }
     FockPlan p = e->plan();
     e->jblk = build_J_part_blocks(p);
-    e->jblk_max = std::max(e->jblk, std::min(4 * 148, std::max(1, e->nup)));
+    e->jblk_max = std::max(e->jblk, std::min(4 * num_sms(), std::max(1, e->nup)));
     RC(dalloc(e, &e->Jt, naux));
     RC(dalloc(e, &e->Jpart, (size_t) e->jblk_max * naux));
     RC(dalloc(e, &e->Jw, std::max(1, e->nup)));
@@ -911,7 +913,21 @@ int guess_impl(TinySCF_t t)
     TSCF_CUDA_CHECK(cudaMemcpyAsync(e->D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, e->s));
     e->h2d += (long long) (sizeof(double) * D.size());
     TSCF_CUDA_CHECK(cudaMemcpyAsync(e->tmp, e->D, sizeof(double) * D.size(), cudaMemcpyDeviceToDevice, e->s));
-    pivoted_cholesky(e->tmp, nbf, 1e-12, e->piv, e->rank, e->pwork, e->s);
+    // the SAD density is block diagonal by atom: the factorisation skips the
+    // other atoms' exact zeros (TINYSCF_PSTF_BLOCKS=0: the dense kernel)
+    const char *pb = getenv("TINYSCF_PSTF_BLOCKS");
+    if (!(pb && pb[0] == '0')) {
+        if (!e->bf_atom) {
+            std::vector<int> ba(nbf, 0);
+            for (int a = 0; a < t->natoms; a++)
+                for (int b = e->sh.atom_bf0[a]; b < e->sh.atom_bf1[a]; b++) ba[b] = a;
+            RC(upload(e, &e->bf_atom, ba));
+            RC(dalloc(e, &e->bf_atom_work, nbf));
+        }
+        pivoted_cholesky(e->tmp, nbf, 1e-12, e->piv, e->rank, e->pwork, e->s, e->bf_atom, e->bf_atom_work);
+    } else {
+        pivoted_cholesky(e->tmp, nbf, 1e-12, e->piv, e->rank, e->pwork, e->s);
+    }
     d2cocc_copy(e->tmp, e->rank, e->Cocc, nbf, nocc, e->s);
     tstop(e, TINYSCF_T_GUESS);
     RC(cuda_rc("initial guess"));
@@ -966,7 +982,7 @@ int autotune_fock(TinySCF_t t)
     int c = tune_lookup(key);
     if (c < 0) {
         const int nt2 = (t->nbasfuncs + 127) / 128, ntiles2 = nt2 * (nt2 + 1) / 2;
-        const int h128 = std::max(1, std::min(64, (2 * 148 + ntiles2 - 1) / ntiles2));
+        const int h128 = std::max(1, std::min(64, (2 * num_sms() + ntiles2 - 1) / ntiles2));
         std::vector<int> cand;
         for (int v : {std::max(1, e->ksplit64 / 2), e->ksplit64, std::min(e->ksplit_max, 2 * e->ksplit64)})
             if (std::find(cand.begin(), cand.end(), 64000 + v) == cand.end()) cand.push_back(64000 + v);
@@ -1016,7 +1032,8 @@ int autotune_fock(TinySCF_t t)
     c = tune_lookup(key);
     if (c < 0) {
         std::vector<int> cand;
-        for (int v : {148, 296, 592})
+        const int nsm = num_sms();
+        for (int v : {nsm, 2 * nsm, 4 * nsm})
             if (v <= e->jblk_max && std::find(cand.begin(), cand.end(), v) == cand.end()) cand.push_back(v);
         if (cand.empty()) cand.push_back(e->jblk);
         c = tune_run(key, cand, [&](int nb) { build_J(p, e->D, e->J, e->Jt, e->Jpart, nb, e->Jw, e->s); }, e->s);
@@ -1922,6 +1939,10 @@ struct TinySCF_batch_struct {
     int *d_kact = nullptr;             // molecules whose K the batched FP64 kernels build this iteration
     int *d_need = nullptr;             // molecules whose density takes an eigensolve this iteration
     std::vector<char> mixed;           // molecules with the tensor-core incremental K
+    KMixBatch *kmb = nullptr;          // their K builds, one launch per tensor-core kernel (null: one by one)
+    std::vector<int> kmb_mol, kmb_act; // batch index and active flag of each of them
+    std::vector<const double *> kmb_C, kmb_S;
+    std::vector<double *> kmb_K;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double scf_ms = 0.0;
     int iterations = 0;
@@ -2102,6 +2123,21 @@ int batch_create_impl(TinySCF_batch_t b, TinySCF_t *ts, int nmol)
     RC(balloc(b, &b->d_need, nmol));
     b->mixed.assign(nmol, 0);
     for (int k = 0; k < nmol; k++) b->mixed[k] = E_(ts[k])->kprec == TINYSCF_K_MIXED && E_(ts[k])->kmix != nullptr;
+    {   // TINYSCF_BATCH_KMIX=0: the mixed molecules' K builds one molecule at a time
+        const char *v = getenv("TINYSCF_BATCH_KMIX");
+        std::vector<KMix *> ks;
+        for (int k = 0; k < nmol; k++)
+            if (b->mixed[k]) {
+                Engine *e = E_(ts[k]);
+                ks.push_back(e->kmix);
+                b->kmb_mol.push_back(k);
+                b->kmb_C.push_back(e->Cocc);
+                b->kmb_S.push_back(e->S);
+                b->kmb_K.push_back(e->Kmix);
+            }
+        b->kmb_act.assign(ks.size(), 0);
+        if (!ks.empty() && !(v && v[0] == '0')) RC(kmix_batch_create(&b->kmb, ks.data(), (int) ks.size(), b->s));
+    }
     RC(make_list(b, c_nup256, p.nup256));
     RC(make_list(b, c_jblk, p.jblk));
     RC(make_list(b, c_naux256, p.naux256));
@@ -2172,10 +2208,14 @@ int batch_scf_impl(TinySCF_batch_t b)
         batch_j(b->plan, b->s);
         cudaEventRecord(b->pev[1], b->s);
         batch_k(b->plan, b->d_kact, b->s);
-        for (int k = 0; k < nmol; k++) {   // tensor-core incremental exchange, one molecule at a time
+        if (b->kmb) {   // tensor-core incremental exchange of every mixed molecule: one launch per kernel
+            for (size_t j = 0; j < b->kmb_mol.size(); j++) b->kmb_act[j] = act[b->kmb_mol[j]];
+            RC(kmix_batch_build(b->kmb, b->kmb_act.data(), b->kmb_C.data(), b->kmb_S.data(), b->kmb_K.data(), b->s));
+        }
+        for (int k = 0; k < nmol; k++) {
             if (!act[k] || !b->mixed[k]) continue;
             Engine *e = E_(b->mols[k]);
-            RC(kmix_build(e->kmix, e->Cocc, e->S, e->Kmix, b->s));
+            if (!b->kmb) RC(kmix_build(e->kmix, e->Cocc, e->S, e->Kmix, b->s));   // one molecule at a time
             TSCF_CUDA_CHECK(cudaMemcpyAsync(e->K, e->Kmix, sizeof(double) * e->nn, cudaMemcpyDeviceToDevice, b->s));
         }
         cudaEventRecord(b->pev[2], b->s);
@@ -2299,6 +2339,7 @@ int batch_scf_impl(TinySCF_batch_t b)
 void batch_free_impl(TinySCF_batch_t b)
 {
     if (b->s) cudaStreamSynchronize(b->s);
+    kmix_batch_destroy(b->kmb);
     for (auto &g : b->groups) eig_destroy(g.eig);
     for (void *p : b->mem) cudaFree(p);
     for (auto &ev : b->pev)

@@ -125,6 +125,8 @@ void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const do
                    const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s);
 // ERR_CUDA (with a message) when a launch since the last check failed; the error is not cleared.
 int cuda_launch_rc(const char *what);
+// Streaming multiprocessors of the current device (queried once per device).
+int num_sms();
 
 // Device buffers of the engine (linalg.cu): from the device's stream-ordered
 // pool, kept reserved across engines, unless TINYSCF_MEMPOOL=0. dev_malloc
@@ -159,8 +161,11 @@ int dominant_subspace(Eig *e, const double *d_M, double *d_U, double *d_W, doubl
 void inv_sqrt_from_eig(const double *d_w, const double *d_V, double *d_X, double *d_tmp, int n, cudaStream_t s);
 
 // LAPACK dpstf2 semantics (unblocked pivoted Cholesky, lower, first-max pivot),
-// applied to a row-major symmetric matrix in place; rank to *d_rank.
-void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s);
+// applied to a row-major symmetric matrix in place; rank to *d_rank. d_blk
+// (optional, n ints; d_blk_work: n ints of scratch): a block id per row when A
+// is block diagonal in those blocks; the result is the same, bit for bit.
+void pivoted_cholesky(double *d_A, int n, double tol, int *d_piv, int *d_rank, double *d_work, cudaStream_t s,
+                      const int *d_blk = nullptr, int *d_blk_work = nullptr);
 // TinySCF_D2Cocc's copy of the factor into Cocc (TinySCF.c:297-319).
 void d2cocc_copy(const double *d_chol, const int *d_rank, double *d_Cocc, int nbf, int nocc, cudaStream_t s);
 
@@ -223,6 +228,15 @@ void kmix_reset(KMix *k, cudaStream_t s);
 int  kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStream_t s,
                 const std::function<void(int)> &mark = nullptr);
 int  kmix_error_flag();
+// Many molecules' incremental K builds with one half-transform launch and one
+// G GEMM launch over all of them (the alignments and reductions stay per
+// molecule). ks: the molecules' KMix objects (owned by the caller).
+struct KMixBatch;
+int  kmix_batch_create(KMixBatch **out, KMix *const *ks, int n, cudaStream_t s);
+void kmix_batch_destroy(KMixBatch *b);
+// active[m] (host): molecules to build; Cocc[m], S[m] their inputs, K[m] their K (FP64, accumulated).
+int  kmix_batch_build(KMixBatch *b, const int *active, const double *const *Cocc, const double *const *S,
+                      double *const *K, cudaStream_t s);
 // Runs the G GEMM kernel's bounded waits out on purpose (no copies issued,
 // waits of wait_cycles clock cycles); *code receives the recorded wait code.
 int  kmix_wait_probe(KMix *k, long long wait_cycles, int *code, cudaStream_t s);
