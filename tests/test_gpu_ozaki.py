@@ -88,3 +88,25 @@ def test_engine_exchange_matches_fp64_kernels(mol, monkeypatch):
     assert n0 == 0 and n1 >= 2
     assert np.abs(K1 - K0).max() <= 1e-12 * np.abs(K0).max()
     assert abs(E1 - E0) < 1e-10, (E0, E1)
+
+
+@pytest.mark.parametrize("mol", ["c10h22", "c20h42"])
+def test_half_transform_variants_agree(mol, monkeypatch):
+    """The FP64 half-transform's tile variants (the autotuner's candidates for
+    build_Fock.c:259-285) give the same K: the 64 x 256 pipelined DMMA tiles
+    (3) against the 168 x 128 ones (4), both with the integer-tensor-core
+    rank-k product that takes its row scales from them."""
+    Ks = {}
+    for variant in ("3", "4"):
+        monkeypatch.setenv("TINYSCF_KHALF", variant)
+        monkeypatch.setenv("TINYSCF_OZAKI", "1")
+        e = tinyscf.TinySCF(os.path.join(DATA, "cc-pvdz", "cc-pvdz.gbs"),
+                            os.path.join(DATA, "cc-pVDZ-RI", "cc-pVDZ-RI.gbs"), os.path.join(DATA, mol + ".xyz"), 10)
+        try:
+            e.setup()
+            e.s.iter = 0
+            e.build_FockMat()
+            Ks[variant] = e.mat("K_mat").copy()
+        finally:
+            e.free()
+    assert np.abs(Ks["4"] - Ks["3"]).max() <= 1e-13 * np.abs(Ks["3"]).max()

@@ -305,6 +305,150 @@ __global__ void __launch_bounds__(256, 1)
     cp_async_wait<0>();
 }
 
+// ---- the same half-transform with 168 x 128 tiles over 12 warps (3 x 4 warps
+// of 56 x 32): n_occ up to 168 in one tile, so each CSR chunk of B is gathered
+// once per (row, aux tile) instead of once per 64-wide occupied tile, and
+// n_occ = 161 pads to 168 instead of 192.
+constexpr int KH2_S = 168, KH2_P = 128, KH2_THREADS = 384;
+constexpr int KH2_AS = KH2_S + 4, KH2_BS = KH2_P + 4;   // strides = 12 / 4 (mod 16) doubles: conflict-free fragments
+constexpr int KH2_STAGE_DOUBLES = KT_K * (KH2_AS + KH2_BS);
+constexpr size_t KH2_PIPE_SMEM = sizeof(double) * KH_STAGES * KH2_STAGE_DOUBLES;
+constexpr int KH2_NA = KT_K * KH2_S / KH2_THREADS;   // 7 Cocc copies per thread per step
+
+__device__ __forceinline__ void kh2_set(KhCursor &c, int item, int n_items, int stiles, int ptiles,
+                                        const int *__restrict__ displs)
+{
+    c.item = item;
+    if (item >= n_items) return;
+    const int per_row = stiles * ptiles;
+    c.i = item / per_row;
+    const int rem = item - c.i * per_row;
+    c.p0 = (rem / stiles) * KH2_P;
+    c.s0 = (rem % stiles) * KH2_S;
+    c.r0 = displs[c.i];
+    c.r_end = displs[c.i + 1];
+    c.step = 0;
+    c.nsteps = max(1, (c.r_end - c.r0 + KT_K - 1) / KT_K);
+}
+
+__device__ __forceinline__ void kh2_next(KhCursor &c, int n_items, int stiles, int ptiles,
+                                         const int *__restrict__ displs)
+{
+    if (c.item >= n_items) return;
+    if (++c.step < c.nsteps) c.r0 += KT_K;
+    else kh2_set(c, c.item + gridDim.x, n_items, stiles, ptiles, displs);
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(KH2_THREADS, 1)
+    k_halftransform_pipe2(const double *__restrict__ B, const double *__restrict__ C, const int *__restrict__ csr_j,
+                          const int *__restrict__ csr_u, const int *__restrict__ displs, int nocc, int naux,
+                          double *__restrict__ T, int n_items, int stiles, int ptiles, unsigned long long *rowmax)
+{
+    extern __shared__ __align__(16) double khsm[];
+    constexpr int BCOPY = VEC ? 2 : 1;                                   // doubles per B copy
+    constexpr int NBC = KT_K * KH2_P / BCOPY;                            // B copies per step
+    constexpr int NB = (NBC + KH2_THREADS - 1) / KH2_THREADS;            // per thread
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ws = (warp >> 2) * 56, wp = (warp & 3) * 32;
+    const int fr = lane >> 2, fc = lane & 3;
+    int iu[NB], ij[KH2_NA];
+    KhCursor P, Q;
+    kh2_set(P, blockIdx.x, n_items, stiles, ptiles, displs);
+    Q = P;
+    auto load_idx = [&]() {
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+            const int c = tid + KH2_THREADS * q;
+            const int r = P.r0 + c / (KH2_P / BCOPY);
+            iu[q] = (c < NBC && P.item < n_items && r < P.r_end) ? csr_u[r] : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < KH2_NA; q++) {
+            const int r = P.r0 + (tid + KH2_THREADS * q) / KH2_S;
+            ij[q] = (P.item < n_items && r < P.r_end) ? csr_j[r] : -1;
+        }
+    };
+    auto issue = [&](int buf) {
+        double *As = khsm + (size_t) buf * KH2_STAGE_DOUBLES, *Bs = As + KT_K * KH2_AS;
+        if (P.item < n_items) {
+#pragma unroll
+            for (int q = 0; q < NB; q++) {
+                const int c = tid + KH2_THREADS * q;
+                if (c < NBC) {
+                    const int kk = c / (KH2_P / BCOPY), cc = (c % (KH2_P / BCOPY)) * BCOPY;
+                    const int pg = P.p0 + cc;
+                    const bool ok = iu[q] >= 0 && pg < naux;
+                    const double *src = ok ? B + (size_t) iu[q] * naux + pg : B;
+                    if (VEC) cp_async16(&Bs[kk * KH2_BS + cc], src, ok ? 16 : 0);
+                    else cp_async8(&Bs[kk * KH2_BS + cc], src, ok ? 8 : 0);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < KH2_NA; q++) {
+                const int c = tid + KH2_THREADS * q;
+                const int kk = c / KH2_S, cc = c % KH2_S, sg = P.s0 + cc;
+                const bool ok = ij[q] >= 0 && sg < nocc;
+                cp_async8(&As[kk * KH2_AS + cc], ok ? C + (size_t) ij[q] * nocc + sg : C, ok ? 8 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    for (int st = 0; st < KH_STAGES - 1; st++) {
+        load_idx();
+        issue(st);
+        kh2_next(P, n_items, stiles, ptiles, displs);
+    }
+    load_idx();
+    double acc[7][4][2];
+#pragma unroll
+    for (int x = 0; x < 7; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y][0] = acc[x][y][1] = 0.0;
+    for (int g = 0; Q.item < n_items; g++) {
+        cp_async_wait<KH_STAGES - 2>();
+        __syncthreads();
+        issue((g + KH_STAGES - 1) % KH_STAGES);
+        kh2_next(P, n_items, stiles, ptiles, displs);
+        load_idx();
+        const double *As = khsm + (size_t) (g % KH_STAGES) * KH2_STAGE_DOUBLES, *Bs = As + KT_K * KH2_AS;
+#pragma unroll
+        for (int k4 = 0; k4 < KT_K; k4 += 4) {
+            double a[7], b[4];
+#pragma unroll
+            for (int x = 0; x < 7; x++) a[x] = As[(k4 + fc) * KH2_AS + ws + 8 * x + fr];
+#pragma unroll
+            for (int y = 0; y < 4; y++) b[y] = Bs[(k4 + fc) * KH2_BS + wp + 8 * y + fr];
+#pragma unroll
+            for (int x = 0; x < 7; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) dmma_8x8x4(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        if (++Q.step == Q.nsteps) {
+            double amax = 0.0;
+#pragma unroll
+            for (int x = 0; x < 7; x++) {
+                const int sg = Q.s0 + ws + 8 * x + fr;
+                double *row = T + ((size_t) Q.i * nocc + (sg < nocc ? sg : 0)) * naux;
+#pragma unroll
+                for (int y = 0; y < 4; y++) {
+                    const int pg = Q.p0 + wp + 8 * y + 2 * fc;
+                    if (sg < nocc && pg < naux) row[pg] = acc[x][y][0];
+                    if (sg < nocc && pg + 1 < naux) row[pg + 1] = acc[x][y][1];
+                    amax = fmax(amax, fmax(fabs(acc[x][y][0]), fabs(acc[x][y][1])));
+                    acc[x][y][0] = acc[x][y][1] = 0.0;
+                }
+            }
+            if (rowmax) {
+                for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffff, amax, o));
+                if (lane == 0 && amax > 0.0) atomicMax(rowmax + Q.i, (unsigned long long) __double_as_longlong(amax));
+            }
+            kh2_set(Q, Q.item + gridDim.x, n_items, stiles, ptiles, displs);
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // K partial tiles: upper tile pairs (bi <= bj) of 64x64, split over the
 // flattened Q = nocc*naux index. Kpart[split][i][j].
 __global__ void __launch_bounds__(256) k_syrk_part(const double *__restrict__ T, int nbf, long long Q, long long qchunk,
@@ -357,7 +501,22 @@ void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T,
 {
     if (p.nbf <= 0 || p.nocc <= 0 || p.naux <= 0) return;   // T is empty: no grid to launch
     g_launches++;
-    if (wide == 3) {
+    if (wide == 4) {
+        if (d_rowmax) cudaMemsetAsync(d_rowmax, 0, sizeof(unsigned long long) * p.nbf, s);
+        const int stiles = (p.nocc + KH2_S - 1) / KH2_S, ptiles = (p.naux + KH2_P - 1) / KH2_P;
+        const long long items = (long long) p.nbf * stiles * ptiles;
+        cudaFuncSetAttribute(k_halftransform_pipe2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int) KH2_PIPE_SMEM);
+        cudaFuncSetAttribute(k_halftransform_pipe2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int) KH2_PIPE_SMEM);
+        const int grid = (int) std::min<long long>(items, num_sms());
+        if (p.naux % 2 == 0)
+            k_halftransform_pipe2<true><<<grid, KH2_THREADS, KH2_PIPE_SMEM, s>>>(
+                p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T, (int) items, stiles, ptiles, d_rowmax);
+        else
+            k_halftransform_pipe2<false><<<grid, KH2_THREADS, KH2_PIPE_SMEM, s>>>(
+                p.B, d_Cocc, p.csr_j, p.csr_u, p.csr_displs, p.nocc, p.naux, d_T, (int) items, stiles, ptiles, d_rowmax);
+    } else if (wide == 3) {
         if (d_rowmax) cudaMemsetAsync(d_rowmax, 0, sizeof(unsigned long long) * p.nbf, s);
         const int stiles = (p.nocc + KH_S - 1) / KH_S, ptiles = (p.naux + KH_P - 1) / KH_P;
         const long long items = (long long) p.nbf * stiles * ptiles;

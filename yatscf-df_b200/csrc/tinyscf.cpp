@@ -1025,9 +1025,11 @@ int autotune_fock(TinySCF_t t)
     }
     snprintf(key, sizeof(key), "khalf:%d:%d:%d:%d", t->nbasfuncs, t->n_occ, t->df_nbf, e->nnz);
     c = tune_lookup(key);
+    if (const char *v = getenv("TINYSCF_KHALF"))   // a fixed half-transform variant (0-4) instead of timing them
+        if (v[0] >= '0' && v[0] <= '4' && v[1] == 0) c = v[0] - '0';
     if (c < 0)
-        c = tune_run(key, {0, 1, 2, 3}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
-    if (c >= 0 && c <= 3) e->khwide = c;
+        c = tune_run(key, {0, 1, 2, 3, 4}, [&](int w) { build_K_halftransform(p, e->Cocc, e->T, e->s, w); }, e->s);
+    if (c >= 0 && c <= 4) e->khwide = c;
     snprintf(key, sizeof(key), "jrows:%d:%d", e->nup, t->df_nbf);
     c = tune_lookup(key);
     if (c < 0) {
@@ -1144,7 +1146,7 @@ int fock_device(TinySCF_t t, bool force_fp64 = false)
     } else {
         // with the pipelined half-transform and the integer-tensor-core K, the
         // row maxima that K's scaling needs come out of the half-transform
-        unsigned long long *rm = (use_oz(e) && e->khwide == 3) ? oz_rowmax(e->oz) : nullptr;
+        unsigned long long *rm = (use_oz(e) && e->khwide >= 3) ? oz_rowmax(e->oz) : nullptr;
         tstart(e, TINYSCF_T_K_HT);
         build_K_halftransform(p, e->Cocc, e->T, e->s, e->khwide, rm);
         tstop(e, TINYSCF_T_K_HT);

@@ -198,9 +198,10 @@ void convert_f32(const double *in, float *out, size_t n, cudaStream_t s);
 // K from Cocc (build_Fock.c:244-347): T(i,s,P) = sum_j C(j,s) B(ij,P) ...
 // wide = 1: 64 x 256 FFMA tiles (k_halftransform_wide), 2: 64 x 256 DMMA tiles
 // (k_halftransform_dmma), 3: the same DMMA tiles in persistent CTAs with a
-// cp.async pipeline over the CSR chunks (k_halftransform_pipe), 0: 64 x 64
-// FFMA tiles
-// d_rowmax (wide = 3 only, else ignored): max_q |T(i, q)| of every row as
+// cp.async pipeline over the CSR chunks (k_halftransform_pipe), 4: 168 x 128
+// DMMA tiles over 12 warps in the same pipeline (k_halftransform_pipe2), 0:
+// 64 x 64 FFMA tiles
+// d_rowmax (wide = 3 or 4, else ignored): max_q |T(i, q)| of every row as
 // double bits, for the integer-tensor-core K.
 void build_K_halftransform(const FockPlan &p, const double *d_Cocc, double *d_T, cudaStream_t s, int wide = 0,
                            unsigned long long *d_rowmax = nullptr);
