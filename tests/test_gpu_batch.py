@@ -88,9 +88,10 @@ def test_batch_mixed_k_matches_single_molecule(tmp_path):
 
 
 def test_batch_mixed_k_one_launch_per_kernel(tmp_path, monkeypatch):
-    """The mixed molecules' tensor-core K of a batch runs as one half-transform
-    launch and one G GEMM launch over all of them: the same arithmetic per
-    molecule as their builds one by one (identical energies), fewer launches."""
+    """With TINYSCF_BATCH_KMIX=1 the mixed molecules' tensor-core K of a batch
+    runs as one half-transform launch and one G GEMM launch over all of them:
+    the same arithmetic per molecule as their builds one by one (identical
+    energies and iteration counts), fewer launches."""
     paths = _molecules(tmp_path)[:6]
     out = {}
     for mode in ("0", "1"):

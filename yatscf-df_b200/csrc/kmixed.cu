@@ -1202,11 +1202,11 @@ static void kmix_prepare(KMix *k, const double *Cocc, const double *S, cudaStrea
     g_launches += 3;
 }
 
-// K += sym(sum over splits of G) (the first build of a solve sets K).
-static void kmix_finish(KMix *k, double *K, cudaStream_t s)
+// K += sym(sum over the first nsplit splits of G) (the first build of a solve sets K).
+static void kmix_finish(KMix *k, double *K, cudaStream_t s, int nsplit)
 {
     const size_t nn = (size_t) k->nbf * k->nbf;
-    k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, k->ksplit, k->nbf, k->first ? 1 : 0, K);
+    k_kmix_reduce<<<(unsigned) ((nn + 255) / 256), 256, 0, s>>>(k->G, nsplit, k->nbf, k->first ? 1 : 0, K);
     g_launches++;
     k->first = false;
 }
@@ -1251,13 +1251,14 @@ int kmix_build(KMix *k, const double *Cocc, const double *S, double *K, cudaStre
     rc = launch_gemm(k, ga, s);
     if (rc) return rc;
     if (mark) mark(2);
-    kmix_finish(k, K, s);
+    kmix_finish(k, K, s, k->ksplit);
     return OK;
 }
 
 // ---------------------------------------------------------------- many molecules in one launch per kernel
 struct KMixBatch {
     std::vector<KMix *> ks;
+    std::vector<int> ksplit;           // the G GEMM's K splits of each molecule in the batch
     KMixDev *d_mols = nullptr;
     int *d_starts = nullptr;           // [2][nmol + 1]: half-transform items, G GEMM pair items
     std::vector<int> h_starts;
@@ -1294,13 +1295,16 @@ int kmix_batch_create(KMixBatch **out, KMix *const *ks, int n, cudaStream_t s)
         d.ha = half_args(k);
         d.ga.part = k->G;
         d.ga.nbf = k->nbf;
+        // the molecule's own K splits: its G sums round exactly as in its builds one by one
+        const int ksb = k->ksplit;
         d.ga.chunks_per_split = k->chunks_per_split;
         d.ga.total_chunks = k->total_chunks;
         d.ga.probe = 0;
         d.ga.wait_cycles = WAIT_CYCLES;
         d.bn = k->bn_half;
         d.mt = (k->nbf + PAIR_N - 1) / PAIR_N;
-        d.ksplit = k->ksplit;
+        d.ksplit = ksb;
+        b->ksplit.push_back(ksb);
         b->max_bn = std::max(b->max_bn, d.bn);
     }
     b->h_starts.assign(2 * (n + 1), 0);
@@ -1329,7 +1333,7 @@ int kmix_batch_build(KMixBatch *b, const int *active, const double *const *Cocc,
         const KMix *k = b->ks[m];
         const int mt = (k->nbf + PAIR_N - 1) / PAIR_N;
         hh[m + 1] = hh[m] + (active[m] ? k->nbf * ((k->naux + UM - 1) / UM) : 0);
-        hg[m + 1] = hg[m] + (active[m] ? mt * mt * k->ksplit : 0);
+        hg[m + 1] = hg[m] + (active[m] ? mt * mt * b->ksplit[m] : 0);
     }
     if (hh[n] == 0) return OK;
     for (int m = 0; m < n; m++)
@@ -1373,7 +1377,7 @@ int kmix_batch_build(KMixBatch *b, const int *active, const double *const *Cocc,
             return ERR_CUDA;
     }
     for (int m = 0; m < n; m++)
-        if (active[m]) kmix_finish(b->ks[m], K[m], s);
+        if (active[m]) kmix_finish(b->ks[m], K[m], s, b->ksplit[m]);
     return cuda_launch_rc("batched tensor-core exchange");
 }
 

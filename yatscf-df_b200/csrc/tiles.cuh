@@ -623,52 +623,16 @@ __device__ __forceinline__ void jt_rows(const BT *__restrict__ B, const int *__r
                                         const double *__restrict__ w, int naux, int r0, int r1,
                                         double *__restrict__ part_row)
 {
-    // RU rows' loads are issued together, and the next group's row indices and
-    // weights are fetched while this group's loads are in flight; the FMAs
-    // still run row by row, so every partial sum is formed in the same order.
-    constexpr int RU = 2;
     double acc[COLS];
 #pragma unroll
     for (int c = 0; c < COLS; c++) acc[c] = 0.0;
-    int un[RU];
-    double wn[RU];
+    for (int r = r0; r < r1; r++) {
+        const double wr = w[r];
+        const BT *row = B + (size_t) up_u[r] * naux;
 #pragma unroll
-    for (int q = 0; q < RU; q++) {
-        un[q] = r0 + q < r1 ? up_u[r0 + q] : -1;
-        wn[q] = r0 + q < r1 ? w[r0 + q] : 0.0;
-    }
-    for (int r = r0; r < r1; r += RU) {
-        int u[RU];
-        double wr[RU];
-#pragma unroll
-        for (int q = 0; q < RU; q++) {
-            u[q] = un[q];
-            wr[q] = wn[q];
-        }
-#pragma unroll
-        for (int q = 0; q < RU; q++) {
-            const int rr = r + RU + q;
-            un[q] = rr < r1 ? up_u[rr] : -1;
-            wn[q] = rr < r1 ? w[rr] : 0.0;
-        }
-        BT v[RU][COLS];
-#pragma unroll
-        for (int q = 0; q < RU; q++) {
-            const BT *row = B + (size_t) (u[q] < 0 ? 0 : u[q]) * naux;
-#pragma unroll
-            for (int c = 0; c < COLS; c++) {
-                const int p = threadIdx.x + c * JT_THREADS;
-                v[q][c] = (u[q] >= 0 && p < naux) ? __ldg(row + p) : (BT) 0;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < RU; q++) {
-            if (u[q] < 0) continue;
-#pragma unroll
-            for (int c = 0; c < COLS; c++) {
-                const int p = threadIdx.x + c * JT_THREADS;
-                if (p < naux) acc[c] = fma(wr[q], (double) v[q][c], acc[c]);
-            }
+        for (int c = 0; c < COLS; c++) {
+            int p = threadIdx.x + c * JT_THREADS;
+            if (p < naux) acc[c] = fma(wr, (double) __ldg(row + p), acc[c]);
         }
     }
 #pragma unroll
