@@ -145,3 +145,21 @@ def test_pair_blocks_reject_uncovered_elements():
         assert "UNSUPPORTED" in str(err).upper(), err
     else:
         raise AssertionError("an uncovered element must be rejected")
+
+
+def test_training_set_is_the_seeded_clusters_and_alkanes():
+    """The trainer's molecules are fixed by their seeds: water clusters from
+    seed 10000 on (4096 of them: seeds 10000-14095) and jittered alkanes from
+    seed 20000 on, the same geometries on every call."""
+    sys.path.insert(0, os.path.join(REPO, "yatscf-df_b200"))
+    import geometry
+    import guess_train
+    jobs = guess_train.training_jobs(3, 2)
+    assert [t for t, _ in jobs] == ["w10000", "w10001", "w10002", "a20000", "a20001"]
+    assert jobs[1][1] == geometry.water_cluster(10001)
+    again = guess_train.training_jobs(3, 2)
+    assert all(a == b for (_, a), (_, b) in zip(jobs, again))
+    for _, atoms in jobs[3:]:
+        el = [a[0] for a in atoms]
+        nc = el.count("C")
+        assert 2 <= nc <= 10 and el.count("H") == 2 * nc + 2

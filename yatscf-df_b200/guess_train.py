@@ -10,7 +10,15 @@ gives one training row per atom pair (TinySCF_guess_dataset). The five block
 networks are then trained on the GPU by the engine's own kernels
 (TinySCF_guess_train) and written to the weights file.
 
+Two ways to converge the training molecules:
+  * one by one, in --workers processes that share the GPU;
+  * --batched: in waves through the batched SCF (TinySCF_batch_do_SCF: one
+    launch per SCF phase over the whole wave), the autotuner off, so that set-up
+    is the engines' own work and no timing runs are made for each new size.
+    A wave grows until less than --reserve-gb of device memory is free.
+
     python guess_train.py --waters 512 --alkanes 96 --out guess_weights.bin
+    python guess_train.py --batched --waters 4096 --alkanes 256 --epochs 300 ...
 """
 import argparse
 import json
@@ -37,6 +45,14 @@ def jittered_alkane(seed):
     q /= np.linalg.norm(q)
     xyz = xyz @ geometry._rotation(q).T
     return [(a[0], float(r[0]), float(r[1]), float(r[2])) for a, r in zip(atoms, xyz)]
+
+
+def training_jobs(waters, alkanes):
+    """(tag, atoms) of the training molecules: water clusters of seeds 10000, ...,
+    10000 + waters - 1, then jittered alkanes of seeds 20000, ..., 20000 + alkanes - 1."""
+    jobs = [("w%d" % s, geometry.water_cluster(s)) for s in range(10000, 10000 + waters)]
+    jobs += [("a%d" % s, jittered_alkane(s)) for s in range(20000, 20000 + alkanes)]
+    return jobs
 
 
 def converge(atoms, bas, dfbas, tmpdir, tag, ene_tol=1e-8, guess=None, weights=None, kmode=None, fast=False):
@@ -103,6 +119,53 @@ def generate(jobs, bas, dfbas, workers):
     return feats, tgts, types, iters
 
 
+def generate_batched(jobs, bas, dfbas, reserve_gb, guess=tinyscf.GUESS_SAD_PROJECTED, ene_tol=1e-8, max_iter=100):
+    """Training rows for all jobs from the batched SCF (FP64 K, full eigensolves),
+    largest molecules first so that a wave holds molecules of similar size.
+    Returns (features, targets, types, iterations, waves, unconverged tags);
+    a molecule that used all max_iter iterations gives no rows."""
+    tinyscf.load_library()
+    tinyscf.set_autotune(False)
+    order = sorted(range(len(jobs)), key=lambda k: -len(jobs[k][1]))
+    feats, tgts, types, iters, unconverged = [], [], [], [], []
+    waves = 0
+    with tempfile.TemporaryDirectory() as td:
+        k = 0
+        while k < len(order):
+            wave = []
+            try:
+                while k < len(order):
+                    tag, atoms = jobs[order[k]]
+                    k += 1
+                    path = os.path.join(td, tag + ".xyz")
+                    geometry.write_xyz(path, atoms)
+                    e = tinyscf.TinySCF(bas, dfbas, path, max_iter)
+                    wave.append((tag, e))
+                    e.setup(guess=guess)
+                    e.s.ene_tol = ene_tol
+                    if tinyscf.device_memory()[0] < reserve_gb * 2 ** 30:
+                        break
+                b = tinyscf.TinySCFBatch([e for _, e in wave])
+                try:
+                    b.do_SCF()
+                finally:
+                    b.free()
+                waves += 1
+                for tag, e in wave:
+                    if e.s.iter >= max_iter:
+                        unconverged.append(tag)
+                        continue
+                    f, t, y = e.guess_dataset(e.mat("D_mat"))
+                    feats.append(f)
+                    tgts.append(t)
+                    types.append(y)
+                    iters.append(e.s.iter)
+            finally:
+                for _, e in wave:
+                    e.free()
+    return feats, tgts, types, iters, waves, unconverged
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--waters", type=int, default=512)
@@ -113,14 +176,22 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "guess_weights.bin"))
     ap.add_argument("--report", default=None, help="JSON summary path")
     ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--batched", action="store_true", help="converge the molecules in waves of the batched SCF")
+    ap.add_argument("--reserve-gb", type=float, default=40.0,
+                    help="--batched: close a wave when less than this much device memory is free")
     ap.add_argument("--bas", required=True)
     ap.add_argument("--dfbas", required=True)
     args = ap.parse_args()
 
     t0 = time.perf_counter()
-    jobs = [("w%d" % s, geometry.water_cluster(s)) for s in range(10000, 10000 + args.waters)]
-    jobs += [("a%d" % s, jittered_alkane(s)) for s in range(20000, 20000 + args.alkanes)]
-    feats, tgts, types, iters = generate(jobs, args.bas, args.dfbas, args.workers)
+    jobs = training_jobs(args.waters, args.alkanes)
+    extra = {}
+    if args.batched:
+        feats, tgts, types, iters, waves, unconverged = generate_batched(jobs, args.bas, args.dfbas, args.reserve_gb)
+        extra = dict(mode="batched", waves=waves, unconverged=unconverged, autotune="off")
+    else:
+        feats, tgts, types, iters = generate(jobs, args.bas, args.dfbas, args.workers)
+        extra = dict(mode="one by one", workers=args.workers)
     stats = dict(molecules=len(jobs), pairs=sum(len(y) for y in types), iters=iters)
     gen_s = time.perf_counter() - t0
     F = np.concatenate(feats)
@@ -134,7 +205,7 @@ def main():
                pairs_per_type=[int((Y == k).sum()) for k in range(5)],
                mean_iterations=float(np.mean(stats["iters"])), data_generation_s=gen_s, training_s=train_s,
                final_loss_per_type=[float(v) for v in loss], weights=os.path.basename(args.out),
-               epochs=args.epochs, batch=args.batch, lr=args.lr, workers=args.workers)
+               epochs=args.epochs, batch=args.batch, lr=args.lr, **extra)
     print(json.dumps(rep))
     if args.report:
         with open(args.report, "w") as f:
