@@ -2,6 +2,7 @@
 // the reference's replacement policy (DIIS.c:12-123) kept entirely on the
 // device, and the density from the orthogonalised Fock eigenvectors
 // (build_density.c:37-69).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -79,23 +80,62 @@ __global__ void k_copy_to_slot(const double *src, double *slots, const DiisState
     if (i < nn) slots[(size_t) st->idx * nn + i] = src[i];
 }
 
-// dots[j] = <R_idx, R_j> for j < len; one block per j.
-__global__ void k_diis_dots(const double *R, DiisState *st, size_t nn)
+// DIIS.c:75-81: store the new residual in slot idx and form
+// dots[j] = <R_idx, R_j> for j < len, over the whole grid: block b takes the
+// elements b * 256 + t + k * 256 * gridDim, reads the new residual once for
+// every j and writes its sums to part[b][j]; k_diis_dots_sum adds the parts in
+// block order, so the dots do not depend on timing.
+constexpr int DOT_THREADS = 256;
+
+__global__ void __launch_bounds__(DOT_THREADS) k_diis_slot_dots(const double *src, double *R, DiisState *st, size_t nn)
 {
-    const int j = blockIdx.x;
-    if (j >= st->len) return;
-    const double *a = R + (size_t) st->idx * nn, *b = R + (size_t) j * nn;
-    double s = 0.0;
-    for (size_t i = threadIdx.x; i < nn; i += blockDim.x) s = fma(a[i], b[i], s);
-    __shared__ double sh[32];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffff, s, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffff, s, o);
-        if (threadIdx.x == 0) st->dots[j] = s;
+    const int len = st->len, idx = st->idx;
+    double *slot = R + (size_t) idx * nn;
+    double s[MAXDIIS];
+#pragma unroll
+    for (int j = 0; j < MAXDIIS; j++) s[j] = 0.0;
+    const size_t step = (size_t) gridDim.x * DOT_THREADS;
+    for (size_t i = (size_t) blockIdx.x * DOT_THREADS + threadIdx.x; i < nn; i += step) {
+        const double a = src[i];
+        slot[i] = a;
+#pragma unroll
+        for (int j = 0; j < MAXDIIS; j++)
+            if (j < len) s[j] = fma(a, j == idx ? a : R[(size_t) j * nn + i], s[j]);
     }
+    __shared__ double sh[MAXDIIS][DOT_THREADS / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < MAXDIIS; j++) {
+        double v = s[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffff, v, o);
+        if (lane == 0) sh[j][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < MAXDIIS) {
+        double v = 0.0;
+        for (int w = 0; w < DOT_THREADS / 32; w++) v += sh[threadIdx.x][w];
+        st->part[blockIdx.x * MAXDIIS + threadIdx.x] = v;
+    }
+}
+
+// One warp per j: dots[j] = sum over the blocks' parts, in a fixed order.
+__global__ void __launch_bounds__(32 * MAXDIIS) k_diis_dots_sum(DiisState *st, int nblocks)
+{
+    const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (j >= st->len) return;   // uniform per warp
+    double v = 0.0;
+    for (int b = lane; b < nblocks; b += 32) v += st->part[b * MAXDIIS + j];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffff, v, o);
+    if (lane == 0) st->dots[j] = v;
+}
+
+// The residual's slot and dots: two launches.
+void diis_slot_dots(const double *src, double *R, DiisState *st, size_t nn, cudaStream_t s)
+{
+    const size_t need = (nn + DOT_THREADS - 1) / DOT_THREADS;
+    const int nblk = (int) std::max<size_t>(1, std::min<size_t>(need, std::min(2 * num_sms(), DIIS_DOT_BLOCKS)));
+    k_diis_slot_dots<<<nblk, DOT_THREADS, 0, s>>>(src, R, st, nn);
+    k_diis_dots_sum<<<1, 32 * MAXDIIS, 0, s>>>(st, nblk);
 }
 
 // DIIS.c:76-110: update B, track the historically largest residual, and
@@ -279,8 +319,7 @@ void diis_step(DiisState *st, int max_diis, const double *d_F, const double *d_D
     k_antisym<<<nb, 256, 0, s>>>(d_tmp2, d_tmp, n);                          // FDS - (FDS)^T
     dgemm(true, false, n, n, n, 1.0, d_X, n, d_tmp, n, 0.0, d_tmp2, n, s);   // X^T (.)
     dgemm(false, false, n, n, n, 1.0, d_tmp2, n, d_X, n, 0.0, d_tmp, n, s);  // (.) X
-    k_copy_to_slot<<<nb, 256, 0, s>>>(d_tmp, d_R, st, nn);
-    k_diis_dots<<<MAXDIIS, 1024, 0, s>>>(d_R, st, nn);
+    diis_slot_dots(d_tmp, d_R, st, nn, s);
     xtfx(d_X, d_F, d_tmp2, d_tmp, n, s);                                     // X^T F X
     k_copy_to_slot<<<nb, 256, 0, s>>>(d_tmp2, d_F0, st, nn);
     k_diis_solve<<<1, 32, 0, s>>>(st);
@@ -316,8 +355,7 @@ void diis_step_cocc(DiisState *st, int max_diis, const double *d_F, const double
     dgemm(true, false, n, o2, n, 1.0, d_X, n, d_tmp, o2, 0.0, d_tmp2, o2, s);     // [A | B] = X^T [P | Q]
     k_swap_neg<<<(unsigned) (((size_t) n * o2 + 255) / 256), 256, 0, s>>>(d_tmp2, d_tmp, n, o);   // [B | -A]
     dgemm(false, true, n, n, o2, 1.0, d_tmp2, o2, d_tmp, o2, 0.0, d_Fout, n, s);  // A B^T - B A^T
-    k_copy_to_slot<<<nb, 256, 0, s>>>(d_Fout, d_R, st, nn);
-    k_diis_dots<<<MAXDIIS, 1024, 0, s>>>(d_R, st, nn);
+    diis_slot_dots(d_Fout, d_R, st, nn, s);
     xtfx(d_X, d_F, d_tmp2, d_tmp, n, s);                                           // X^T F X
     k_copy_to_slot<<<nb, 256, 0, s>>>(d_tmp2, d_F0, st, nn);
     k_diis_solve<<<1, 32, 0, s>>>(st);

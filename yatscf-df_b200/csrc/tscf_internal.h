@@ -257,6 +257,7 @@ int  oz_error_flag();
 void oz_info(const OzSyrk *o, int info[6]);
 
 // ---------------------------------------------------------------- DIIS / density (scf.cu)
+constexpr int DIIS_DOT_BLOCKS = 512;      // most blocks of the DIIS residual dots
 struct DiisState {            // device-resident DIIS bookkeeping (DIIS.c:12-123)
     int len;
     int bmax_id;
@@ -266,6 +267,7 @@ struct DiisState {            // device-resident DIIS bookkeeping (DIIS.c:12-123
     double B[(MAXDIIS + 1) * (MAXDIIS + 1)];
     double coef[MAXDIIS + 1];
     double dots[MAXDIIS];
+    double part[DIIS_DOT_BLOCKS * MAXDIIS];   // per-block partial sums of the dots
 };
 void diis_init(DiisState *d_st, cudaStream_t s);
 void diis_step(DiisState *d_st, int max_diis, const double *d_F, const double *d_D, const double *d_S,
