@@ -43,7 +43,8 @@ __global__ void __launch_bounds__(JT_THREADS) kb_j_tpart(const MolDev *mols, con
     const int nblk = wl.start[mol + 1] - wl.start[mol];
     const int rows = (m.nup + nblk - 1) / nblk;
     const int r0 = li * rows, r1 = min(m.nup, r0 + rows);
-    if (use32 && m.B32) jt_rows<float>(m.B32, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
+    if (use32 && jt_pairs_ok(m.B32, m.naux)) jt_rows_f2(m.B32, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
+    else if (use32 && m.B32) jt_rows<float>(m.B32, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
     else jt_rows<double>(m.B, m.up_u, m.Jw, m.naux, r0, r1, m.Jpart + (size_t) li * m.naux);
 }
 
@@ -61,9 +62,7 @@ __global__ void kb_j_treduce(const MolDev *mols, const int *active, WorkList wl)
     BATCH_ITEM(wl)
     const int p = li * blockDim.x + threadIdx.x;
     if (p >= m.naux) return;
-    double s = 0.0;
-    for (int b = 0; b < m.jblk; b++) s += m.Jpart[(size_t) b * m.naux + p];
-    m.Jt[p] = s;
+    m.Jt[p] = jt_reduce_col(m.Jpart, m.jblk, m.naux, p);
 }
 
 // 8 warps, 8 upper pairs per warp per item

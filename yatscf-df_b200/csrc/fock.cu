@@ -37,81 +37,22 @@ __global__ void __launch_bounds__(JT_THREADS) k_j_tpart(const BT *__restrict__ B
     jt_rows<BT, COLS>(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
 }
 
-// The FP32 copy of B with an even naux: each thread takes column pairs
-// (float2 loads) and two rows per step, so as many bytes are in flight as with
-// the FP64 rows; every column is still summed row by row, so the partial sums
-// equal jt_rows<float, 8>'s bit for bit. Needs naux <= 8 * JT_THREADS.
+// The FP32 copy of B with an even naux (jt_rows_f2: float2 column pairs, two
+// rows per step, the same sums as jt_rows<float> bit for bit).
 __global__ void __launch_bounds__(JT_THREADS) k_j_tpart_f2(const float *__restrict__ B, const int *__restrict__ up_u,
                                                            const double *__restrict__ w, int nup, int naux,
                                                            int rows_per_blk, double *__restrict__ part)
 {
-    constexpr int PAIRS = 4;   // 4 * JT_THREADS column pairs
     const int r0 = blockIdx.x * rows_per_blk, r1 = min(nup, r0 + rows_per_blk);
-    const int npair = naux >> 1;
-    double ax[PAIRS], ay[PAIRS];
-#pragma unroll
-    for (int c = 0; c < PAIRS; c++) ax[c] = ay[c] = 0.0;
-    int r = r0;
-    for (; r + 1 < r1; r += 2) {
-        const double w0 = w[r], w1 = w[r + 1];
-        const float2 *ra = (const float2 *) (B + (size_t) up_u[r] * naux);
-        const float2 *rb = (const float2 *) (B + (size_t) up_u[r + 1] * naux);
-        float2 va[PAIRS], vb[PAIRS];
-#pragma unroll
-        for (int c = 0; c < PAIRS; c++) {
-            const int q = threadIdx.x + c * JT_THREADS;
-            va[c] = q < npair ? __ldg(ra + q) : make_float2(0.f, 0.f);
-            vb[c] = q < npair ? __ldg(rb + q) : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int c = 0; c < PAIRS; c++) {
-            ax[c] = fma(w0, (double) va[c].x, ax[c]);
-            ay[c] = fma(w0, (double) va[c].y, ay[c]);
-            ax[c] = fma(w1, (double) vb[c].x, ax[c]);
-            ay[c] = fma(w1, (double) vb[c].y, ay[c]);
-        }
-    }
-    if (r < r1) {
-        const double w0 = w[r];
-        const float2 *ra = (const float2 *) (B + (size_t) up_u[r] * naux);
-#pragma unroll
-        for (int c = 0; c < PAIRS; c++) {
-            const int q = threadIdx.x + c * JT_THREADS;
-            if (q < npair) {
-                const float2 v = __ldg(ra + q);
-                ax[c] = fma(w0, (double) v.x, ax[c]);
-                ay[c] = fma(w0, (double) v.y, ay[c]);
-            }
-        }
-    }
-    double *prow = part + (size_t) blockIdx.x * naux;
-#pragma unroll
-    for (int c = 0; c < PAIRS; c++) {
-        const int q = threadIdx.x + c * JT_THREADS;
-        if (q < npair) {
-            prow[2 * q] = ax[c];
-            prow[2 * q + 1] = ay[c];
-        }
-    }
+    jt_rows_f2(B, up_u, w, naux, r0, r1, part + (size_t) blockIdx.x * naux);
 }
 
-// t(P) = sum over the blocks' partial rows, in block order; the loads of 16
-// blocks are issued before their additions.
+// t(P) = sum over the blocks' partial rows, in block order (jt_reduce_col).
 __global__ void k_j_treduce(const double *part, int nblk, int naux, double *t)
 {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= naux) return;
-    double s = 0.0;
-    int b = 0;
-    for (; b + 16 <= nblk; b += 16) {
-        double v[16];
-#pragma unroll
-        for (int u = 0; u < 16; u++) v[u] = part[(size_t) (b + u) * naux + p];
-#pragma unroll
-        for (int u = 0; u < 16; u++) s += v[u];
-    }
-    for (; b < nblk; b++) s += part[(size_t) b * naux + p];
-    t[p] = s;
+    t[p] = jt_reduce_col(part, nblk, naux, p);
 }
 
 template <typename BT>
@@ -151,8 +92,7 @@ static void build_J_t(const FockPlan &p, const BT *B, const double *d_D, double 
     g_launches += 4;
     k_j_weights<<<(p.nup + 255) / 256, 256, 0, s>>>(p.up_i, p.up_j, d_D, d_w, p.nup, p.nbf);
     int rows_per_blk = (p.nup + nblk - 1) / nblk;
-    const bool pairs = sizeof(BT) == sizeof(float) && p.naux % 2 == 0 && ((uintptr_t) B & 7) == 0;
-    if (pairs && p.naux <= 8 * JT_THREADS)
+    if (sizeof(BT) == sizeof(float) && jt_pairs_ok((const float *) B, p.naux))
         k_j_tpart_f2<<<nblk, JT_THREADS, 0, s>>>((const float *) B, p.up_u, d_w, p.nup, p.naux, rows_per_blk,
                                                  d_part);
     else if (p.naux <= 8 * JT_THREADS)

@@ -642,6 +642,85 @@ __device__ __forceinline__ void jt_rows(const BT *__restrict__ B, const int *__r
     }
 }
 
+// The FP32 copy with an even naux <= 8 * JT_THREADS and rows 8-byte aligned:
+// each thread takes column pairs (float2 loads) and two rows per step, so as
+// many bytes are in flight as with FP64 rows; every column is still summed
+// row by row, so part_row equals jt_rows<float>'s bit for bit.
+__device__ __forceinline__ void jt_rows_f2(const float *__restrict__ B, const int *__restrict__ up_u,
+                                           const double *__restrict__ w, int naux, int r0, int r1,
+                                           double *__restrict__ part_row)
+{
+    constexpr int PAIRS = 4;   // 4 * JT_THREADS column pairs
+    const int npair = naux >> 1;
+    double ax[PAIRS], ay[PAIRS];
+#pragma unroll
+    for (int c = 0; c < PAIRS; c++) ax[c] = ay[c] = 0.0;
+    int r = r0;
+    for (; r + 1 < r1; r += 2) {
+        const double w0 = w[r], w1 = w[r + 1];
+        const float2 *ra = (const float2 *) (B + (size_t) up_u[r] * naux);
+        const float2 *rb = (const float2 *) (B + (size_t) up_u[r + 1] * naux);
+        float2 va[PAIRS], vb[PAIRS];
+#pragma unroll
+        for (int c = 0; c < PAIRS; c++) {
+            const int q = threadIdx.x + c * JT_THREADS;
+            va[c] = q < npair ? __ldg(ra + q) : make_float2(0.f, 0.f);
+            vb[c] = q < npair ? __ldg(rb + q) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int c = 0; c < PAIRS; c++) {
+            ax[c] = fma(w0, (double) va[c].x, ax[c]);
+            ay[c] = fma(w0, (double) va[c].y, ay[c]);
+            ax[c] = fma(w1, (double) vb[c].x, ax[c]);
+            ay[c] = fma(w1, (double) vb[c].y, ay[c]);
+        }
+    }
+    if (r < r1) {
+        const double w0 = w[r];
+        const float2 *ra = (const float2 *) (B + (size_t) up_u[r] * naux);
+#pragma unroll
+        for (int c = 0; c < PAIRS; c++) {
+            const int q = threadIdx.x + c * JT_THREADS;
+            if (q < npair) {
+                const float2 v = __ldg(ra + q);
+                ax[c] = fma(w0, (double) v.x, ax[c]);
+                ay[c] = fma(w0, (double) v.y, ay[c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < PAIRS; c++) {
+        const int q = threadIdx.x + c * JT_THREADS;
+        if (q < npair) {
+            part_row[2 * q] = ax[c];
+            part_row[2 * q + 1] = ay[c];
+        }
+    }
+}
+
+// Whether jt_rows_f2 applies to an FP32 copy B with naux columns.
+__host__ __device__ __forceinline__ bool jt_pairs_ok(const float *B, int naux)
+{
+    return B != nullptr && naux % 2 == 0 && naux <= 8 * JT_THREADS && ((uintptr_t) B & 7) == 0;
+}
+
+// t(P) = sum_b part[b][p] in block order for one column p; the loads of 16
+// blocks are issued before their additions.
+__device__ __forceinline__ double jt_reduce_col(const double *part, int nblk, int naux, int p)
+{
+    double s = 0.0;
+    int b = 0;
+    for (; b + 16 <= nblk; b += 16) {
+        double v[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) v[u] = part[(size_t) (b + u) * naux + p];
+#pragma unroll
+        for (int u = 0; u < 16; u++) s += v[u];
+    }
+    for (; b < nblk; b++) s += part[(size_t) b * naux + p];
+    return s;
+}
+
 // ---- F = H + 2J - K and the partial energy sum D (F + H) of one strided range
 __device__ __forceinline__ double fock_energy_range(const double *H, const double *J, const double *K,
                                                     const double *D, double *F, size_t beg, size_t n, size_t stride)
