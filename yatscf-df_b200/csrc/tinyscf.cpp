@@ -92,6 +92,7 @@ int parse_xyz(const char *fn, Molecule &m)
         if (nsc < 1 || !isalpha((unsigned char) str[0])) continue;
         int e = (strlen(str) <= 2) ? elem_index(str) : -1;
         if (e < 0 || nsc < 4) { rc = ERR_INPUT; break; }
+        if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(z)) { rc = ERR_INPUT; break; }
         m.eid.push_back(e);
         m.xyz.push_back(x * A2BOHR);
         m.xyz.push_back(y * A2BOHR);
@@ -106,7 +107,9 @@ int parse_xyz(const char *fn, Molecule &m)
         for (int b = a + 1; b < m.natoms; b++) {
             double dx = m.xyz[3 * a] - m.xyz[3 * b], dy = m.xyz[3 * a + 1] - m.xyz[3 * b + 1],
                    dz = m.xyz[3 * a + 2] - m.xyz[3 * b + 2];
-            m.enuc += (m.eid[a] + 1.0) * (m.eid[b] + 1.0) / sqrt(dx * dx + dy * dy + dz * dz);
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(r > 1e-6)) return ERR_INPUT;   // coincident nuclei: infinite repulsion
+            m.enuc += (m.eid[a] + 1.0) * (m.eid[b] + 1.0) / r;
         }
     return OK;
 }
@@ -147,8 +150,16 @@ int parse_gbs(const char *fn, BasisDef &b)
                 for (int p = 0; p < nexp; p++) {
                     const std::string &R = lines[i + p];
                     if (R.empty() || R[0] == '*' || isalpha((unsigned char) R[0])) return ERR_INPUT;
+                    // an exponent and ns finite coefficients; Fortran 'D' exponents
+                    // (1.0D+01) read as 'E'
+                    std::string Rn = R;
+                    for (char &c : Rn)
+                        if (c == 'D' || c == 'd') c = 'E';
                     double v[4] = {0, 0, 0, 0};
-                    sscanf(R.c_str(), "%lf %lf %lf %lf", &v[0], &v[1], &v[2], &v[3]);
+                    const int got = sscanf(Rn.c_str(), "%lf %lf %lf %lf", &v[0], &v[1], &v[2], &v[3]);
+                    if (got < 1 + ns || !std::isfinite(v[0]) || !(v[0] > 0.0)) return ERR_INPUT;
+                    for (int k = 0; k < ns; k++)
+                        if (!std::isfinite(v[1 + k])) return ERR_INPUT;
                     ex[p] = v[0];
                     for (int k = 0; k < 3; k++) cc[k][p] = v[1 + k];
                 }
