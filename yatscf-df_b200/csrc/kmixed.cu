@@ -994,7 +994,7 @@ int kmix_create(KMix **out, const FockPlan &p, const int *h_displs, cudaStream_t
     k->total_chunks = (int) (k->Qp / BK);
     // Split count: at least 4 CTAs per SM, at most MAX_SEGS segments per split
     // (their FP32 register sums are written once, as FP64, at the end), and
-    // the CTA count rounded up to whole waves of 148 when that costs little.
+    // the CTA count rounded up to whole waves of the SM count when that costs little.
     const int mt = (p.nbf + UM - 1) / UM;
     const int tiles = mt * mt;
     const int nsm = num_sms();

@@ -257,18 +257,19 @@ void dgemm_untuned(bool ta, bool tb, int m, int n, int k, double alpha, const do
     dgemm_variant(v, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
 
+// SM count of the current device (cached for the first 64 ordinals).
 int num_sms()
 {
-    static int cached[64] = {};
+    static std::atomic<int> cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return 148;
-    if (!cached[dev]) {
-        int v = 0;
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-        cached[dev] = v > 0 ? v : 1;
-    }
-    return cached[dev];
+    const bool cacheable = dev >= 0 && dev < 64;
+    if (cacheable && cached[dev].load(std::memory_order_relaxed) > 0) return cached[dev].load(std::memory_order_relaxed);
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    if (v <= 0) v = 1;
+    if (cacheable) cached[dev].store(v, std::memory_order_relaxed);
+    return v;
 }
 
 int cuda_launch_rc(const char *what)
