@@ -16,6 +16,8 @@
 #include <string>
 #include <vector>
 
+#include <sys/mman.h>
+
 #include "TinySCF.h"
 #include "DIIS.h"
 #include "build_DF_tensor.h"
@@ -481,12 +483,43 @@ DevShells shells_view(const DevArrays &d, int nsh)
     return v;
 }
 
+// Host mirrors: 64-byte aligned and zero-filled. Blocks of 128 KB and more
+// are fresh anonymous mappings, which are zero without being touched
+// (transparent huge pages asked for, so the first write of a large one faults
+// 2 MB at a time): an nbf x nbf mirror costs page faults only when a call
+// first fills it. Smaller blocks come from the heap. A 64-byte header records
+// which, for afree.
+constexpr size_t AHDR = 64, ABIG = (size_t) 128 << 10;
+constexpr unsigned long long AMAGIC_HEAP = 0x6865617074736366ULL, AMAGIC_MAP = 0x6d61707074736366ULL;
+
 void *amalloc(size_t bytes)
 {
-    void *p = nullptr;
-    if (posix_memalign(&p, 64, bytes ? bytes : 64)) return nullptr;
-    memset(p, 0, bytes ? bytes : 64);
-    return p;
+    if (bytes == 0) bytes = 64;
+    const size_t len = bytes + AHDR;
+    unsigned long long *h = nullptr;
+    if (bytes >= ABIG) {
+        void *b = mmap(nullptr, len, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+        if (b == MAP_FAILED) return nullptr;
+        madvise(b, len, MADV_HUGEPAGE);   // advice only: ignored where huge pages are off
+        h = (unsigned long long *) b;
+        h[0] = AMAGIC_MAP;
+    } else {
+        void *b = nullptr;
+        if (posix_memalign(&b, 64, len)) return nullptr;
+        memset(b, 0, len);
+        h = (unsigned long long *) b;
+        h[0] = AMAGIC_HEAP;
+    }
+    h[1] = len;
+    return (char *) h + AHDR;
+}
+
+void afree(void *p)
+{
+    if (!p) return;
+    unsigned long long *h = (unsigned long long *) ((char *) p - AHDR);
+    if (h[0] == AMAGIC_MAP) munmap(h, h[1]);
+    else free(h);
 }
 
 #define RC(x)                    \
@@ -1565,7 +1598,7 @@ void free_impl(TinySCF_t t)
                   t->bf_pair_j, t->bf_pair_diag, t->bf_mask_displs, t->shell_bf_sind, t->shell_bf_num,
                   t->df_shell_bf_sind, t->df_shell_bf_num, t->Hcore_mat, t->S_mat, t->F_mat, t->D_mat, t->J_mat,
                   t->K_mat, t->X_mat, t->tmp_mat, t->Cocc_mat, t->eigval, t->ev_idx};
-    for (void *p : hp) free(p);
+    for (void *p : hp) afree(p);
 }
 
 void die(const char *fn, int rc)
