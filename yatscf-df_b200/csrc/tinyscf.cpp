@@ -13,6 +13,7 @@
 #include <cstring>
 #include <ctime>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -487,39 +488,43 @@ DevShells shells_view(const DevArrays &d, int nsh)
 // are fresh anonymous mappings, which are zero without being touched
 // (transparent huge pages asked for, so the first write of a large one faults
 // 2 MB at a time): an nbf x nbf mirror costs page faults only when a call
-// first fills it. Smaller blocks come from the heap. A 64-byte header records
-// which, for afree.
-constexpr size_t AHDR = 64, ABIG = (size_t) 128 << 10;
-constexpr unsigned long long AMAGIC_HEAP = 0x6865617074736366ULL, AMAGIC_MAP = 0x6d61707074736366ULL;
+// first fills it. Smaller blocks come from the heap. afree tells the two apart
+// by a registry of the mappings (any other pointer goes to free()).
+constexpr size_t ABIG = (size_t) 128 << 10;
+std::mutex g_amap_mu;
+std::map<void *, size_t> g_amaps;
 
 void *amalloc(size_t bytes)
 {
     if (bytes == 0) bytes = 64;
-    const size_t len = bytes + AHDR;
-    unsigned long long *h = nullptr;
     if (bytes >= ABIG) {
-        void *b = mmap(nullptr, len, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+        void *b = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
         if (b == MAP_FAILED) return nullptr;
-        madvise(b, len, MADV_HUGEPAGE);   // advice only: ignored where huge pages are off
-        h = (unsigned long long *) b;
-        h[0] = AMAGIC_MAP;
-    } else {
-        void *b = nullptr;
-        if (posix_memalign(&b, 64, len)) return nullptr;
-        memset(b, 0, len);
-        h = (unsigned long long *) b;
-        h[0] = AMAGIC_HEAP;
+        madvise(b, bytes, MADV_HUGEPAGE);   // advice only: ignored where huge pages are off
+        std::lock_guard<std::mutex> lk(g_amap_mu);
+        g_amaps[b] = bytes;
+        return b;
     }
-    h[1] = len;
-    return (char *) h + AHDR;
+    void *b = nullptr;
+    if (posix_memalign(&b, 64, bytes)) return nullptr;
+    memset(b, 0, bytes);
+    return b;
 }
 
 void afree(void *p)
 {
     if (!p) return;
-    unsigned long long *h = (unsigned long long *) ((char *) p - AHDR);
-    if (h[0] == AMAGIC_MAP) munmap(h, h[1]);
-    else free(h);
+    size_t len = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_amap_mu);
+        auto it = g_amaps.find(p);
+        if (it != g_amaps.end()) {
+            len = it->second;
+            g_amaps.erase(it);
+        }
+    }
+    if (len) munmap(p, len);
+    else free(p);
 }
 
 #define RC(x)                    \
