@@ -491,8 +491,19 @@ DevShells shells_view(const DevArrays &d, int nsh)
 // first fills it. Smaller blocks come from the heap. afree tells the two apart
 // by a registry of the mappings (any other pointer goes to free()).
 constexpr size_t ABIG = (size_t) 128 << 10;
-std::mutex g_amap_mu;
-std::map<void *, size_t> g_amaps;
+
+// The registry is never destroyed, so engines freed while the process exits still find it.
+std::map<void *, size_t> &amaps()
+{
+    static auto *m = new std::map<void *, size_t>();
+    return *m;
+}
+
+std::mutex &amaps_mu()
+{
+    static auto *mu = new std::mutex();
+    return *mu;
+}
 
 void *amalloc(size_t bytes)
 {
@@ -501,8 +512,8 @@ void *amalloc(size_t bytes)
         void *b = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
         if (b == MAP_FAILED) return nullptr;
         madvise(b, bytes, MADV_HUGEPAGE);   // advice only: ignored where huge pages are off
-        std::lock_guard<std::mutex> lk(g_amap_mu);
-        g_amaps[b] = bytes;
+        std::lock_guard<std::mutex> lk(amaps_mu());
+        amaps()[b] = bytes;
         return b;
     }
     void *b = nullptr;
@@ -516,11 +527,11 @@ void afree(void *p)
     if (!p) return;
     size_t len = 0;
     {
-        std::lock_guard<std::mutex> lk(g_amap_mu);
-        auto it = g_amaps.find(p);
-        if (it != g_amaps.end()) {
+        std::lock_guard<std::mutex> lk(amaps_mu());
+        auto it = amaps().find(p);
+        if (it != amaps().end()) {
             len = it->second;
-            g_amaps.erase(it);
+            amaps().erase(it);
         }
     }
     if (len) munmap(p, len);
