@@ -5,6 +5,7 @@ import os
 import sys
 
 import numpy as np
+import pytest
 
 from conftest import REPO
 
@@ -163,3 +164,69 @@ def test_training_set_is_the_seeded_clusters_and_alkanes():
         el = [a[0] for a in atoms]
         nc = el.count("C")
         assert 2 <= nc <= 10 and el.count("H") == 2 * nc + 2
+
+
+def test_batched_generation_waves_with_fake_engines(monkeypatch, tmp_path):
+    """guess_train.generate_batched on fake engines (host logic only): waves
+    close when free memory drops below the reserve, largest molecules first,
+    every engine is freed, unconverged molecules give no rows, and a failed
+    set-up frees the engines of its wave."""
+    sys.path.insert(0, os.path.join(REPO, "yatscf-df_b200"))
+    import guess_train
+    import tinyscf
+
+    class S:
+        def __init__(self):
+            self.ene_tol, self.iter = 0.0, 0
+
+    created, freed, waves = [], [], []
+
+    class FakeEngine:
+        def __init__(self, bas, dfbas, path, max_iter):
+            self.path, self.max_iter, self.s = path, max_iter, S()
+            created.append(self)
+
+        def setup(self, guess=None):
+            if "bad" in self.path:
+                raise tinyscf.TinySCFError("setup")
+
+        def mat(self, name):
+            return np.zeros((2, 2))
+
+        def guess_dataset(self, D):
+            return np.ones((3, 4), np.float32), np.ones((3, 5), np.float32), np.zeros(3, np.int32)
+
+        def free(self):
+            freed.append(self)
+
+    class FakeBatch:
+        def __init__(self, engines):
+            waves.append([len(open(e.path).read().splitlines()) for e in engines])
+            for e in engines:
+                e.s.iter = e.max_iter if "stuck" in e.path else 7
+
+        def do_SCF(self):
+            pass
+
+        def free(self):
+            pass
+
+    free_mem = iter([50, 30, 50, 50, 30, 50, 50, 50] * 4)
+    monkeypatch.setattr(tinyscf, "TinySCF", FakeEngine)
+    monkeypatch.setattr(tinyscf, "TinySCFBatch", FakeBatch)
+    monkeypatch.setattr(tinyscf, "load_library", lambda: None)
+    monkeypatch.setattr(tinyscf, "set_autotune", lambda on: None)
+    monkeypatch.setattr(tinyscf, "device_memory", lambda device=0: (next(free_mem) * 2 ** 30, 0))
+    atoms = lambda n: [("H", 0.0, 0.0, float(k)) for k in range(n)]
+    jobs = [("a", atoms(2)), ("stuck", atoms(5)), ("c", atoms(3)), ("d", atoms(4)), ("e", atoms(1))]
+    f, t, y, iters, nw, unconv = guess_train.generate_batched(jobs, "b", "d", reserve_gb=40.0)
+    assert nw == len(waves) == 2
+    sizes = [n - 2 for w in waves for n in w]          # xyz lines minus the two header lines
+    assert sizes == sorted(sizes, reverse=True)
+    assert unconv == ["stuck"] and len(f) == len(iters) == 4 and all(i == 7 for i in iters)
+    assert len(freed) == len(created) == 5
+
+    created.clear(), freed.clear()
+    with pytest.raises(tinyscf.TinySCFError):
+        guess_train.generate_batched([("ok", atoms(3)), ("bad", atoms(2))], "b", "d", reserve_gb=0.0)
+    assert len(freed) == len(created) == 2
