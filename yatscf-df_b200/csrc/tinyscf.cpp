@@ -1584,22 +1584,44 @@ int scf_impl(TinySCF_t t)
     return sync_host_impl(t);
 }
 
+// Host wall-clock seconds (for the release breakdown of TINYSCF_VERBOSE >= 2).
+static double wall_s()
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
 void free_impl(TinySCF_t t)
 {
+    // with verbose >= 2, the wall time of each release step (ms)
+    const bool report = t->verbose >= 2;
+    double tl = wall_s(), ms[8] = {};
+    auto lap = [&](int k) {
+        const double now = wall_s();
+        ms[k] += 1e3 * (now - tl);
+        tl = now;
+    };
     Engine *e = E_(t);
     if (e) {
         if (e->s) cudaStreamSynchronize(e->s);
+        lap(0);
         graph_release(e);
         if (e->s_body) cudaStreamDestroy(e->s_body);
+        lap(1);
         if (e->h_rctl) cudaFreeHost(e->h_rctl);
         if (e->h_E) cudaFreeHost(e->h_E);
+        lap(2);
         guessnet_free(e->gnet);
+        lap(3);
         eig_destroy(e->eig);
         kmix_destroy(e->kmix);
         oz_destroy(e->oz);
+        lap(4);
         for (void *p : e->allocs) dev_free(p, e->s);
         e->allocs.clear();
         if (e->s) cudaStreamSynchronize(e->s);
+        lap(5);
         if (e->s) {
             for (int k = 0; k < TINYSCF_T_COUNT; k++) {
                 cudaEventDestroy(e->ev0[k]);
@@ -1609,12 +1631,18 @@ void free_impl(TinySCF_t t)
         }
         delete e;
         t->dev = nullptr;
+        lap(6);
     }
     void *hp[] = {t->sp_scrval, t->bf_pair_scrval, t->df_sp_scrval, t->uniq_sp_lid, t->uniq_sp_rid, t->bf_pair_mask,
                   t->bf_pair_j, t->bf_pair_diag, t->bf_mask_displs, t->shell_bf_sind, t->shell_bf_num,
                   t->df_shell_bf_sind, t->df_shell_bf_num, t->Hcore_mat, t->S_mat, t->F_mat, t->D_mat, t->J_mat,
                   t->K_mat, t->X_mat, t->tmp_mat, t->Cocc_mat, t->eigval, t->ev_idx};
     for (void *p : hp) afree(p);
+    lap(7);
+    if (report)
+        printf("* release (ms): sync %.2f, graphs %.2f, pinned %.2f, guess net %.2f, eig/K-mix/rank-k %.2f, "
+               "buffers %.2f, events/stream %.2f, host mirrors %.2f\n",
+               ms[0], ms[1], ms[2], ms[3], ms[4], ms[5], ms[6], ms[7]);
 }
 
 void die(const char *fn, int rc)
